@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""PageRank GTEPS on one B200: R-MAT scale 24, edge factor 16, run to normalised
+L1 residual <= 1e-8 (damping 0.85, FP32 values, FP64 residual).
+
+One step = one full PageRank solve (Jacobi, uniform init) to the tolerance on
+the device-resident graph. Synthetic input: the seeded R-MAT generator of
+csrc/gcg_rng.h (a/b/c/d = .57/.19/.19/.05), duplicates and self-loops removed by
+the device sharder, 64 vertex intervals.
+
+  value      GTEPS = edges x sweeps / device time, inputs resident in HBM
+  e2e        same metric through the C ABI with host buffers: pinned host edge
+             arrays -> gcg_graph_from_edges (H2D + device sharder) ->
+             gcg_pagerank -> ranks to host, every step
+  roofline   the main sweep kernel (k_pr_sweep): 8E+16V algorithmic bytes per
+             launch / its CUDA-event launch time, against measured HBM copy GB/s
+  cpu_baseline  the reference's own PageRank app (oracle/_ref/pagerank, built
+             from the reference sources) on a bounded sample, all host cores
+
+--impl reference times the reference alone (rank 0; other ranks exit).
+Under torchrun (N > 1) every rank solves its own replica (the path does not
+shard: replicas only); value sums the ranks' edges over the max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "graphchi-cpp_b200"))
+
+METRIC = "PageRank GTEPS (R-MAT scale 24, ef 16, to L1 residual 1e-8)"
+UNIT = "GTEPS"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic_per_edge():
+    """DRAM bytes per edge of one k_pr_sweep launch, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pagerank_sweep_rmat.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_edge_and_vertex:"):
+                a, b = line.split(":", 1)[1].split()
+                return float(a), float(b)
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def reference_pagerank_sample(scale, ef, seed, niters, threads, steps=1, warmup=0):
+    """Times oracle/_ref/pagerank (example_apps/pagerank.cpp) on an R-MAT sample.
+    Returns (GTEPS per step list, edges, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np  # noqa: F401
+    import oracle as O
+    import gcgpu
+    if not O.ref_available():
+        raise RuntimeError("oracle/_ref is not built")
+    s, d = gcgpu.generate_rmat(scale, ef << scale, seed=seed)
+    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
+    E = int(cs.shape[0])
+    vals = []
+    with O.RefWorkdir(prefix="gcg_bench_ref_") as w:
+        el = w.file("g.el")
+        O.write_edgelist(el, cs, cd)
+        # sharding (untimed preparation): a 1-iteration run creates the shards
+        O.run_ref("pagerank", el, {"niters": 1, "nshards": "auto"}, threads)
+        for i in range(warmup + steps):
+            out, wall = O.run_ref("pagerank", el, {"niters": niters, "nshards": "auto"}, threads)
+            rt = O.ref_runtime(out) or wall
+            if i >= warmup:
+                vals.append(E * niters / rt / 1e9)
+    sample = (f"oracle/_ref/pagerank (example_apps/pagerank.cpp, in-memory vertex program) on R-MAT scale {scale} "
+              f"ef {ef} seed {seed} ({E} edges after dedup), {niters} iterations, engine 'runtime' metric, "
+              f"GTEPS = edges x iterations / runtime, shards prepared untimed, membudget 800 MB")
+    return vals, E, sample
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    try:
+        vals, E, sample = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters, threads,
+                                                    steps=args.steps, warmup=args.warmup)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"[:300]}))
+        return
+    v = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"pagerank_rmat{args.ref_scale}_ef{args.ef}_cpu_sample", "sample_of":
+                   f"pagerank_rmat{args.scale}_ef{args.ef}_to_{args.tol:g}"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gcgpu
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    m = args.ef << args.scale
+
+    # ---- input: seeded R-MAT on the device, sharded on the device ----
+    ts = torch.empty(m, dtype=torch.int32, device="cuda")
+    td = torch.empty(m, dtype=torch.int32, device="cuda")
+    gcgpu.generate_rmat(args.scale, m, 0.57, 0.19, 0.19, seed=args.seed, src=ts, dst=td)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = gcgpu.Graph.from_edges(ts, td, dedup=True, nshards=args.nshards, out_csr=False)
+    torch.cuda.synchronize()
+    shard_s = time.perf_counter() - t0
+    V, E = g.num_vertices, g.num_edges
+    g.set_stream(stream.cuda_stream)
+    out = torch.empty(V, dtype=torch.float32, device="cuda")
+
+    def solve(time_sweeps=False):
+        return g.pagerank(max_sweeps=args.max_sweeps, tol=args.tol, out=out, time_sweeps=time_sweeps)[1]
+
+    for _ in range(args.warmup):
+        st = solve()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K solves, inputs resident ----
+    stats = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(solve(time_sweeps=True))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    sweeps = [s.sweeps for s in stats]
+    edges_done = sum(E * s for s in sweeps) * world
+    value = edges_done / (ms / 1e3) / 1e9
+    launches = sum(s.kernel_launches for s in stats)
+    kern_ms = sum(s.sweep_kernel_ms for s in stats)
+    kern_n = sum(s.timed_sweeps for s in stats)
+    per_launch_s = kern_ms / kern_n / 1e3
+    alg_bytes = 8.0 * E + 16.0 * V
+    achieved = alg_bytes / per_launch_s / 1e9
+    peak, peak_kind = load_peaks()
+    tr = load_traffic_per_edge()
+    traffic = (tr[0] * E + tr[1] * V) if tr else None
+
+    # ---- e2e: host buffers through the C ABI ----
+    hs = torch.empty(m, dtype=torch.int32, pin_memory=True)
+    hd = torch.empty(m, dtype=torch.int32, pin_memory=True)
+    hs.copy_(ts)
+    hd.copy_(td)
+    del ts, td
+    host_rank = np.zeros(V, dtype=np.float32)
+    e2e_times, e2e_edges = [], 0
+    for i in range(args.e2e_warmup + args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with gcgpu.Graph.from_edges(hs, hd, dedup=True, nshards=args.nshards, out_csr=False) as ge:
+            _, st = ge.pagerank(max_sweeps=args.max_sweeps, tol=args.tol, out=host_rank)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if i >= args.e2e_warmup:
+            e2e_times.append(dt)
+            e2e_edges += E * st.sweeps
+    e2e_s = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = e2e_edges * world / e2e_s / 1e9
+
+    # ---- CPU baseline: the reference's own PageRank on a bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            vals, Es, sample = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters,
+                                                         os.cpu_count() or 1)
+            cpu = {"value": vals[0], "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": sample}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"[:300]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"pagerank_rmat{args.scale}_ef{args.ef}_to_{args.tol:g}",
+                       "vertices": V, "edges": E, "raw_edges": m, "nshards": args.nshards,
+                       "sweeps_per_step": sweeps[0], "residual": stats[-1].residual,
+                       "teleport": 0.15, "damping": 0.85, "init": 1.0,
+                       "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (col index array alone > 126 MB)",
+                       "sharding_ms": shard_s * 1e3},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_pr_sweep",
+                         "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_s * 1e3,
+                         "peak_kind": peak_kind},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 4 * V,
+                    "ms_per_step": e2e_s / max(1, args.e2e_steps) * 1e3},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    g.free()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gcgpu", choices=["gcgpu", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--ef", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--max-sweeps", type=int, default=1000)
+    ap.add_argument("--nshards", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-warmup", type=int, default=1)
+    ap.add_argument("--ref-scale", type=int, default=20)
+    ap.add_argument("--ref-iters", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

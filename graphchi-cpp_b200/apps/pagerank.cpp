@@ -1,0 +1,42 @@
+/*
+ * PageRank app on the B200 engine: same command line, outputs and vertex-value
+ * file as example_apps/pagerank.cpp (:148-188). The vertex program is the
+ * in-memory Gauss-Seidel program (pagerank.cpp:121-146), run bit-exactly by
+ * gcg_pagerank(GCG_PR_GS_EXACT). Options: file, niters (4), nshards (auto),
+ * top (20); tol > 0 switches to the Jacobi iteration run to that residual.
+ */
+#include "graphchi_gpu/graphchi_gpu.hpp"
+
+using namespace graphchi;
+
+struct PagerankProgram : public GraphChiProgram<float, float> {
+    double tol = 0.0;
+    device_program device_kind() const override {
+        return device_program::pagerank_vertex_api;
+    }
+    double tolerance() const override { return tol; }
+};
+
+int main(int argc, const char **argv) {
+    try {
+        graphchi_init(argc, argv);
+        metrics m("pagerank");
+        std::string filename = get_option_string("file");
+        int niters = get_option_int("niters", 4);
+        int ntop = get_option_int("top", 20);
+        int nshards = convert_if_notexists<float>(filename, get_option_string("nshards", "auto"));
+        graphchi_engine<float, float> engine(filename, nshards, false, m);
+        PagerankProgram program;
+        program.tol = atof(get_option_string("tol", "0").c_str());
+        engine.run(program, program.tol > 0 ? get_option_int("niters", 1000) : niters);
+        std::vector<vertex_value<float>> top = get_top_vertices<float>(filename, ntop);
+        std::cout << "Print top " << ntop << " vertices:" << std::endl;
+        for (int i = 0; i < (int)top.size(); i++)
+            std::cout << (i + 1) << ". " << top[i].vertex << "\t" << top[i].value << std::endl;
+        metrics_report(m);
+    } catch (const std::exception &e) {
+        std::cerr << "pagerank: " << e.what() << std::endl;
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,149 @@
+/*
+ * Connected components: replaces graphchi_engine::run(ConnectedComponentsProgram)
+ * (example_apps/connectedcomponents.cpp:79-138), whose fixpoint labels every
+ * vertex with the minimum vertex id of its weakly connected component.
+ *
+ * Device form: min-label propagation on roots with pointer-jumping shortcuts
+ * (hook-and-compress). parent[v] starts at v; every edge (u,v) hooks the larger
+ * of the two current roots under the smaller with a CAS (labels only move to
+ * smaller ids, so parent[x] <= x always holds and each final root is the
+ * minimum id of its component); finds shorten paths by pointer jumping (path
+ * halving) as they go; a last pass jumps every vertex to its root. The edge pass
+ * walks the merge-path tiles of the in-CSR, so hubs and empty rows are spread
+ * evenly over the CTAs; one pass suffices because hooking is transitive.
+ * The CAS loop has no waits on other threads: each failed CAS moves to a
+ * strictly smaller id, so it ends.
+ */
+#include <algorithm>
+
+#include "gcg_internal.cuh"
+#include "gcg_mergepath.cuh"
+
+namespace gcg {
+namespace {
+
+__device__ __forceinline__ uint32_t find_root(uint32_t *parent, uint32_t x) {
+    uint32_t p = ((volatile uint32_t *)parent)[x];
+    while (p != x) {
+        uint32_t gp = ((volatile uint32_t *)parent)[p];
+        if (gp != p) ((volatile uint32_t *)parent)[x] = gp; /* path halving: gp < p <= x */
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void hook(uint32_t *parent, uint32_t u, uint32_t v) {
+    uint32_t a = find_root(parent, u);
+    uint32_t b = find_root(parent, v);
+    while (a != b) {
+        uint32_t hi = a > b ? a : b, lo = a > b ? b : a;
+        uint32_t old = atomicCAS(parent + hi, hi, lo);
+        if (old == hi) return;
+        /* hi was hooked elsewhere meanwhile: continue from its new parent */
+        a = find_root(parent, old);
+        b = lo == a ? a : find_root(parent, lo);
+    }
+}
+
+__global__ void k_cc_init(uint32_t nv, uint32_t *parent) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) parent[v] = v;
+}
+
+__global__ void __launch_bounds__(MP_THREADS) k_cc_hook(const uint32_t *__restrict__ rowptr,
+                                                        const uint32_t *__restrict__ col,
+                                                        const uint32_t *__restrict__ tile_row,
+                                                        const uint32_t *__restrict__ tile_edge, uint32_t ntiles,
+                                                        uint32_t *parent) {
+    __shared__ uint32_t s_rowend[MP_TILE];
+    __shared__ uint32_t s_src[MP_TILE];
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t r0 = tile_row[t], r1 = tile_row[t + 1];
+        const uint32_t e0 = tile_edge[t], e1 = tile_edge[t + 1];
+        const uint32_t nrows = r1 - r0, nedges = e1 - e0;
+        for (uint32_t k = threadIdx.x; k < nrows; k += MP_THREADS) s_rowend[k] = rowptr[r0 + k + 1] - e0;
+        for (uint32_t k = threadIdx.x; k < nedges; k += MP_THREADS) s_src[k] = __ldg(col + e0 + k);
+        __syncthreads();
+        const uint32_t items = nrows + nedges;
+        const uint32_t d0 = min((uint32_t)threadIdx.x * MP_ITEMS, items);
+        const uint32_t d1 = min(d0 + MP_ITEMS, items);
+        uint32_t ti = mp_search(s_rowend, nrows, nedges, d0);
+        uint32_t tj = d0 - ti;
+        for (uint32_t d = d0; d < d1; ++d) {
+            if (ti < nrows && s_rowend[ti] <= tj) {
+                ++ti;
+            } else {
+                hook(parent, s_src[tj], r0 + ti);
+                ++tj;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_cc_compress(uint32_t nv, uint32_t *parent, uint32_t *nroots) {
+    uint32_t roots = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        uint32_t r = find_root(parent, v);
+        parent[v] = r;
+        roots += (r == v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) roots += __shfl_down_sync(0xFFFFFFFFu, roots, o);
+    if ((threadIdx.x & 31) == 0 && roots) atomicAdd(nroots, roots);
+}
+
+}  // namespace
+}  // namespace gcg
+
+using namespace gcg;
+
+extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_stats *stats) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_connected_components: null graph");
+    GCG_TRY(ensure_plan(g));
+    cudaStream_t s = g->stream;
+    const uint32_t nv = g->nv;
+    const PrPlan &pl = *g->plan;
+    tbuf<uint32_t> parent_tmp, cnt;
+    uint32_t *parent;
+    const bool dev_out = labels && is_device_ptr(labels);
+    if (dev_out) {
+        parent = labels;
+    } else {
+        GCG_TRY(parent_tmp.alloc(nv, s));
+        parent = parent_tmp.get();
+    }
+    GCG_TRY(cnt.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
+    unsigned vb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, (uint64_t)num_sms() * 16));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cc_hook, MP_THREADS, 0) != cudaSuccess || per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    unsigned tb = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(pl.ntiles, (uint32_t)(num_sms() * per_sm)));
+    cudaEvent_t ev0, ev1;
+    GCG_CUDA(cudaEventCreate(&ev0));
+    GCG_CUDA(cudaEventCreate(&ev1));
+    GCG_CUDA(cudaEventRecord(ev0, s));
+    k_cc_init<<<vb, 256, 0, s>>>(nv, parent);
+    k_cc_hook<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(), pl.tile_edge.get(),
+                                       pl.ntiles, parent);
+    k_cc_compress<<<vb, 256, 0, s>>>(nv, parent, cnt.get());
+    GCG_LAUNCH_CHECK();
+    GCG_CUDA(cudaEventRecord(ev1, s));
+    uint32_t nroots = 0;
+    GCG_CUDA(cudaMemcpyAsync(&nroots, cnt.get(), 4, cudaMemcpyDeviceToHost, s));
+    if (labels && !dev_out) GCG_TRY(copy_out(labels, parent, (size_t)nv * 4, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (stats) {
+        stats->passes = 1;
+        stats->ncomponents = nroots;
+        stats->device_ms = ms;
+    }
+    return GCG_OK;
+}

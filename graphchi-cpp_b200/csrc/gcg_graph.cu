@@ -1,0 +1,407 @@
+/*
+ * The device sharder: edge list -> HBM-resident interval-sorted CSR blocks.
+ *
+ * Replaces (src/preprocessing/sharder.hpp):
+ *   preprocessing_add_edge :427-446  self-loop drop, max vertex id
+ *   shard_flushinfo::flush :161-202  shovel radix sort by dst       -> one device radix sort of
+ *   kway_merge + add       :861-892  merge by dst, interval cuts        (dst<<b | src) keys
+ *   finish_shard           :620-848  per-shard sort by src, adjacency -> stable re-sort by src
+ *   degrees                :748-751, :996-1006                        -> CSR row-pointer differences
+ * Intervals are cut with the sink's exact rule (a shard closes before the first
+ * edge of a new destination once it holds >= edges_per_shard edges; the quota is
+ * recomputed after each cut), found with binary searches over the in-CSR row
+ * pointers instead of a sequential merge.
+ */
+#include <stdio.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gcg_internal.cuh"
+
+namespace gcg {
+namespace {
+
+struct ScanInfo {
+    unsigned long long kept;
+    uint32_t maxid;
+    uint32_t bad;
+};
+
+__global__ void k_scan_edges(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t m,
+                             uint32_t nv_limit, ScanInfo *info) {
+    uint32_t mx = 0, bad = 0;
+    unsigned long long kept = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t s = src[i], d = dst[i];
+        if (s == d) continue; /* sharder.hpp:428-431: self-loops never reach max_vertex_id */
+        ++kept;
+        mx = max(mx, max(s, d));
+        if (nv_limit && (s >= nv_limit || d >= nv_limit)) bad = 1;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_down_sync(0xFFFFFFFFu, mx, o));
+        kept += __shfl_down_sync(0xFFFFFFFFu, kept, o);
+        bad |= __shfl_down_sync(0xFFFFFFFFu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (kept) atomicAdd(&info->kept, kept);
+        if (mx) atomicMax(&info->maxid, mx);
+        if (bad) atomicOr(&info->bad, 1u);
+    }
+}
+
+/* key = (row << vbits) | col; self-loops become the all-ones sentinel, which
+ * sorts after every real key (a real key never has row == col == all ones). */
+__global__ void k_make_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t m,
+                            uint32_t vbits, int sym, uint64_t *__restrict__ keys) {
+    const uint64_t sent = (vbits >= 32) ? ~0ull : ((1ull << (2 * vbits)) - 1ull);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t s = src[i], d = dst[i];
+        bool self = s == d;
+        keys[i] = self ? sent : ((d << vbits) | s);
+        if (sym) keys[m + i] = self ? sent : ((s << vbits) | d);
+    }
+}
+
+__global__ void k_unique_flags(const uint64_t *__restrict__ keys, uint64_t n, uint32_t *__restrict__ flags) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_unique_scatter(const uint64_t *__restrict__ keys, uint64_t n, const uint32_t *__restrict__ pos,
+                                 uint64_t *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (i == 0 || keys[i] != keys[i - 1]) out[pos[i]] = keys[i];
+}
+
+/* Sorted keys -> CSR: col = low bits; rowptr[r] = index of the first key of row r.
+ * The thread owning key i writes the row pointers of rows (row(i-1), row(i)]. */
+__global__ void k_csr_from_keys(const uint64_t *__restrict__ keys, uint64_t n, uint32_t vbits, uint32_t nv,
+                                uint32_t *__restrict__ rowptr, uint32_t *__restrict__ col) {
+    const uint64_t mask = (1ull << vbits) - 1ull;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k = keys[i];
+        col[i] = (uint32_t)(k & mask);
+        int64_t row = (int64_t)(k >> vbits);
+        int64_t prev = (i == 0) ? -1 : (int64_t)(keys[i - 1] >> vbits);
+        for (int64_t r = prev + 1; r <= row; ++r) rowptr[r] = (uint32_t)i;
+        if (i == n - 1)
+            for (int64_t r = row + 1; r <= (int64_t)nv; ++r) rowptr[r] = (uint32_t)n;
+    }
+}
+
+/* Swap the halves of each key: (a << b | c) -> (c << b | a). */
+__global__ void k_swap_key(const uint64_t *__restrict__ in, uint64_t n, uint32_t vbits, uint64_t *__restrict__ out) {
+    const uint64_t mask = (1ull << vbits) - 1ull;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k = in[i];
+        out[i] = ((k & mask) << vbits) | (k >> vbits);
+    }
+}
+
+__global__ void k_degree(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t *__restrict__ deg) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        deg[v] = rowptr[v + 1] - rowptr[v];
+}
+
+__global__ void k_outdeg_hist(const uint32_t *__restrict__ col, uint64_t n, uint32_t *__restrict__ outdeg) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(outdeg + col[i], 1u);
+}
+
+__device__ uint32_t row_of(const uint32_t *rowptr, uint32_t nv, uint32_t x) {
+    /* largest r in [0, nv) with rowptr[r] <= x (the non-empty row holding edge x) */
+    uint32_t lo = 0, hi = nv; /* answer in [lo, hi) */
+    while (hi - lo > 1) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if (rowptr[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+/* One thread: the k-way merge sink's interval cuts (sharder.hpp:861-892, :962). */
+__global__ void k_intervals(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t P, uint32_t *last,
+                            uint32_t *count) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint64_t E = rowptr[nv];
+    const uint32_t max_vid = nv - 1;
+    if (E == 0 || P <= 1) {
+        last[0] = max_vid;
+        *count = 1;
+        return;
+    }
+    uint64_t eps = E / P + 1, base = 0;
+    uint32_t shard = 0;
+    while (shard < P - 1) {
+        uint64_t target = base + (eps > 0 ? eps : 1);
+        if (target >= E) break;
+        uint32_t r = row_of(rowptr, nv, (uint32_t)target);
+        uint64_t j = (rowptr[r] == target) ? target : (uint64_t)rowptr[r + 1];
+        if (j >= E) break;
+        last[shard++] = row_of(rowptr, nv, (uint32_t)(j - 1));
+        eps = (E - j) / (P - shard);
+        base = j;
+    }
+    last[shard] = (shard == P - 1) ? max_vid : row_of(rowptr, nv, (uint32_t)(E - 1));
+    *count = shard + 1;
+}
+
+}  // namespace
+
+unsigned grid_for(uint64_t n, int threads = 256);
+
+int unique_u64(const uint64_t *in, uint64_t n, uint32_t *flags, uint32_t *total_dev, uint64_t *out, cudaStream_t s) {
+    if (n == 0) {
+        GCG_CUDA(cudaMemsetAsync(total_dev, 0, 4, s));
+        return GCG_OK;
+    }
+    k_unique_flags<<<grid_for(n), 256, 0, s>>>(in, n, flags);
+    GCG_LAUNCH_CHECK();
+    GCG_TRY(scan_u32(flags, flags, n, total_dev, s));
+    k_unique_scatter<<<grid_for(n), 256, 0, s>>>(in, n, flags, out);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
+int csr_from_sorted_keys(const uint64_t *keys, uint64_t n, uint32_t vbits, uint32_t nrows, uint32_t *rowptr,
+                         uint32_t *col, cudaStream_t s) {
+    if (n == 0) {
+        GCG_CUDA(cudaMemsetAsync(rowptr, 0, ((size_t)nrows + 1) * 4, s));
+        return GCG_OK;
+    }
+    k_csr_from_keys<<<grid_for(n), 256, 0, s>>>(keys, n, vbits, nrows, rowptr, col);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
+unsigned grid_for(uint64_t n, int threads) {
+    uint64_t b = (n + threads - 1) / threads;
+    uint64_t cap = (uint64_t)num_sms() * 32;
+    if (b > cap) b = cap;
+    if (b == 0) b = 1;
+    return (unsigned)b;
+}
+
+namespace {
+
+int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32_t nv_given, uint32_t flags,
+                uint32_t nshards, gcg_graph **out) {
+    cudaStream_t s = 0;
+    /* stage inputs */
+    tbuf<uint32_t> sbuf, dbuf_;
+    const uint32_t *src = src_u, *dst = dst_u;
+    if (m > 0 && !is_device_ptr(src_u)) {
+        GCG_TRY(sbuf.alloc(m, s));
+        GCG_TRY(copy_in(sbuf.get(), src_u, m * 4, s));
+        src = sbuf.get();
+    }
+    if (m > 0 && !is_device_ptr(dst_u)) {
+        GCG_TRY(dbuf_.alloc(m, s));
+        GCG_TRY(copy_in(dbuf_.get(), dst_u, m * 4, s));
+        dst = dbuf_.get();
+    }
+    /* max id, kept count, range check */
+    tbuf<ScanInfo> d_info;
+    GCG_TRY(d_info.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(d_info.get(), 0, sizeof(ScanInfo), s));
+    if (m > 0) {
+        k_scan_edges<<<grid_for(m), 256, 0, s>>>(src, dst, m, nv_given, d_info.get());
+        GCG_LAUNCH_CHECK();
+    }
+    ScanInfo info;
+    GCG_CUDA(cudaMemcpyAsync(&info, d_info.get(), sizeof(info), cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    if (info.bad) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: vertex id >= num_vertices");
+    uint32_t nv = nv_given ? nv_given : info.maxid + 1; /* sharder.hpp:925: 1 + max_vertex_id */
+    const bool sym = (flags & GCG_BUILD_SYMMETRISE) != 0;
+    const uint64_t nk = sym ? 2 * m : m;
+    const uint64_t kept = sym ? 2 * (uint64_t)info.kept : (uint64_t)info.kept;
+    if (kept > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "more than 2^32-1 edges after filtering");
+    uint32_t vbits = 1;
+    while (vbits < 32 && (1ull << vbits) < nv) ++vbits;
+
+    gcg_graph *g = new gcg_graph();
+    g->nv = nv;
+    g->vbits = vbits;
+    g->stream = s;
+    auto cleanup = [&](int st) {
+        delete g;
+        return st;
+    };
+
+    tbuf<uint64_t> keys, tmp;
+    uint64_t *sorted = nullptr;
+    uint64_t ne = kept;
+    if (nk > 0) {
+        if (keys.alloc(nk, s) || tmp.alloc(nk, s)) return cleanup(GCG_ERR_NOMEM);
+        k_make_keys<<<grid_for(m), 256, 0, s>>>(src, dst, m, vbits, sym ? 1 : 0, keys.get());
+        if (cudaGetLastError() != cudaSuccess) return cleanup(fail(GCG_ERR_CUDA, "k_make_keys launch"));
+        int st = radix_sort_u64(keys.get(), tmp.get(), nk, 0, 2 * (int)vbits, &sorted, s);
+        if (st) return cleanup(st);
+        if ((flags & GCG_BUILD_DEDUP) && kept > 0) {
+            tbuf<uint32_t> fl;
+            tbuf<uint32_t> d_total;
+            if (fl.alloc(kept, s) || d_total.alloc(1, s)) return cleanup(GCG_ERR_NOMEM);
+            uint64_t *other = (sorted == keys.get()) ? tmp.get() : keys.get();
+            if ((st = unique_u64(sorted, kept, fl.get(), d_total.get(), other, s))) return cleanup(st);
+            uint32_t total = 0;
+            if (cudaMemcpyAsync(&total, d_total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                return cleanup(fail(GCG_ERR_CUDA, "dedup: readback failed"));
+            sorted = other;
+            ne = total;
+        }
+    }
+    g->ne = ne;
+    if (g->in_rowptr.alloc((size_t)nv + 1) || g->in_col.alloc(ne) || g->indeg.alloc(nv) || g->outdeg.alloc(nv))
+        return cleanup(GCG_ERR_NOMEM);
+    if (ne == 0) {
+        cudaMemsetAsync(g->in_rowptr.get(), 0, ((size_t)nv + 1) * 4, s);
+    } else {
+        k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(sorted, ne, vbits, nv, g->in_rowptr.get(), g->in_col.get());
+    }
+    k_degree<<<grid_for(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, g->indeg.get());
+    if (!(flags & GCG_BUILD_NO_OUT_CSR)) {
+        if (g->out_rowptr.alloc((size_t)nv + 1) || g->out_col.alloc(ne)) return cleanup(GCG_ERR_NOMEM);
+        if (ne == 0) {
+            cudaMemsetAsync(g->out_rowptr.get(), 0, ((size_t)nv + 1) * 4, s);
+        } else {
+            uint64_t *a = (sorted == keys.get()) ? tmp.get() : keys.get();
+            uint64_t *b = sorted;
+            k_swap_key<<<grid_for(ne), 256, 0, s>>>(sorted, ne, vbits, a);
+            uint64_t *res = nullptr;
+            /* stable sort by the source half only: (dst, src) order -> (src, dst) */
+            int st = radix_sort_u64(a, b, ne, (int)vbits, 2 * (int)vbits, &res, s);
+            if (st) return cleanup(st);
+            k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(res, ne, vbits, nv, g->out_rowptr.get(), g->out_col.get());
+        }
+        k_degree<<<grid_for(nv), 256, 0, s>>>(g->out_rowptr.get(), nv, g->outdeg.get());
+        g->has_out = true;
+    } else {
+        cudaMemsetAsync(g->outdeg.get(), 0, (size_t)nv * 4, s);
+        if (ne > 0) {
+            /* sources are the low halves of the sorted keys; take them from in_col */
+            k_outdeg_hist<<<grid_for(ne), 256, 0, s>>>(g->in_col.get(), ne, g->outdeg.get());
+        }
+    }
+    /* intervals */
+    uint32_t P = nshards ? nshards : 1;
+    tbuf<uint32_t> d_count;
+    if (g->intervals_dev.alloc(P) || d_count.alloc(1, s)) return cleanup(GCG_ERR_NOMEM);
+    k_intervals<<<1, 32, 0, s>>>(g->in_rowptr.get(), nv, P, g->intervals_dev.get(), d_count.get());
+    if (cudaGetLastError() != cudaSuccess) return cleanup(fail(GCG_ERR_CUDA, "graph build kernels failed to launch"));
+    uint32_t cnt = 0;
+    g->intervals_host = (uint32_t *)malloc((size_t)P * 4);
+    if (cudaMemcpyAsync(&cnt, d_count.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(g->intervals_host, g->intervals_dev.get(), (size_t)P * 4, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return cleanup(fail(GCG_ERR_CUDA, std::string("graph build failed: ") + cudaGetErrorString(cudaGetLastError())));
+    g->nshards = cnt;
+    *out = g;
+    return GCG_OK;
+}
+
+}  // namespace
+}  // namespace gcg
+
+using namespace gcg;
+
+extern "C" {
+
+int gcg_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t num_vertices,
+                         uint32_t flags, uint32_t nshards, gcg_graph **out) {
+    if (!out) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: null out");
+    *out = nullptr;
+    if (m > 0 && (!src || !dst)) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: null edge arrays");
+    if (m > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_from_edges: more than 2^32-1 edges");
+    return build_graph(src, dst, m, num_vertices, flags, nshards, out);
+}
+
+int gcg_graph_intervals(const gcg_graph *g, uint32_t *last_vid) {
+    if (!g || !last_vid) return fail(GCG_ERR_INVALID, "gcg_graph_intervals: null argument");
+    GCG_CUDA(cudaMemcpy(last_vid, g->intervals_host, (size_t)g->nshards * 4, cudaMemcpyDefault));
+    return GCG_OK;
+}
+
+}  // extern "C"
+
+namespace gcg {
+namespace {
+__global__ void k_interleave_deg(const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ outdeg, uint32_t nv,
+                                 int32_t *__restrict__ pairs) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        pairs[2 * (size_t)v] = (int32_t)indeg[v];
+        pairs[2 * (size_t)v + 1] = (int32_t)outdeg[v];
+    }
+}
+}  // namespace
+}  // namespace gcg
+
+extern "C" {
+
+int gcg_graph_degrees(const gcg_graph *g, int32_t *pairs) {
+    if (!g || !pairs) return fail(GCG_ERR_INVALID, "gcg_graph_degrees: null argument");
+    tbuf<int32_t> tmp;
+    int32_t *dst = pairs;
+    bool dev = is_device_ptr(pairs);
+    if (!dev) {
+        GCG_TRY(tmp.alloc((size_t)g->nv * 2, g->stream));
+        dst = tmp.get();
+    }
+    k_interleave_deg<<<grid_for(g->nv), 256, 0, g->stream>>>(g->indeg.get(), g->outdeg.get(), g->nv, dst);
+    GCG_LAUNCH_CHECK();
+    if (!dev) GCG_TRY(copy_out(pairs, dst, (size_t)g->nv * 8, g->stream));
+    else GCG_CUDA(cudaStreamSynchronize(g->stream));
+    return GCG_OK;
+}
+
+int gcg_graph_csr(const gcg_graph *g, int which, uint32_t *rowptr, uint32_t *col) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_graph_csr: null graph");
+    const uint32_t *rp, *cl;
+    if (which == GCG_CSR_IN) {
+        rp = g->in_rowptr.get();
+        cl = g->in_col.get();
+    } else if (which == GCG_CSR_OUT) {
+        if (!g->has_out) return fail(GCG_ERR_INVALID, "gcg_graph_csr: graph built without the out-edge CSR");
+        rp = g->out_rowptr.get();
+        cl = g->out_col.get();
+    } else {
+        return fail(GCG_ERR_INVALID, "gcg_graph_csr: which must be GCG_CSR_IN or GCG_CSR_OUT");
+    }
+    if (rowptr) GCG_TRY(copy_out(rowptr, rp, ((size_t)g->nv + 1) * 4, g->stream));
+    if (col) GCG_TRY(copy_out(col, cl, (size_t)g->ne * 4, g->stream));
+    GCG_CUDA(cudaStreamSynchronize(g->stream));
+    return GCG_OK;
+}
+
+int gcg_graph_write_metadata(const gcg_graph *g, const char *base) {
+    if (!g || !base) return fail(GCG_ERR_INVALID, "gcg_graph_write_metadata: null argument");
+    std::string b(base);
+    /* <base>.<P>.intervals: one last-vid per line (sharder.hpp:909-920) */
+    std::string fi = b + "." + std::to_string(g->nshards) + ".intervals";
+    FILE *f = fopen(fi.c_str(), "w");
+    if (!f) return fail(GCG_ERR_IO, "cannot write " + fi);
+    for (uint32_t i = 0; i < g->nshards; ++i) fprintf(f, "%u\n", g->intervals_host[i]);
+    fclose(f);
+    /* <base>.numvertices (sharder.hpp:922-926) */
+    std::string fn = b + ".numvertices";
+    f = fopen(fn.c_str(), "w");
+    if (!f) return fail(GCG_ERR_IO, "cannot write " + fn);
+    fprintf(f, "%u\n", g->nv);
+    fclose(f);
+    /* <base>_degs.bin: struct degree {int in, out} per vertex (sharder.hpp:996-1006) */
+    std::vector<int32_t> deg((size_t)g->nv * 2);
+    GCG_TRY(gcg_graph_degrees(g, deg.data()));
+    std::string fd = b + "_degs.bin";
+    f = fopen(fd.c_str(), "wb");
+    if (!f) return fail(GCG_ERR_IO, "cannot write " + fd);
+    size_t w = fwrite(deg.data(), sizeof(int32_t), deg.size(), f);
+    fclose(f);
+    if (w != deg.size()) return fail(GCG_ERR_IO, "short write to " + fd);
+    return GCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,172 @@
+/*
+ * Internal declarations shared by the libgcgpu translation units.
+ * Not part of the C ABI (that is include/gcgpu.h).
+ */
+#ifndef GCG_INTERNAL_CUH
+#define GCG_INTERNAL_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "gcgpu.h"
+
+namespace gcg {
+
+/* ---- error handling: every exported entry point returns a gcg_status;
+ *      the message of the last failure on this thread is kept. ---------- */
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+
+#define GCG_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t _e = (call);                                                         \
+        if (_e != cudaSuccess) {                                                         \
+            return ::gcg::fail(_e == cudaErrorMemoryAllocation ? GCG_ERR_NOMEM : GCG_ERR_CUDA, \
+                               std::string(#call) + ": " + cudaGetErrorString(_e));      \
+        }                                                                                \
+    } while (0)
+
+#define GCG_TRY(expr)                 \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != GCG_OK) return _s;  \
+    } while (0)
+
+#define GCG_LAUNCH_CHECK() GCG_CUDA(cudaGetLastError())
+
+/* ---- device buffers ----------------------------------------------------- */
+template <typename T>
+struct dbuf {
+    T *p = nullptr;
+    size_t n = 0;
+    dbuf() = default;
+    dbuf(const dbuf &) = delete;
+    dbuf &operator=(const dbuf &) = delete;
+    ~dbuf() { release(); }
+    int alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(GCG_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+                                            " bytes: " + cudaGetErrorString(e));
+        }
+        n = count;
+        return GCG_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    T *get() const { return p; }
+};
+
+/* Stream-ordered temporary buffer: allocated with cudaMallocAsync and released
+ * with cudaFreeAsync on the same stream, so its lifetime follows the kernels
+ * queued on that stream without host synchronisation. */
+template <typename T>
+struct tbuf {
+    T *p = nullptr;
+    cudaStream_t s = 0;
+    tbuf() = default;
+    tbuf(const tbuf &) = delete;
+    tbuf &operator=(const tbuf &) = delete;
+    ~tbuf() { release(); }
+    int alloc(size_t count, cudaStream_t stream) {
+        release();
+        s = stream;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), stream);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(GCG_ERR_NOMEM, std::string("cudaMallocAsync of ") + std::to_string(count * sizeof(T)) +
+                                            " bytes: " + cudaGetErrorString(e));
+        }
+        return GCG_OK;
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+    }
+    T *get() const { return p; }
+};
+
+/* Pointer classification: device-resident buffers are used in place; anything
+ * else is treated as host memory and staged through a device copy. */
+bool is_device_ptr(const void *p);
+
+/* Copy count elements between a user pointer (host or device) and device memory. */
+int copy_in(void *dst_dev, const void *src_user, size_t bytes, cudaStream_t s);
+int copy_out(void *dst_user, const void *src_dev, size_t bytes, cudaStream_t s);
+
+/* Number of SMs on the current device (cached). */
+int num_sms();
+
+/* ---- the graph handle: device-resident CSR blocks ---------------------- */
+struct PrPlan;
+
+}  // namespace gcg
+
+struct gcg_graph {
+    uint32_t nv = 0;       /* vertices: max id + 1 (sharder.hpp:925) or caller-given */
+    uint64_t ne = 0;       /* directed edges after filtering */
+    uint32_t nshards = 0;  /* intervals produced */
+    uint32_t vbits = 0;    /* bits of a vertex id (ceil log2 nv) */
+    cudaStream_t stream = 0;
+
+    /* in-edges grouped by destination, sources ascending (memory shard order) */
+    gcg::dbuf<uint32_t> in_rowptr, in_col;
+    /* out-edges grouped by source, destinations ascending (shard order by src) */
+    gcg::dbuf<uint32_t> out_rowptr, out_col;
+    bool has_out = false;
+    gcg::dbuf<uint32_t> indeg, outdeg;
+    gcg::dbuf<uint32_t> intervals_dev; /* last vid per interval */
+    uint32_t *intervals_host = nullptr;
+
+    /* merge-path tiling of the in-CSR, built on first use */
+    gcg::PrPlan *plan = nullptr;
+
+    ~gcg_graph();
+};
+
+namespace gcg {
+
+/* ---- radix sort (gcg_sort.cu) ------------------------------------------ */
+/* Stable LSD sort of n 64-bit keys by bits [begin_bit, end_bit). keys and tmp
+ * are device arrays of n; the sorted keys end in *result (keys or tmp). */
+int radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int begin_bit, int end_bit,
+                   uint64_t **result, cudaStream_t s);
+
+/* Exclusive scan of n uint32 values (device), returns the total through *total_dev
+ * (device pointer, may be null). in and out may alias. */
+int scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total_dev, cudaStream_t s);
+
+/* Unique of sorted keys: out[0..total) = distinct keys (flags: n scratch). */
+int unique_u64(const uint64_t *in, uint64_t n, uint32_t *flags, uint32_t *total_dev, uint64_t *out, cudaStream_t s);
+
+/* Sorted (row << vbits | col) keys -> CSR with nrows rows. */
+int csr_from_sorted_keys(const uint64_t *keys, uint64_t n, uint32_t vbits, uint32_t nrows, uint32_t *rowptr,
+                         uint32_t *col, cudaStream_t s);
+
+/* ---- merge-path plan (gcg_pagerank.cu) --------------------------------- */
+struct PrPlan {
+    uint32_t ntiles = 0;
+    dbuf<uint32_t> tile_row, tile_edge; /* ntiles+1 merge-path coordinates */
+    dbuf<uint32_t> fix_start;           /* per tile: first tile of a head-split row ending here, or ~0 */
+};
+int ensure_plan(gcg_graph *g);
+
+/* exact Gauss-Seidel PageRank (gcg_pagerank_gs.cu) */
+int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats);
+
+constexpr int MP_THREADS = 256;
+constexpr int MP_ITEMS = 8;
+constexpr int MP_TILE = MP_THREADS * MP_ITEMS;
+
+}  // namespace gcg
+
+#endif

@@ -1,0 +1,249 @@
+/*
+ * Device radix sort and scan: the B200 replacement of the sharder's shovel sort
+ * (stable LSD radix sort with 8-bit digits, src/util/radixSort.hpp:50-116, used by
+ * shard_flushinfo::flush sharder.hpp:192 and finish_shard sharder.hpp:640).
+ *
+ * Design (HBM-bound integer work, no tensor cores):
+ *   per 8-bit digit pass: upsweep (per-tile digit histogram, warp-aggregated with
+ *   __match_any_sync, no atomics) -> exclusive scan of the digit-major count table
+ *   -> downsweep (stable in-tile ranking in 16 rounds of 256 keys, keys regrouped
+ *   by digit in shared memory, then written so that each digit run of a tile is a
+ *   contiguous, coalesced store).
+ * Tiles are 4096 keys (256 threads x 16); keys are read with striped, coalesced loads.
+ */
+#include "gcg_internal.cuh"
+
+namespace gcg {
+
+namespace {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) rs_upsweep(const uint64_t *__restrict__ keys, uint64_t n,
+                                                         int shift, uint32_t dmask, uint32_t ntiles,
+                                                         uint32_t *__restrict__ counts) {
+    __shared__ uint32_t hist[RS_WARPS][256];
+    for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS) (&hist[0][0])[i] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t dig[RS_ITEMS];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        uint64_t i = base + (uint64_t)k * RS_THREADS + threadIdx.x;
+        dig[k] = (i < n) ? (uint32_t)((__ldg(keys + i) >> shift) & dmask) : 256u;
+    }
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        uint32_t d = dig[k];
+        uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        if (d < 256u && lane == __ffs(peers) - 1) hist[warp][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) s += hist[w][threadIdx.x];
+    counts[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s;
+}
+
+/* Block-wide exclusive scan of one uint32 per thread (RS_THREADS threads). */
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t x, uint32_t *s_warp) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t v = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) s_warp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < RS_WARPS) ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < RS_WARPS) s_warp[lane] = w;
+    }
+    __syncthreads();
+    uint32_t before = warp ? s_warp[warp - 1] : 0u;
+    return before + v - x;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint64_t *__restrict__ keys_in,
+                                                           uint64_t *__restrict__ keys_out, uint64_t n,
+                                                           int shift, uint32_t dmask, uint32_t ntiles,
+                                                           const uint32_t *__restrict__ counts,
+                                                           const uint32_t *__restrict__ offsets) {
+    __shared__ uint64_t s_keys[RS_TILE];
+    __shared__ uint32_t s_gofs[256];
+    __shared__ uint32_t s_lstart[256];
+    __shared__ uint16_t s_wcnt[RS_WARPS][256];
+    __shared__ uint16_t s_wpre[RS_WARPS][256];
+    __shared__ uint32_t s_scan[RS_WARPS];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+    const uint32_t tile_n = (n - base) < (uint64_t)RS_TILE ? (uint32_t)(n - base) : (uint32_t)RS_TILE;
+
+    uint64_t key[RS_ITEMS];
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        uint64_t i = base + (uint64_t)k * RS_THREADS + tid;
+        key[k] = (i < n) ? __ldg(keys_in + i) : 0ull;
+    }
+    s_gofs[tid] = offsets[(uint64_t)tid * ntiles + blockIdx.x];
+    uint32_t h = counts[(uint64_t)tid * ntiles + blockIdx.x];
+    for (int w = 0; w < RS_WARPS; ++w) s_wcnt[w][tid] = 0;
+    uint32_t lstart = block_excl_scan(h, s_scan);
+    s_lstart[tid] = lstart;
+    uint32_t run = 0; /* owner thread tid keeps the running count of digit tid */
+    __syncthreads();
+
+#pragma unroll 1
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const bool valid = (uint64_t)k * RS_THREADS + tid < tile_n;
+        const uint32_t d = valid ? (uint32_t)((key[k] >> shift) & dmask) : 256u;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t rank = __popc(peers & lanemask_lt());
+        if (valid && lane == __ffs(peers) - 1) s_wcnt[warp][d] = (uint16_t)__popc(peers);
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) {
+            uint32_t c = s_wcnt[w][tid];
+            s_wpre[w][tid] = (uint16_t)run;
+            s_wcnt[w][tid] = 0;
+            run += c;
+        }
+        __syncthreads();
+        if (valid) s_keys[s_lstart[d] + s_wpre[warp][d] + rank] = key[k];
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+        uint64_t kk = s_keys[i];
+        uint32_t d = (uint32_t)((kk >> shift) & dmask);
+        keys_out[(uint64_t)s_gofs[d] + (i - s_lstart[d])] = kk;
+    }
+}
+
+/* ---- scan -------------------------------------------------------------- */
+
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 16;
+constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
+
+__global__ void __launch_bounds__(SC_THREADS) sc_reduce(const uint32_t *__restrict__ in, uint64_t n,
+                                                        uint32_t *__restrict__ sums) {
+    __shared__ uint32_t s_warp[SC_THREADS / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * SC_TILE;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SC_ITEMS; ++k) {
+        uint64_t i = base + (uint64_t)k * SC_THREADS + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < SC_THREADS / 32; ++w) t += s_warp[w];
+        sums[blockIdx.x] = t;
+    }
+}
+
+/* Exclusive scan of one tile with a carried-in offset (offsets[blockIdx] or 0). */
+__global__ void __launch_bounds__(SC_THREADS) sc_scan_tile(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                           const uint32_t *__restrict__ block_off,
+                                                           uint32_t *total) {
+    __shared__ uint32_t s_v[SC_TILE];
+    __shared__ uint32_t s_warp[SC_THREADS / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * SC_TILE;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < SC_ITEMS; ++k) {
+        uint64_t i = base + (uint64_t)k * SC_THREADS + tid;
+        s_v[k * SC_THREADS + tid] = (i < n) ? in[i] : 0u;
+    }
+    __syncthreads();
+    uint32_t loc[SC_ITEMS];
+    uint32_t t = 0;
+#pragma unroll
+    for (int k = 0; k < SC_ITEMS; ++k) {
+        loc[k] = t;
+        t += s_v[tid * SC_ITEMS + k];
+    }
+    uint32_t pre = block_excl_scan(t, s_warp);
+    uint32_t off = block_off ? block_off[blockIdx.x] : 0u;
+#pragma unroll
+    for (int k = 0; k < SC_ITEMS; ++k) s_v[tid * SC_ITEMS + k] = off + pre + loc[k];
+    if (total && tid == SC_THREADS - 1 && (uint64_t)(blockIdx.x + 1) * SC_TILE >= n) *total = off + pre + t;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SC_ITEMS; ++k) {
+        uint64_t i = base + (uint64_t)k * SC_THREADS + tid;
+        if (i < n) out[i] = s_v[k * SC_THREADS + tid];
+    }
+}
+
+}  // namespace
+
+int scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total_dev, cudaStream_t s) {
+    if (n == 0) {
+        if (total_dev) GCG_CUDA(cudaMemsetAsync(total_dev, 0, sizeof(uint32_t), s));
+        return GCG_OK;
+    }
+    uint64_t nb = (n + SC_TILE - 1) / SC_TILE;
+    if (nb == 1) {
+        sc_scan_tile<<<1, SC_THREADS, 0, s>>>(in, out, n, nullptr, total_dev);
+        GCG_LAUNCH_CHECK();
+        return GCG_OK;
+    }
+    tbuf<uint32_t> sums;
+    GCG_TRY(sums.alloc(nb, s));
+    sc_reduce<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, n, sums.get());
+    GCG_LAUNCH_CHECK();
+    GCG_TRY(scan_u32(sums.get(), sums.get(), nb, nullptr, s));
+    sc_scan_tile<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, out, n, sums.get(), total_dev);
+    GCG_LAUNCH_CHECK();
+    /* sums is released stream-ordered, after the kernels above. */
+    return GCG_OK;
+}
+
+int radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int begin_bit, int end_bit,
+                   uint64_t **result, cudaStream_t s) {
+    *result = keys;
+    if (n <= 1 || end_bit <= begin_bit) return GCG_OK;
+    if (n > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "radix sort: more than 2^32-1 keys");
+    uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    tbuf<uint32_t> counts, offsets;
+    GCG_TRY(counts.alloc((size_t)256 * ntiles, s));
+    GCG_TRY(offsets.alloc((size_t)256 * ntiles, s));
+    uint64_t *a = keys, *b = tmp;
+    for (int shift = begin_bit; shift < end_bit; shift += 8) {
+        const int nb = end_bit - shift < 8 ? end_bit - shift : 8;
+        const uint32_t dmask = (1u << nb) - 1u;
+        rs_upsweep<<<ntiles, RS_THREADS, 0, s>>>(a, n, shift, dmask, ntiles, counts.get());
+        GCG_LAUNCH_CHECK();
+        GCG_TRY(scan_u32(counts.get(), offsets.get(), (uint64_t)256 * ntiles, nullptr, s));
+        rs_downsweep<<<ntiles, RS_THREADS, 0, s>>>(a, b, n, shift, dmask, ntiles, counts.get(), offsets.get());
+        GCG_LAUNCH_CHECK();
+        uint64_t *t = a; a = b; b = t;
+    }
+    *result = a;
+    return GCG_OK;
+}
+
+}  // namespace gcg

@@ -1,0 +1,240 @@
+/*
+ * Triangle counting: replaces order_by_degree + the dynamic-graph engine running
+ * TriangleCountingProgram + sum_vertices / 3
+ * (src/preprocessing/util/orderbydegree.hpp:59-143,
+ *  example_apps/trianglecounting.cpp:95-357, :476-477).
+ *
+ * Device form:
+ *   1. rank vertices by (in+out degree, id) ascending with one radix sort
+ *      (orderbydegree.hpp:16-25, 71-89): vertexmap[v] = rank.
+ *   2. orient every edge from the lower to the higher rank, radix sort and
+ *      deduplicate (reciprocal edges collapse, like the reference's lastvid
+ *      checks, trianglecounting.cpp:182,309) -> CSR of higher-ranked neighbours,
+ *      each list ascending.
+ *   3. one warp per vertex a; for each b in N+(a) the lanes take the shorter of
+ *      N+(a) after b and N+(b), binary-search each element in the longer, and
+ *      count matches with warp ballots. A match c is a triangle (a,b,c): c's
+ *      count is bumped per match, b's and a's by the ballot totals — the
+ *      per-rank incident-triangle counts of <base>_degord.4B.vout.
+ * Algorithmic traffic (whole count): 4*sum_{(a,b)}(d+(a)+d+(b)) + 4*E+ + 4*V.
+ */
+#include <algorithm>
+
+#include "gcg_internal.cuh"
+#include "gcg_mergepath.cuh"
+
+namespace gcg {
+namespace {
+
+inline unsigned vgrid(uint64_t n) {
+    uint64_t b = (n + 255) / 256;
+    uint64_t cap = (uint64_t)num_sms() * 16;
+    return (unsigned)std::max<uint64_t>(1, std::min(b, cap));
+}
+
+__global__ void k_degree_keys(const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ outdeg, uint32_t nv,
+                              uint32_t vbits, uint64_t *__restrict__ keys, uint32_t *maxdeg) {
+    uint32_t m = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        uint64_t d = (uint64_t)indeg[v] + outdeg[v];
+        keys[v] = (d << vbits) | v;
+        m = max(m, d > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxdeg, m);
+}
+
+__global__ void k_rank_scatter(const uint64_t *__restrict__ sorted, uint32_t nv, uint32_t vbits,
+                               uint32_t *__restrict__ rank) {
+    const uint64_t mask = (1ull << vbits) - 1ull;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        rank[(uint32_t)(sorted[i] & mask)] = i;
+}
+
+/* key of edge e (row v, source u): (min rank << vbits) | max rank */
+__global__ void __launch_bounds__(MP_THREADS) k_orient_keys(const uint32_t *__restrict__ rowptr,
+                                                            const uint32_t *__restrict__ col,
+                                                            const uint32_t *__restrict__ tile_row,
+                                                            const uint32_t *__restrict__ tile_edge, uint32_t ntiles,
+                                                            const uint32_t *__restrict__ rank, uint32_t vbits,
+                                                            uint64_t *__restrict__ keys) {
+    __shared__ uint32_t s_rowend[MP_TILE];
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t r0 = tile_row[t], r1 = tile_row[t + 1];
+        const uint32_t e0 = tile_edge[t], e1 = tile_edge[t + 1];
+        const uint32_t nrows = r1 - r0, nedges = e1 - e0;
+        for (uint32_t k = threadIdx.x; k < nrows; k += MP_THREADS) s_rowend[k] = rowptr[r0 + k + 1] - e0;
+        __syncthreads();
+        const uint32_t items = nrows + nedges;
+        const uint32_t d0 = min((uint32_t)threadIdx.x * MP_ITEMS, items);
+        const uint32_t d1 = min(d0 + MP_ITEMS, items);
+        uint32_t ti = mp_search(s_rowend, nrows, nedges, d0);
+        uint32_t tj = d0 - ti;
+        for (uint32_t d = d0; d < d1; ++d) {
+            if (ti < nrows && s_rowend[ti] <= tj) {
+                ++ti;
+            } else {
+                uint64_t a = rank[__ldg(col + e0 + tj)], b = rank[r0 + ti];
+                keys[e0 + tj] = a < b ? ((a << vbits) | b) : ((b << vbits) | a);
+                ++tj;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ bool bsearch_u32(const uint32_t *a, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < x) lo = mid + 1; else hi = mid;
+    }
+    return lo < n && __ldg(a + lo) == x;
+}
+
+__global__ void k_tc_count(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ cl, uint32_t nv,
+                           uint32_t *__restrict__ cnt, unsigned long long *total) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long mine = 0;
+    for (uint32_t a = warp; a < nv; a += nwarps) {
+        const uint32_t ab = rp[a], ae = rp[a + 1];
+        uint32_t acc = 0;
+        for (uint32_t j = ab; j + 1 < ae; ++j) {
+            const uint32_t b = __ldg(cl + j);
+            const uint32_t *A = cl + j + 1;
+            const uint32_t na = ae - j - 1;
+            const uint32_t *B = cl + rp[b];
+            const uint32_t nb = rp[b + 1] - rp[b];
+            if (nb == 0) continue;
+            const uint32_t *S = na <= nb ? A : B, *L = na <= nb ? B : A;
+            const uint32_t ns = na <= nb ? na : nb, nl = na <= nb ? nb : na;
+            uint32_t cab = 0;
+            for (uint32_t base = 0; base < ns; base += 32) {
+                const uint32_t k = base + lane;
+                bool f = false;
+                uint32_t x = 0;
+                if (k < ns) {
+                    x = __ldg(S + k);
+                    f = bsearch_u32(L, nl, x);
+                    if (f) atomicAdd(cnt + x, 1u);
+                }
+                cab += __popc(__ballot_sync(0xFFFFFFFFu, f));
+            }
+            if (cab) {
+                if (lane == 0) atomicAdd(cnt + b, cab);
+                acc += cab;
+            }
+        }
+        if (acc && lane == 0) {
+            atomicAdd(cnt + a, acc);
+            mine += acc;
+        }
+    }
+    if (lane == 0 && mine) atomicAdd(total, mine);
+}
+
+}  // namespace
+}  // namespace gcg
+
+using namespace gcg;
+
+extern "C" int gcg_triangle_count(gcg_graph *g, uint64_t *total, uint32_t *per_rank, uint32_t *vertexmap,
+                                  gcg_tc_stats *stats) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_triangle_count: null graph");
+    GCG_TRY(ensure_plan(g));
+    cudaStream_t s = g->stream;
+    const uint32_t nv = g->nv, vbits = g->vbits;
+    const uint64_t ne = g->ne;
+    const PrPlan &pl = *g->plan;
+
+    cudaEvent_t ev0, ev1;
+    GCG_CUDA(cudaEventCreate(&ev0));
+    GCG_CUDA(cudaEventCreate(&ev1));
+    GCG_CUDA(cudaEventRecord(ev0, s));
+
+    /* 1. degree ranking */
+    tbuf<uint64_t> keys, tmp;
+    tbuf<uint32_t> rank, dmax;
+    GCG_TRY(keys.alloc(std::max<uint64_t>(nv, ne), s));
+    GCG_TRY(tmp.alloc(std::max<uint64_t>(nv, ne), s));
+    GCG_TRY(rank.alloc(nv, s));
+    GCG_TRY(dmax.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(dmax.get(), 0, 4, s));
+    k_degree_keys<<<vgrid(nv), 256, 0, s>>>(g->indeg.get(), g->outdeg.get(), nv, vbits, keys.get(), dmax.get());
+    uint32_t maxdeg = 0;
+    GCG_CUDA(cudaMemcpyAsync(&maxdeg, dmax.get(), 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    uint32_t dbits = 1;
+    while (dbits < 33 && (1ull << dbits) <= maxdeg) ++dbits;
+    if (vbits + dbits > 64) return fail(GCG_ERR_UNSUPPORTED, "gcg_triangle_count: degree and id do not fit 64 bits");
+    uint64_t *sorted = nullptr;
+    GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nv, 0, (int)(vbits + dbits), &sorted, s));
+    k_rank_scatter<<<vgrid(nv), 256, 0, s>>>(sorted, nv, vbits, rank.get());
+    GCG_LAUNCH_CHECK();
+
+    /* 2. oriented, deduplicated edges in rank space */
+    uint64_t m_or = 0;
+    dbuf<uint32_t> rp, cl;
+    GCG_TRY(rp.alloc((size_t)nv + 1));
+    if (ne > 0) {
+        int per_sm = 4;
+        unsigned tb = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(pl.ntiles, (uint32_t)(num_sms() * per_sm)));
+        k_orient_keys<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(),
+                                               pl.tile_edge.get(), pl.ntiles, rank.get(), vbits, keys.get());
+        GCG_LAUNCH_CHECK();
+        GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), ne, 0, 2 * (int)vbits, &sorted, s));
+        /* unique: flags + scan + scatter, then CSR by the low-rank half */
+        tbuf<uint32_t> fl, d_tot;
+        GCG_TRY(fl.alloc(ne, s));
+        GCG_TRY(d_tot.alloc(1, s));
+        uint64_t *other = sorted == keys.get() ? tmp.get() : keys.get();
+        GCG_TRY(unique_u64(sorted, ne, fl.get(), d_tot.get(), other, s));
+        uint32_t tot = 0;
+        GCG_CUDA(cudaMemcpyAsync(&tot, d_tot.get(), 4, cudaMemcpyDeviceToHost, s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+        m_or = tot;
+        GCG_TRY(cl.alloc(m_or));
+        GCG_TRY(csr_from_sorted_keys(other, m_or, vbits, nv, rp.get(), cl.get(), s));
+    } else {
+        GCG_TRY(cl.alloc(1));
+        GCG_CUDA(cudaMemsetAsync(rp.get(), 0, ((size_t)nv + 1) * 4, s));
+    }
+
+    /* 3. count */
+    tbuf<uint32_t> cnt;
+    tbuf<unsigned long long> d_total;
+    uint32_t *cnt_ptr;
+    const bool dev_counts = per_rank && is_device_ptr(per_rank);
+    if (dev_counts) {
+        cnt_ptr = per_rank;
+    } else {
+        GCG_TRY(cnt.alloc(nv, s));
+        cnt_ptr = cnt.get();
+    }
+    GCG_TRY(d_total.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(cnt_ptr, 0, (size_t)nv * 4, s));
+    GCG_CUDA(cudaMemsetAsync(d_total.get(), 0, 8, s));
+    unsigned cb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv * 32 + 255) / 256, (uint64_t)num_sms() * 32));
+    k_tc_count<<<cb, 256, 0, s>>>(rp.get(), cl.get(), nv, cnt_ptr, d_total.get());
+    GCG_LAUNCH_CHECK();
+    GCG_CUDA(cudaEventRecord(ev1, s));
+    unsigned long long tri = 0;
+    GCG_CUDA(cudaMemcpyAsync(&tri, d_total.get(), 8, cudaMemcpyDeviceToHost, s));
+    if (per_rank && !dev_counts) GCG_TRY(copy_out(per_rank, cnt_ptr, (size_t)nv * 4, s));
+    if (vertexmap) GCG_TRY(copy_out(vertexmap, rank.get(), (size_t)nv * 4, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (total) *total = tri;
+    if (stats) {
+        stats->triangles = tri;
+        stats->oriented_edges = m_or;
+        stats->device_ms = ms;
+    }
+    return GCG_OK;
+}

@@ -1,0 +1,295 @@
+"""ctypes binding of libgcgpu, the C ABI declared in include/gcgpu.h.
+
+This is plumbing for Python callers (tests, bench): every call goes straight to
+the CUDA library. There is no CPU fallback: if ``lib/libgcgpu.so`` has not been
+built, importing this package raises ImportError.
+
+Arrays may be numpy arrays (host memory) or CUDA torch tensors (device memory);
+the library uses device memory in place and stages host memory itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libgcgpu.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libgcgpu.so not found at {LIB_PATH}: build it with `make -C graphchi-cpp_b200` "
+        "(or __graft_entry__.build()); there is no CPU fallback")
+
+_lib = C.CDLL(LIB_PATH)
+
+GCG_OK = 0
+STATUS_NAMES = {0: "GCG_OK", -1: "GCG_ERR_INVALID", -2: "GCG_ERR_CUDA", -3: "GCG_ERR_NOMEM",
+                -4: "GCG_ERR_IO", -5: "GCG_ERR_FORMAT", -6: "GCG_ERR_UNSUPPORTED",
+                -7: "GCG_ERR_TIMEOUT"}
+
+BUILD_DEDUP = 0x1
+BUILD_SYMMETRISE = 0x2
+BUILD_NO_OUT_CSR = 0x4
+CSR_IN = 0
+CSR_OUT = 1
+PR_JACOBI = 0
+PR_GS_EXACT = 1
+PR_TIME_SWEEPS = 0x1
+
+# Every symbol include/gcgpu.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "gcg_graph_from_edges", "gcg_graph_from_edgelist_file", "gcg_parse_edgelist_file",
+    "gcg_graph_free", "gcg_graph_set_stream", "gcg_graph_get_info", "gcg_graph_intervals",
+    "gcg_graph_degrees", "gcg_graph_csr", "gcg_graph_write_metadata", "gcg_write_vout",
+    "gcg_pr_params_default", "gcg_pagerank", "gcg_connected_components", "gcg_triangle_count",
+    "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
+]
+
+
+class GcgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("num_vertices", C.c_uint32), ("nshards", C.c_uint32), ("num_edges", C.c_uint64),
+                ("has_out_csr", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class PrParams(C.Structure):
+    _fields_ = [("mode", C.c_int), ("max_sweeps", C.c_int), ("teleport", C.c_double),
+                ("damping", C.c_double), ("tol", C.c_double), ("init", C.c_float),
+                ("flags", C.c_uint32), ("init_rank", C.c_void_p), ("residuals", C.c_void_p)]
+
+
+class PrStats(C.Structure):
+    _fields_ = [("sweeps", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
+                ("device_ms", C.c_double), ("sweep_kernel_ms", C.c_double), ("timed_sweeps", C.c_int),
+                ("kernel_launches", C.c_int)]
+
+
+class CcStats(C.Structure):
+    _fields_ = [("passes", C.c_int), ("ncomponents", C.c_uint32), ("device_ms", C.c_double)]
+
+
+class TcStats(C.Structure):
+    _fields_ = [("triangles", C.c_uint64), ("oriented_edges", C.c_uint64), ("device_ms", C.c_double)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_vp = C.c_void_p
+_u32, _u64, _i = C.c_uint32, C.c_uint64, C.c_int
+_graph_from_edges = _sig("gcg_graph_from_edges", _i, _vp, _vp, _u64, _u32, _u32, _u32, C.POINTER(_vp))
+_graph_from_file = _sig("gcg_graph_from_edgelist_file", _i, C.c_char_p, _u32, _u32, C.POINTER(_vp))
+_parse_file = _sig("gcg_parse_edgelist_file", _i, C.c_char_p, _vp, _vp, _u64, C.POINTER(_u64))
+_graph_free = _sig("gcg_graph_free", _i, _vp)
+_graph_set_stream = _sig("gcg_graph_set_stream", _i, _vp, _vp)
+_graph_info = _sig("gcg_graph_get_info", _i, _vp, C.POINTER(GraphInfo))
+_graph_intervals = _sig("gcg_graph_intervals", _i, _vp, _vp)
+_graph_degrees = _sig("gcg_graph_degrees", _i, _vp, _vp)
+_graph_csr = _sig("gcg_graph_csr", _i, _vp, _i, _vp, _vp)
+_write_meta = _sig("gcg_graph_write_metadata", _i, _vp, C.c_char_p)
+_write_vout = _sig("gcg_write_vout", _i, C.c_char_p, _vp, _u32, _u32)
+_pr_default = _sig("gcg_pr_params_default", None, C.POINTER(PrParams))
+_pagerank = _sig("gcg_pagerank", _i, _vp, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
+_cc = _sig("gcg_connected_components", _i, _vp, _vp, C.POINTER(CcStats))
+_tc = _sig("gcg_triangle_count", _i, _vp, _vp, _vp, _vp, C.POINTER(TcStats))
+_gen_rmat = _sig("gcg_generate_rmat", _i, _u32, _u64, C.c_double, C.c_double, C.c_double, _u64, _vp, _vp)
+_gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
+_last_error = _sig("gcg_last_error", C.c_char_p)
+_version = _sig("gcg_version", C.c_char_p)
+
+
+def last_error() -> str:
+    return _last_error().decode()
+
+
+def version() -> str:
+    return _version().decode()
+
+
+def check(status: int) -> None:
+    if status != GCG_OK:
+        raise GcgError(status, last_error())
+
+
+def ptr(a):
+    """Address of a numpy array (host) or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"], "array must be contiguous"
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous(), "tensor must be contiguous"
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _u32_host(a):
+    if isinstance(a, np.ndarray):
+        return np.ascontiguousarray(a, dtype=np.uint32)
+    return a
+
+
+class Graph:
+    """Device-resident graph built by the device sharder (gcg_graph_from_edges)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_edges(cls, src, dst, num_vertices=0, dedup=False, symmetrise=False, nshards=1,
+                   out_csr=True) -> "Graph":
+        src, dst = _u32_host(src), _u32_host(dst)
+        m = int(src.shape[0])
+        flags = (BUILD_DEDUP if dedup else 0) | (BUILD_SYMMETRISE if symmetrise else 0) | \
+                (0 if out_csr else BUILD_NO_OUT_CSR)
+        h = _vp()
+        check(_graph_from_edges(ptr(src), ptr(dst), m, num_vertices, flags, nshards, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edgelist_file(cls, path, dedup=False, symmetrise=False, nshards=1, out_csr=True) -> "Graph":
+        flags = (BUILD_DEDUP if dedup else 0) | (BUILD_SYMMETRISE if symmetrise else 0) | \
+                (0 if out_csr else BUILD_NO_OUT_CSR)
+        h = _vp()
+        check(_graph_from_file(os.fsencode(path), flags, nshards, C.byref(h)))
+        return cls(h)
+
+    def free(self):
+        if self._h:
+            _graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int):
+        check(_graph_set_stream(self._h, stream_ptr))
+
+    def info(self) -> GraphInfo:
+        i = GraphInfo()
+        check(_graph_info(self._h, C.byref(i)))
+        return i
+
+    @property
+    def num_vertices(self) -> int:
+        return self.info().num_vertices
+
+    @property
+    def num_edges(self) -> int:
+        return self.info().num_edges
+
+    def intervals(self) -> np.ndarray:
+        out = np.zeros(self.info().nshards, dtype=np.uint32)
+        check(_graph_intervals(self._h, ptr(out)))
+        return out
+
+    def degrees(self) -> np.ndarray:
+        """(V, 2) int32 array of (indegree, outdegree), the _degs.bin layout."""
+        out = np.zeros((self.num_vertices, 2), dtype=np.int32)
+        check(_graph_degrees(self._h, ptr(out)))
+        return out
+
+    def csr(self, which=CSR_IN):
+        i = self.info()
+        rp = np.zeros(i.num_vertices + 1, dtype=np.uint32)
+        col = np.zeros(max(1, i.num_edges), dtype=np.uint32)
+        check(_graph_csr(self._h, which, ptr(rp), ptr(col)))
+        return rp, col[: i.num_edges]
+
+    def write_metadata(self, base: str):
+        check(_write_meta(self._h, os.fsencode(base)))
+
+    def pagerank(self, mode=PR_JACOBI, max_sweeps=3, teleport=0.15, damping=0.85, tol=0.0, init=1.0,
+                 init_rank=None, out=None, residuals=None, time_sweeps=False):
+        """Returns (ranks, PrStats). out/init_rank/residuals: numpy or device tensors."""
+        p = PrParams()
+        _pr_default(C.byref(p))
+        p.mode, p.max_sweeps, p.teleport, p.damping, p.tol, p.init = (
+            mode, max_sweeps, teleport, damping, tol, init)
+        p.flags = PR_TIME_SWEEPS if time_sweeps else 0
+        if init_rank is not None:
+            init_rank = init_rank if not isinstance(init_rank, np.ndarray) else \
+                np.ascontiguousarray(init_rank, dtype=np.float32)
+            p.init_rank = ptr(init_rank)
+        if residuals is not None:
+            p.residuals = ptr(residuals)
+        if out is None:
+            out = np.zeros(self.num_vertices, dtype=np.float32)
+        st = PrStats()
+        check(_pagerank(self._h, C.byref(p), ptr(out), C.byref(st)))
+        return out, st
+
+    def connected_components(self, out=None):
+        if out is None:
+            out = np.zeros(self.num_vertices, dtype=np.uint32)
+        st = CcStats()
+        check(_cc(self._h, ptr(out), C.byref(st)))
+        return out, st
+
+    def triangle_count(self, per_rank=True, vertexmap=True):
+        n = self.num_vertices
+        pr = np.zeros(n, dtype=np.uint32) if per_rank is True else per_rank
+        vm = np.zeros(n, dtype=np.uint32) if vertexmap is True else vertexmap
+        tot = C.c_uint64(0)
+        st = TcStats()
+        check(_tc(self._h, C.byref(tot), ptr(pr) if pr is not None and pr is not False else None,
+                  ptr(vm) if vm is not None and vm is not False else None, C.byref(st)))
+        return int(tot.value), pr, vm, st
+
+
+def parse_edgelist_file(path):
+    m = _u64(0)
+    check(_parse_file(os.fsencode(path), None, None, 0, C.byref(m)))
+    src = np.zeros(max(1, m.value), dtype=np.uint32)
+    dst = np.zeros(max(1, m.value), dtype=np.uint32)
+    check(_parse_file(os.fsencode(path), ptr(src), ptr(dst), m.value, C.byref(m)))
+    return src[: m.value], dst[: m.value]
+
+
+def generate_rmat(scale, m, a=0.57, b=0.19, c=0.19, seed=1, src=None, dst=None):
+    """R-MAT edges into src/dst (allocated as numpy if not given)."""
+    if src is None:
+        src = np.zeros(m, dtype=np.uint32)
+        dst = np.zeros(m, dtype=np.uint32)
+    check(_gen_rmat(scale, m, a, b, c, seed, ptr(src), ptr(dst)))
+    return src, dst
+
+
+def generate_er(n, m, seed=1, src=None, dst=None):
+    if src is None:
+        src = np.zeros(m, dtype=np.uint32)
+        dst = np.zeros(m, dtype=np.uint32)
+    check(_gen_er(n, m, seed, ptr(src), ptr(dst)))
+    return src, dst
+
+
+def write_vout(base, values):
+    values = np.ascontiguousarray(values) if isinstance(values, np.ndarray) else values
+    elem = values.dtype.itemsize if isinstance(values, np.ndarray) else values.element_size()
+    n = values.shape[0]
+    check(_write_vout(os.fsencode(base), ptr(values), n, elem))

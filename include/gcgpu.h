@@ -1,0 +1,213 @@
+/*
+ * gcgpu — C ABI of the B200-native engine for GraphChi's parallel-sliding-windows
+ * hot path: sharder -> graphchi_engine::run() -> GraphChiProgram::update() for
+ * PageRank, connected components and triangle counting.
+ *
+ * Plain C types only: pointers, sizes, status codes. Every call returns a
+ * gcg_status (0 = OK, negative = error) and never aborts; gcg_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * Pointer arguments marked "host or device" may point to host memory (pageable
+ * or pinned) or to device memory of the current CUDA device; device memory is
+ * used in place, host memory is staged through device copies on the graph's
+ * stream. All work of a graph runs on its stream (gcg_graph_set_stream).
+ * Calls on one graph handle are not thread-safe; distinct handles are.
+ *
+ * Each entry point cites the reference interface it replaces
+ * (paths relative to the graphchi-cpp source tree).
+ */
+#ifndef GCGPU_H
+#define GCGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GCG_OK = 0,
+    GCG_ERR_INVALID = -1,     /* bad argument (null, out of range, vertex id >= nv) */
+    GCG_ERR_CUDA = -2,        /* CUDA runtime error (no device, launch failure) */
+    GCG_ERR_NOMEM = -3,       /* device allocation failed */
+    GCG_ERR_IO = -4,          /* file could not be read or written */
+    GCG_ERR_FORMAT = -5,      /* malformed edge-list line */
+    GCG_ERR_UNSUPPORTED = -6, /* request outside this build's limits */
+    GCG_ERR_TIMEOUT = -7      /* a bounded device wait ran out */
+} gcg_status;
+
+typedef struct gcg_graph gcg_graph;
+
+/* ---- graph construction: the device sharder ---------------------------- */
+
+#define GCG_BUILD_DEDUP 0x1u      /* keep one copy of repeated (src,dst) */
+#define GCG_BUILD_SYMMETRISE 0x2u /* add (dst,src) for every (src,dst) before dedup */
+#define GCG_BUILD_NO_OUT_CSR 0x4u /* skip the src-grouped (out-edge) CSR */
+
+/* Replaces sharder<ET>::preprocessing_add_edge + execute_sharding
+ * (src/preprocessing/sharder.hpp:427-446, :535-548, :861-1008) for an edge list
+ * already in memory. Self-loops are dropped (sharder.hpp:428-431). Builds, in
+ * HBM: the in-edge CSR grouped by destination with sources ascending (what each
+ * memory shard holds, memoryshard.hpp:384-519), the out-edge CSR grouped by
+ * source with destinations ascending (each shard's src-sorted order,
+ * sharder.hpp:640), in/out degrees (sharder.hpp:748-751) and `nshards` vertex
+ * intervals split exactly like the sharder's k-way merge sink
+ * (sharder.hpp:861-892). num_vertices = 0 means max id + 1 (sharder.hpp:925);
+ * otherwise every id must be < num_vertices. nshards = 0 means 1.
+ * src/dst: m entries each, host or device. Limits: m < 2^32 after filtering. */
+int gcg_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m,
+                         uint32_t num_vertices, uint32_t flags, uint32_t nshards,
+                         gcg_graph **out);
+
+/* Replaces convert_edgelist (src/preprocessing/conversions.hpp:210-288) followed
+ * by the sharder: parses a text edge list ("src<ws|,>dst[ value]" per line,
+ * '#'/'%' comment lines, delimiters "\t, ", decimal ids), then builds the graph
+ * as gcg_graph_from_edges. Parsing is multithreaded on the host. */
+int gcg_graph_from_edgelist_file(const char *path, uint32_t flags, uint32_t nshards,
+                                 gcg_graph **out);
+
+/* Parses a text edge list into caller arrays without building a graph.
+ * With src/dst NULL only counts: *m_out receives the number of edge lines. */
+int gcg_parse_edgelist_file(const char *path, uint32_t *src, uint32_t *dst, uint64_t capacity,
+                            uint64_t *m_out);
+
+int gcg_graph_free(gcg_graph *g);
+
+/* Makes all later work on g run on `stream` (a cudaStream_t; NULL = legacy default). */
+int gcg_graph_set_stream(gcg_graph *g, void *stream);
+
+typedef struct {
+    uint32_t num_vertices; /* graphchi_engine::num_vertices() (graphchi_engine.hpp:625-627) */
+    uint32_t nshards;      /* intervals produced */
+    uint64_t num_edges;    /* graphchi_engine::num_edges() */
+    uint32_t has_out_csr;
+    uint32_t reserved;
+} gcg_graph_info;
+int gcg_graph_get_info(const gcg_graph *g, gcg_graph_info *info);
+
+/* Last vertex id of each interval: the contents of <base>.<P>.intervals
+ * (sharder.hpp:909-920, read by load_vertex_intervals chifilenames.hpp:380-405).
+ * last_vid: nshards entries, host or device. */
+int gcg_graph_intervals(const gcg_graph *g, uint32_t *last_vid);
+
+/* In/out degrees as struct degree {int indegree; int outdegree;} per vertex:
+ * the contents of <base>_degs.bin (src/engine/auxdata/degree_data.hpp:45-48,
+ * sharder.hpp:996-1006). pairs: 2*num_vertices int32, host or device. */
+int gcg_graph_degrees(const gcg_graph *g, int32_t *pairs);
+
+#define GCG_CSR_IN 0
+#define GCG_CSR_OUT 1
+/* Copies a CSR: rowptr (num_vertices+1) and col (num_edges), host or device. */
+int gcg_graph_csr(const gcg_graph *g, int which, uint32_t *rowptr, uint32_t *col);
+
+/* Writes the sharder's metadata files for `base`: <base>.<P>.intervals,
+ * <base>.numvertices and <base>_degs.bin (sharder.hpp:909-926, :996-1006), so the
+ * reference's readers (load_vertex_intervals, degree_data) accept the graph. */
+int gcg_graph_write_metadata(const gcg_graph *g, const char *base);
+
+/* Writes a vertex-value array as <base>.<elem_size>B.vout, the file
+ * vertex_data_store writes and get_top_vertices / foreach_vertices /
+ * sum_vertices / analyze_labels read (src/engine/auxdata/vertex_data.hpp:52-211,
+ * src/api/chifilenames.hpp:65-71). values: host or device. */
+int gcg_write_vout(const char *base, const void *values, uint32_t num_vertices, uint32_t elem_size);
+
+/* ---- PageRank ---------------------------------------------------------- */
+
+#define GCG_PR_JACOBI 0   /* bulk-synchronous (functional engine, sync mode) */
+#define GCG_PR_GS_EXACT 1 /* vertex-API Gauss-Seidel in id order, bit-exact */
+
+typedef struct {
+    int mode;               /* GCG_PR_JACOBI or GCG_PR_GS_EXACT */
+    int max_sweeps;         /* update sweeps after the initial one (niters - 1) */
+    double teleport;        /* added term: 0.15 (pagerank.cpp:94) or 0.15/N (pagerank_functional.cpp:74) */
+    double damping;         /* 0.85 */
+    double tol;             /* stop after the sweep whose normalised L1 change <= tol; 0 = run max_sweeps */
+    float init;             /* initial vertex value when init_rank is NULL (1.0) */
+    uint32_t flags;         /* GCG_PR_TIME_SWEEPS: time each sweep kernel with CUDA events */
+    const float *init_rank; /* optional initial vector (num_vertices, host or device): the warm start */
+    double *residuals;      /* optional: per-sweep residual log (max_sweeps doubles, host or device) */
+} gcg_pr_params;
+
+#define GCG_PR_TIME_SWEEPS 0x1u
+
+typedef struct {
+    int sweeps;             /* sweeps run */
+    int converged;          /* 1 if the tolerance was met */
+    double residual;        /* normalised L1 change of the last sweep (double) */
+    double device_ms;       /* device time of the sweeps (CUDA events on the graph's stream) */
+    double sweep_kernel_ms; /* with GCG_PR_TIME_SWEEPS: summed time of the main sweep kernel */
+    int timed_sweeps;       /* launches summed into sweep_kernel_ms */
+    int kernel_launches;    /* kernels this call launched (early-exit launches included) */
+} gcg_pr_stats;
+
+/* Fills params with the vertex-API defaults: Jacobi, teleport 0.15, damping 0.85,
+ * init 1.0, 3 sweeps (niters 4, pagerank.cpp:155), tol 0. */
+void gcg_pr_params_default(gcg_pr_params *p);
+
+/* Replaces graphchi_engine::run(PagerankProgram / PagerankProgramInmem / the
+ * functional pagerank_kernel, niters) (graphchi_engine.hpp:718-992,
+ * example_apps/pagerank.cpp:73-144, example_apps/pagerank_functional.cpp:48-83).
+ * JACOBI: r <- init; each sweep r[v] = (float)(teleport + damping * sum_{u->v}
+ * r[u]/outdeg[u]) with float contributions and float sums, FP64 residual.
+ * GS_EXACT: the in-memory vertex program's id-ordered Gauss-Seidel, writing the
+ * same final values as pagerank.cpp:140-143 (pr * outdeg).
+ * out_rank: num_vertices floats, host or device. stats may be NULL. */
+int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats);
+
+/* ---- connected components ---------------------------------------------- */
+
+typedef struct {
+    int passes;        /* edge passes run */
+    uint32_t ncomponents;
+    double device_ms;
+} gcg_cc_stats;
+
+/* Replaces graphchi_engine::run(ConnectedComponentsProgram, niters)
+ * (example_apps/connectedcomponents.cpp:79-138): labels = the fixpoint of
+ * min-label propagation over in- and out-edges, i.e. the minimum vertex id of
+ * each weakly connected component. labels: num_vertices, host or device. */
+int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_stats *stats);
+
+/* ---- triangle counting ------------------------------------------------- */
+
+typedef struct {
+    uint64_t triangles;
+    uint64_t oriented_edges; /* undirected simple edges after orientation */
+    double device_ms;
+} gcg_tc_stats;
+
+/* Replaces order_by_degree + graphchi_dynamicgraph_engine::run(
+ * TriangleCountingProgram) + sum_vertices/3
+ * (src/preprocessing/util/orderbydegree.hpp:59-143,
+ * example_apps/trianglecounting.cpp:288-477). Vertices are ranked by
+ * (in+out degree, id); vertexmap[v] = rank (<base>.vertexmap); per_rank[r] = the
+ * number of triangles through the vertex of rank r (<base>_degord.4B.vout).
+ * total, per_rank and vertexmap may each be NULL; arrays host or device. */
+int gcg_triangle_count(gcg_graph *g, uint64_t *total, uint32_t *per_rank, uint32_t *vertexmap,
+                       gcg_tc_stats *stats);
+
+/* ---- synthetic inputs -------------------------------------------------- */
+
+/* R-MAT edges (quadrant probabilities a, b, c, d = 1-a-b-c), m edges over
+ * 2^scale vertices, seeded; src/dst: m entries each, host or device (device
+ * arrays are filled by a kernel, host arrays by host threads: identical). */
+int gcg_generate_rmat(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed,
+                      uint32_t *src, uint32_t *dst);
+
+/* Erdos-Renyi G(n, m) edges (uniform src and dst in [0, n)), seeded. */
+int gcg_generate_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t *src, uint32_t *dst);
+
+/* ---- errors ------------------------------------------------------------ */
+
+/* Message of the last failure on this thread ("" if none). Replaces the
+ * reference's logstream(LOG_FATAL)/assert exits with a returned status. */
+const char *gcg_last_error(void);
+
+/* Library version string. */
+const char *gcg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,141 @@
+"""The oracle restatement (oracle/oracle.c) pinned against the reference's own
+outputs (tests/golden/*.npz, produced by tests/golden/make_golden.py from the
+compiled reference). CPU only."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_input, golden_names, load_golden
+
+SMALL = [n for n in golden_names() if "s20" not in n]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def check(z, key, arr):
+    if key in z.files:
+        assert np.array_equal(arr, z[key]), key
+    else:
+        assert sha(arr) == str(z[key + "_sha"]), key
+
+
+@pytest.fixture(scope="module", params=SMALL)
+def case(request):
+    z, spec = load_golden(request.param)
+    s, d = golden_input(spec)
+    g = O.OracleGraph(s, d, symmetrise=spec.get("sym", False))
+    return z, spec, g
+
+
+def test_graph_shape(case):
+    z, spec, g = case
+    assert g.nv == int(z["nv"]) and g.ne == int(z["ne"])
+
+
+def test_sharder_intervals_degrees_shards(case):
+    """sharder.hpp:861-892 interval cuts, :748-751 degrees, :620-848 shard contents."""
+    z, spec, g = case
+    for k in z.files:
+        if not k.startswith("intervals_"):
+            continue
+        P = int(k.split("_")[1])
+        assert np.array_equal(g.intervals(P), z[k])
+        assert int(z[f"numvertices_{P}"]) == g.nv
+        check(z, f"degrees_{P}", g.degrees())
+        lo, ss, dd = 0, [], []
+        for hi in z[k]:
+            m = (g.dst >= lo) & (g.dst <= hi)
+            o = np.lexsort((g.dst[m], g.src[m]))
+            ss.append(g.src[m][o])
+            dd.append(g.dst[m][o])
+            lo = int(hi) + 1
+        assert np.array_equal(np.array([len(x) for x in ss]), z[f"shard_sizes_{P}"])
+        check(z, f"shard_src_{P}", np.concatenate(ss))
+        check(z, f"shard_dst_{P}", np.concatenate(dd))
+
+
+def test_pagerank_vertex_api_bitexact(case):
+    """example_apps/pagerank.cpp in-memory program == sequential Gauss-Seidel, bit for bit."""
+    z, spec, g = case
+    keys = [k for k in z.files if k.startswith("pr_gs_") and not k.endswith("_sha")] + \
+           [k[:-4] for k in z.files if k.startswith("pr_gs_") and k.endswith("_sha")]
+    for k in keys:
+        niters = int(k.split("_")[2])
+        check(z, k, g.pagerank_gs_inmem(niters))
+
+
+def test_pagerank_functional_sync(case):
+    """pagerank_functional --mode sync (Jacobi, 0.15/N): normalised L1 <= 1e-6."""
+    z, spec, g = case
+    for k in z.files:
+        if not k.startswith("pr_func_"):
+            continue
+        niters = int(k.split("_")[2])
+        v, _, _ = g.pagerank_jacobi(teleport=0.15 / g.nv, max_sweeps=niters - 1)
+        ref = z[k]
+        assert np.abs(v - ref).sum() / np.abs(ref).sum() <= 1e-6
+
+
+def test_pagerank_residual_stop(case):
+    """Residual-stopped Jacobi with the vertex formula: same residual trace and stop."""
+    z, spec, g = case
+    for k in z.files:
+        if not (k.startswith("pr_oracle_") and k.endswith("_iters")):
+            continue
+        tag = k[: -len("_iters")]
+        niters, tol = int(tag.split("_")[2]), float(tag.split("_")[3])
+        v, n, log = g.pagerank_jacobi(max_sweeps=niters - 1, tol=tol)
+        assert n + 1 == int(z[k])  # the reference counts iteration 0
+        np.testing.assert_allclose(log, z[tag + "_res"], rtol=1e-9, atol=0)
+        ref = z[tag]
+        assert np.abs(v - ref).sum() / np.abs(ref).sum() <= 1e-6
+
+
+def test_connected_components(case):
+    z, spec, g = case
+    if "cc" not in z.files and "cc_sha" not in z.files:
+        pytest.skip("no CC output in this case")
+    lab, _ = g.cc()
+    check(z, "cc", lab)
+    assert int((lab == np.arange(g.nv)).sum()) == int(z["cc_ncomp"])
+
+
+def test_triangle_counting(case):
+    z, spec, g = case
+    if "tc_total" not in z.files:
+        pytest.skip("no TC output in this case")
+    t, per, vm = g.tc()
+    assert t == int(z["tc_total"])
+    check(z, "tc_per_rank", per)
+    check(z, "tc_vertexmap", vm)
+    assert int(per.astype(np.uint64).sum()) == 3 * t
+
+
+def test_auto_nshards():
+    # sharder.hpp:572-575 with membudget 800 MB and 4-byte edge values
+    assert O.auto_nshards(954947, 4, 800) == 1
+    assert O.auto_nshards(268_000_000, 4, 800) == 11
+
+
+def test_generators_restatement_matches_library_host_path():
+    import gcgpu
+    s1, d1 = gcgpu.generate_rmat(12, 50_000, 0.57, 0.19, 0.19, seed=11)
+    s2, d2 = O.rmat_numpy(12, 50_000, 0.57, 0.19, 0.19, seed=11)
+    assert np.array_equal(s1, s2) and np.array_equal(d1, d2)
+    e1, f1 = gcgpu.generate_er(7777, 30_000, seed=5)
+    e2, f2 = O.er_numpy(7777, 30_000, seed=5)
+    assert np.array_equal(e1, e2) and np.array_equal(f1, f2)
+
+
+def test_planted_mistake_is_caught():
+    """A plain Jacobi sweep differs from the reference's Gauss-Seidel app: the
+    golden check must notice (guards against a vacuous comparison)."""
+    z, spec = load_golden("rmat_s10_ef16_seed1")
+    s, d = golden_input(spec)
+    g = O.OracleGraph(s, d)
+    v, _, _ = g.pagerank_jacobi(teleport=0.15, max_sweeps=3, init=1.0)
+    assert not np.array_equal(v, z["pr_gs_4_1_0"])
