@@ -11,7 +11,7 @@ the device sharder, 64 vertex intervals.
   e2e        same metric through the C ABI with host buffers: pinned host edge
              arrays -> gcg_graph_from_edges (H2D + device sharder) ->
              gcg_pagerank -> ranks to host, every step
-  roofline   the main sweep kernel (k_pr_sweep): 8E+16V algorithmic bytes per
+  roofline   the main sweep kernel (k_pr_edges): 8E+16V algorithmic bytes per
              launch / its CUDA-event launch time, against measured HBM copy GB/s
   cpu_baseline  the reference's own PageRank app (oracle/_ref/pagerank, built
              from the reference sources) on a bounded sample, all host cores
@@ -49,7 +49,7 @@ def load_peaks():
 
 
 def load_traffic_per_edge():
-    """DRAM bytes per edge of one k_pr_sweep launch, from the committed ncu summary."""
+    """DRAM bytes per edge and per vertex of one k_pr_edges launch, from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "pagerank_sweep_rmat.md")
     try:
         for line in open(path):
@@ -77,7 +77,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -278,7 +278,7 @@ def run_ours(args, rank, world):
                        "l2": "inputs larger than L2 (col index array alone > 126 MB)",
                        "sharding_ms": shard_s * 1e3},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_pr_sweep",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_pr_edges",
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_s * 1e3,
                          "peak_kind": peak_kind},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * m, "d2h_bytes_per_step": 4 * V,

@@ -81,11 +81,24 @@ __global__ void __launch_bounds__(MP_THREADS) k_cc_hook(const uint32_t *__restri
     }
 }
 
+/* Final pass: every vertex jumps to its root. The find here only reads (no path
+ * halving): a halving store racing with another vertex's final store could put
+ * a non-root ancestor back. The only stores are parent[v] = root(v) by v's own
+ * thread, and a root is an ancestor, so concurrent readers stay correct. */
+__device__ __forceinline__ uint32_t find_root_ro(const uint32_t *parent, uint32_t x) {
+    uint32_t p = ((const volatile uint32_t *)parent)[x];
+    while (p != x) {
+        x = p;
+        p = ((const volatile uint32_t *)parent)[x];
+    }
+    return x;
+}
+
 __global__ void k_cc_compress(uint32_t nv, uint32_t *parent, uint32_t *nroots) {
     uint32_t roots = 0;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        uint32_t r = find_root(parent, v);
-        parent[v] = r;
+        uint32_t r = find_root_ro(parent, v);
+        ((volatile uint32_t *)parent)[v] = r;
         roots += (r == v);
     }
 #pragma unroll

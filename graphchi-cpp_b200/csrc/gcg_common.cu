@@ -50,6 +50,23 @@ int copy_out(void *dst_user, const void *src_dev, size_t bytes, cudaStream_t s) 
     return GCG_OK;
 }
 
+void pool_keep_memory() {
+    static bool done[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return;
+    }
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    done[dev] = true;
+}
+
 int num_sms() {
     static int cached = 0;
     if (cached == 0) {
@@ -116,6 +133,7 @@ static void host_parallel_for(uint64_t m, F f) {
 
 gcg_graph::~gcg_graph() {
     delete plan;
+    gcg::free_chunk_plan(cplan);
     free(intervals_host);
 }
 

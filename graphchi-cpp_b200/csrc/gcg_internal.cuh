@@ -65,6 +65,11 @@ struct dbuf {
     T *get() const { return p; }
 };
 
+/* Keeps memory freed to the current device's default pool cached in this
+ * process (release threshold = max), so repeated calls do not map and unmap
+ * device memory at every synchronisation. Process-local; ends with the process. */
+void pool_keep_memory();
+
 /* Stream-ordered temporary buffer: allocated with cudaMallocAsync and released
  * with cudaFreeAsync on the same stream, so its lifetime follows the kernels
  * queued on that stream without host synchronisation. */
@@ -78,6 +83,7 @@ struct tbuf {
     ~tbuf() { release(); }
     int alloc(size_t count, cudaStream_t stream) {
         release();
+        pool_keep_memory();
         s = stream;
         if (count == 0) count = 1;
         cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), stream);
@@ -108,6 +114,8 @@ int num_sms();
 
 /* ---- the graph handle: device-resident CSR blocks ---------------------- */
 struct PrPlan;
+struct ChunkPlan;
+void free_chunk_plan(ChunkPlan *p);
 
 }  // namespace gcg
 
@@ -127,8 +135,10 @@ struct gcg_graph {
     gcg::dbuf<uint32_t> intervals_dev; /* last vid per interval */
     uint32_t *intervals_host = nullptr;
 
-    /* merge-path tiling of the in-CSR, built on first use */
+    /* merge-path tiling of the in-CSR (CC, TC), built on first use */
     gcg::PrPlan *plan = nullptr;
+    /* 256-edge chunk plan of the in-CSR (PageRank), built on first use */
+    gcg::ChunkPlan *cplan = nullptr;
 
     ~gcg_graph();
 };
@@ -152,11 +162,10 @@ int unique_u64(const uint64_t *in, uint64_t n, uint32_t *flags, uint32_t *total_
 int csr_from_sorted_keys(const uint64_t *keys, uint64_t n, uint32_t vbits, uint32_t nrows, uint32_t *rowptr,
                          uint32_t *col, cudaStream_t s);
 
-/* ---- merge-path plan (gcg_pagerank.cu) --------------------------------- */
+/* ---- merge-path plan (gcg_plan.cu) ------------------------------------- */
 struct PrPlan {
     uint32_t ntiles = 0;
     dbuf<uint32_t> tile_row, tile_edge; /* ntiles+1 merge-path coordinates */
-    dbuf<uint32_t> fix_start;           /* per tile: first tile of a head-split row ending here, or ~0 */
 };
 int ensure_plan(gcg_graph *g);
 

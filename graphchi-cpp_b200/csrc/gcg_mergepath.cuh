@@ -7,11 +7,6 @@
  * degree skew (R-MAT hubs with 10^5 in-edges and long runs of empty rows alike).
  * Tile t covers rows [tile_row[t], tile_row[t+1]) that END in it and edges
  * [tile_edge[t], tile_edge[t+1]).
- *
- * A row whose edges began in an earlier tile (rowptr[r] < tile_edge[t]) is a
- * "head-split" row: its in-tile partial goes to head_part[t] and the row is
- * finished by a fix-up pass that adds the tail partials of the earlier tiles in
- * tile order, so every sum is computed in one fixed order (deterministic).
  */
 #ifndef GCG_MERGEPATH_CUH
 #define GCG_MERGEPATH_CUH
@@ -43,55 +38,6 @@ __device__ __forceinline__ uint32_t mp_search_global(const uint32_t *rowptr, uin
         else hi = mid;
     }
     return (uint32_t)lo;
-}
-
-/* Segmented scan element: f = "a row ended in this thread", v = running partial. */
-struct SegVal {
-    int f;
-    float v;
-};
-
-/* Block-wide segmented scan over MP_THREADS threads. Returns the exclusive
- * prefix value for this thread (the carry into its first finished row) and
- * writes the block's inclusive total value to *total (all threads). */
-__device__ __forceinline__ float seg_scan_excl(SegVal x, SegVal *s_warp, float *total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    SegVal inc = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int fu = __shfl_up_sync(0xFFFFFFFFu, inc.f, o);
-        float vu = __shfl_up_sync(0xFFFFFFFFu, inc.v, o);
-        if (lane >= o) {
-            if (!inc.f) inc.v = vu + inc.v;
-            inc.f |= fu;
-        }
-    }
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        SegVal w = (lane < MP_THREADS / 32) ? s_warp[lane] : SegVal{0, 0.0f};
-#pragma unroll
-        for (int o = 1; o < MP_THREADS / 32; o <<= 1) {
-            int fu = __shfl_up_sync(0xFFFFFFFFu, w.f, o);
-            float vu = __shfl_up_sync(0xFFFFFFFFu, w.v, o);
-            if (lane >= o) {
-                if (!w.f) w.v = vu + w.v;
-                w.f |= fu;
-            }
-        }
-        if (lane < MP_THREADS / 32) s_warp[lane] = w; /* inclusive over warps 0..lane */
-    }
-    __syncthreads();
-    /* prefix of all earlier warps */
-    SegVal wp = warp ? s_warp[warp - 1] : SegVal{0, 0.0f};
-    /* inclusive of the previous lane in this warp */
-    int fp = __shfl_up_sync(0xFFFFFFFFu, inc.f, 1);
-    float vp = __shfl_up_sync(0xFFFFFFFFu, inc.v, 1);
-    float excl;
-    if (lane == 0) excl = wp.v;
-    else excl = fp ? vp : wp.v + vp;
-    *total = s_warp[MP_THREADS / 32 - 1].v;
-    return excl;
 }
 
 }  // namespace gcg

@@ -1,23 +1,31 @@
 /*
- * PageRank on the HBM-resident in-edge CSR.
+ * PageRank on the HBM-resident in-edge CSR (Jacobi / bulk-synchronous form).
  *
  * Replaces graphchi_engine::run() driving the PageRank update()
  * (src/engine/graphchi_engine.hpp:718-992; example_apps/pagerank.cpp:73-144;
  * example_apps/pagerank_functional.cpp:48-83 with
  * src/api/functional/functional_bulksync.hpp:91-113).
  *
- * Jacobi sweep = one persistent merge-path kernel + one fix-up kernel:
- *   k_pr_sweep: per tile, gather contrib[src] for the tile's edges into shared
- *     memory, run each thread's slice of the merge path sequentially, join the
- *     slices with a block segmented scan (warp shuffles), then apply
- *     r' = (float)(teleport + damping*(double)sum), c' = r'/outdeg in float, and
- *     accumulate |r'-r| and |r'| in FP64.
- *   k_pr_fixup: finishes rows split across tiles (tail partials + head partial,
- *     in tile order) and, in the last block to finish, reduces the FP64 residual
- *     partials in a fixed order, logs the residual and raises `done` when the
- *     tolerance is met. Later sweeps already queued see `done` and return at once.
- * Algorithmic traffic per sweep: 8*E + 16*V bytes (col + gathered contrib per
- * edge; rowptr + old rank + new rank + new contrib per vertex).
+ * One sweep = three kernels, all on the graph's stream:
+ *   k_pr_edges   one warp per chunk of 256 consecutive in-edges (8 per lane):
+ *                two 128-bit column loads per lane (streamed: no L1 allocation,
+ *                L2 evict-first), eight independent gathers of contrib[src]
+ *                (L2 evict-last, so the contrib vector stays resident while the
+ *                columns stream past), row starts read from a 1-bit-per-edge
+ *                head bitmap, in-lane segment sums, and a warp segmented scan
+ *                (shuffles) to join rows across lanes. Rows inside the chunk get
+ *                their sum written; a row crossing chunk boundaries leaves one
+ *                partial per chunk.
+ *   k_pr_fix     rows that cross chunks: partials added in chunk order.
+ *   k_pr_vertex  apply for every vertex with in-edges:
+ *                r' = (float)(teleport + damping*(double)sum), c' = r'/outdeg
+ *                (float), FP64 |r'-r| and |r'|; the last block to finish reduces
+ *                the block partials in a fixed order, logs the residual and raises
+ *                `done` when it is <= tol (later queued sweeps return at once).
+ *                Vertices without in-edges are constant (r' = teleport) and are
+ *                written only in the first two sweeps (one per buffer).
+ * Every sum is formed in a fixed order, so results are deterministic.
+ * Algorithmic traffic per sweep: 8*E + 16*V bytes.
  */
 #include <math.h>
 
@@ -25,187 +33,338 @@
 #include <vector>
 
 #include "gcg_internal.cuh"
-#include "gcg_mergepath.cuh"
 
 namespace gcg {
 
 namespace {
 
-__global__ void k_plan(const uint32_t *__restrict__ rowptr, uint32_t nv, uint64_t ne, uint32_t ntiles,
-                       uint32_t *__restrict__ tile_row, uint32_t *__restrict__ tile_edge) {
-    const uint64_t total = (uint64_t)nv + ne;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles; t += gridDim.x * blockDim.x) {
-        uint64_t diag = (uint64_t)t * MP_TILE < total ? (uint64_t)t * MP_TILE : total;
-        uint32_t r = mp_search_global(rowptr, nv, ne, diag);
-        tile_row[t] = r;
-        tile_edge[t] = (uint32_t)(diag - r);
-    }
+constexpr int CH = 256;  /* edges per warp chunk */
+constexpr int EPL = 8;   /* edges per lane */
+
+/* ---- cache-policy loads --------------------------------------------------- */
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint4 ld_stream_v4(const uint32_t *p, uint64_t pol) {
+    uint4 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
+__device__ __forceinline__ float ld_keep_f32(const float *p, uint64_t pol) {
+    float r;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
+    return r;
 }
 
-/* fix_start[t] = first tile whose tail row is the head-split row finished in t. */
-__global__ void k_plan_fix(const uint32_t *__restrict__ rowptr, uint32_t ntiles, const uint32_t *__restrict__ tile_row,
-                           const uint32_t *__restrict__ tile_edge, uint32_t *__restrict__ fix_start) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
-        uint32_t r0 = tile_row[t];
-        uint32_t res = 0xFFFFFFFFu;
-        if (tile_row[t + 1] > r0 && rowptr[r0] < tile_edge[t]) {
-            /* smallest k < t with tile_row[k+1] == r0 (row r0 current at the end of tile k) */
-            uint32_t lo = 0, hi = t;
-            while (lo < hi) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (tile_row[mid + 1] >= r0) hi = mid; else lo = mid + 1;
-            }
-            res = lo;
+/* ---- per-graph plan kernels -------------------------------------------- */
+__global__ void k_nonzero_flags(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t *__restrict__ f) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        f[v] = rowptr[v + 1] > rowptr[v] ? 1u : 0u;
+}
+
+__global__ void k_split_rows(const uint32_t *__restrict__ rowptr, uint32_t nv, const uint32_t *__restrict__ pos,
+                             uint32_t *__restrict__ nz_rows, uint32_t *__restrict__ nz_start,
+                             uint32_t *__restrict__ zero_rows) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        uint32_t b = rowptr[v], e = rowptr[v + 1];
+        if (e > b) {
+            nz_rows[pos[v]] = v;
+            nz_start[pos[v]] = b;
+        } else {
+            zero_rows[v - pos[v]] = v;
         }
-        fix_start[t] = res;
     }
 }
 
-struct PrArgs {
-    const uint32_t *rowptr, *col, *outdeg;
-    const uint32_t *tile_row, *tile_edge, *fix_start;
-    uint32_t ntiles, nv;
-    const float *c_old, *r_old;
-    float *c_new, *r_new;
-    float *head_part, *tail_part;
-    double2 *block_res; /* main kernel partials (gridDim of k_pr_sweep) */
-    uint32_t nblock_res;
-    double2 *fix_res;   /* fix-up kernel partials */
+__global__ void k_head_bits(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint32_t *__restrict__ bits) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        uint32_t p = nz_start[i];
+        atomicOr(bits + (p >> 5), 1u << (p & 31u));
+    }
+}
+
+/* chunk_nz[c] = index of the non-empty row holding edge c*CH */
+__global__ void k_chunk_nz(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint32_t nchunks,
+                           uint32_t *__restrict__ chunk_nz) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const uint64_t pos = (uint64_t)c * CH;
+        uint32_t lo = 0, hi = nnz; /* largest i with nz_start[i] <= pos */
+        while (hi - lo > 1) {
+            uint32_t mid = lo + ((hi - lo) >> 1);
+            if ((uint64_t)nz_start[mid] <= pos) lo = mid; else hi = mid;
+        }
+        chunk_nz[c] = lo;
+    }
+}
+
+__global__ void k_split_flags(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint64_t ne,
+                              uint32_t *__restrict__ f) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        uint64_t b = nz_start[i], e = (i + 1 < nnz) ? nz_start[i + 1] : ne;
+        f[i] = ((b / CH) != ((e - 1) / CH)) ? 1u : 0u;
+    }
+}
+
+__global__ void k_split_list(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint64_t ne,
+                             const uint32_t *__restrict__ pos, uint4 *__restrict__ split) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        uint64_t b = nz_start[i], e = (i + 1 < nnz) ? nz_start[i + 1] : ne;
+        uint32_t cs = (uint32_t)(b / CH), ce = (uint32_t)((e - 1) / CH);
+        if (cs != ce) split[pos[i]] = make_uint4(i, cs, ce, 0u);
+    }
+}
+
+/* ---- sweep kernels ------------------------------------------------------ */
+struct SweepArgs {
+    /* graph / plan */
+    const uint32_t *col, *outdeg;
+    const uint8_t *heads;
+    const uint32_t *chunk_nz, *nz_rows, *zero_rows;
+    const uint4 *split;
+    uint64_t ne;
+    uint32_t nchunks, nnz, nzero, nsplit;
+    uint32_t hub; /* contribs of relabelled sources [0, hub) are cached in shared memory */
+    const uint32_t *nz_cidx, *zero_cidx; /* relabelled ids of the nz / zero rows */
+    /* state (contribs indexed by relabelled id) */
+    const float *c_old;
+    float *c_new;
+    const float *r_nz_old; /* ranks of the vertices with in-edges, compact (nz order) */
+    float *r_nz_new;
+    const uint32_t *od_nz; /* their out-degrees, compact */
+    const float *r_init;   /* full initial vector (residual of the first sweep) */
+    float *nzsum, *head_part, *tail_part;
+    double2 *block_res;
     uint32_t *ticket;
-    int *done;
-    int *sweeps_done;
-    double *res_log;    /* device, max_sweeps entries */
-    double *last_res;
-    double teleport, damping, tol;
+    int *done, *sweeps_done;
+    double *res_log, *last_res;
+    double teleport, damping, tol, norm_const;
 };
 
-__device__ __forceinline__ void pr_apply(const PrArgs &a, uint32_t v, float sum, double &dsum, double &nsum) {
-    float rn = (float)(a.teleport + a.damping * (double)sum);
-    float ro = a.r_old[v];
-    a.r_new[v] = rn;
-    uint32_t od = a.outdeg[v];
-    a.c_new[v] = od ? rn / (float)od : 0.0f;
-    dsum += fabs((double)rn - (double)ro);
-    nsum += fabs((double)rn);
+constexpr int EDGE_THREADS = 1024;
+constexpr uint32_t HUB_MAX = 49152; /* 192 KB of shared memory */
+
+__global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
+    if (*(volatile const int *)a.done) return;
+    extern __shared__ float s_hub[];
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint64_t pol_stream = policy_evict_first();
+    const uint64_t pol_keep = policy_evict_last();
+    /* hub cache: contribs of the highest out-degree sources (relabelled 0..hub-1) */
+    {
+        const uint32_t n4 = a.hub >> 2;
+        const float4 *src4 = (const float4 *)a.c_old;
+        float4 *dst4 = (float4 *)s_hub;
+        for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
+        for (uint32_t i = (n4 << 2) + threadIdx.x; i < a.hub; i += blockDim.x) s_hub[i] = __ldcg(a.c_old + i);
+        __syncthreads();
+    }
+
+    for (uint32_t ch = gwarp; ch < a.nchunks; ch += nwarps) {
+        const uint64_t e0 = (uint64_t)ch * CH;
+        const uint64_t e = e0 + (uint64_t)EPL * lane;
+        const uint32_t nvalid = e < a.ne ? (uint32_t)((a.ne - e) < EPL ? (a.ne - e) : EPL) : 0u;
+        uint32_t col[EPL];
+        if (nvalid == EPL) {
+            uint4 x = ld_stream_v4(a.col + e, pol_stream);
+            uint4 y = ld_stream_v4(a.col + e + 4, pol_stream);
+            col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
+            col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
+        }
+        const uint32_t flags = nvalid ? (uint32_t)a.heads[e >> 3] : 0u;
+        float val[EPL];
+#pragma unroll
+        for (int j = 0; j < EPL; ++j) {
+            const uint32_t x = col[j];
+            val[j] = (uint32_t)j >= nvalid ? 0.0f : (x < a.hub ? s_hub[x] : ld_keep_f32(a.c_old + x, pol_keep));
+        }
+
+        const uint32_t base = a.chunk_nz[ch];
+        const uint32_t head0 = __shfl_sync(FULL, flags, 0) & 1u;
+        const uint32_t nh_lane = __popc(flags);
+        uint32_t incl = nh_lane;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        const uint32_t H = incl - nh_lane; /* heads in earlier lanes of this chunk */
+        const uint32_t Htot = __shfl_sync(FULL, incl, 31);
+        const uint32_t rowbase = base + (head0 ? 0u : 1u) + H; /* row started by this lane's first head */
+
+        /* in-lane segments: rows that start and end inside this lane are final */
+        float run = 0.0f, pre = 0.0f;
+        uint32_t nh = 0;
+#pragma unroll
+        for (int j = 0; j < EPL; ++j) {
+            if ((uint32_t)j < nvalid) {
+                if ((flags >> j) & 1u) {
+                    if (nh == 0) pre = run;
+                    else a.nzsum[rowbase + nh - 1] = run;
+                    ++nh;
+                    run = 0.0f;
+                }
+                run += val[j];
+            }
+        }
+        /* warp segmented inclusive scan of (lane has a head, lane tail sum) */
+        int finc = nh > 0;
+        float vinc = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int fu = __shfl_up_sync(FULL, finc, o);
+            float vu = __shfl_up_sync(FULL, vinc, o);
+            if (lane >= (uint32_t)o) {
+                if (!finc) vinc = vu + vinc;
+                finc |= fu;
+            }
+        }
+        const float prev = __shfl_up_sync(FULL, vinc, 1);
+        const float carry = lane ? prev : 0.0f;
+        if (nh > 0) {
+            /* the row that ends at this lane's first head */
+            const float s = carry + pre;
+            if (H == 0 && !head0) a.head_part[ch] = s;          /* began in an earlier chunk */
+            else if (!(lane == 0 && head0)) a.nzsum[rowbase - 1] = s; /* began in an earlier lane */
+        }
+        /* the chunk's last row */
+        const uint32_t L = (a.ne - e0 >= (uint64_t)CH) ? 31u : (uint32_t)((a.ne - 1 - e0) / EPL);
+        if (lane == L) {
+            if (Htot == 0) {
+                a.head_part[ch] = vinc; /* the whole chunk lies inside one row */
+            } else {
+                const bool ends_here = (e0 + CH >= a.ne) || (a.heads[(e0 + CH) >> 3] & 1u);
+                const uint32_t idx = base + (head0 ? 0u : 1u) + Htot - 1;
+                if (ends_here) a.nzsum[idx] = vinc;
+                else a.tail_part[ch] = vinc;
+            }
+        }
+    }
 }
 
-__device__ __forceinline__ double2 block_sum2(double a, double b, double2 *s_red) {
+/* Rows that cross chunk boundaries: tail partial of the first chunk plus the
+ * head partials of the later chunks. A warp takes 32 consecutive split rows;
+ * each lane finishes its own row when it spans few chunks, and the warp sums the
+ * partials of each long (hub) row cooperatively: lane-strided partial sums, then
+ * a fixed xor-shuffle tree, so the order is fixed. */
+__global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
+    if (*(volatile const int *)a.done) return;
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; wb < a.nsplit; wb += nwarps * 32u) {
+        const uint32_t k = wb + lane;
+        uint4 sp = make_uint4(0, 0, 0, 0);
+        if (k < a.nsplit) sp = a.split[k];
+        const bool valid = k < a.nsplit;
+        const bool lng = valid && (sp.z - sp.y) > 8u;
+        if (valid && !lng) {
+            float s = a.tail_part[sp.y];
+            for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += a.head_part[c];
+            a.nzsum[sp.x] = s;
+        }
+        uint32_t m = __ballot_sync(FULL, lng);
+        while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t row = __shfl_sync(FULL, sp.x, src);
+            const uint32_t cs = __shfl_sync(FULL, sp.y, src);
+            const uint32_t ce = __shfl_sync(FULL, sp.z, src);
+            float s = 0.0f;
+            for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) s += a.head_part[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+            if (lane == 0) a.nzsum[row] = a.tail_part[cs] + s;
+        }
+    }
+}
+
+/* separate round-to-nearest multiply and add (no FMA contraction), as the
+ * reference computes (float)(teleport + damping * (double)sum) */
+__device__ __forceinline__ float pr_value(const SweepArgs &a, float sum) {
+    return (float)__dadd_rn(a.teleport, __dmul_rn(a.damping, (double)sum));
+}
+
+__device__ __forceinline__ double2 block_sum2(double x, double y, double2 *s_red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xFFFFFFFFu, a, o);
-        b += __shfl_down_sync(0xFFFFFFFFu, b, o);
+        x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+        y += __shfl_down_sync(0xFFFFFFFFu, y, o);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) s_red[warp] = make_double2(a, b);
+    if (lane == 0) s_red[warp] = make_double2(x, y);
     __syncthreads();
     double2 r = make_double2(0.0, 0.0);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0)
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
             r.x += s_red[w].x;
             r.y += s_red[w].y;
         }
-    }
+    __syncthreads();
     return r; /* valid in thread 0 */
 }
 
-__global__ void __launch_bounds__(MP_THREADS) k_pr_sweep(PrArgs a, int sweep) {
-    if (*(volatile int *)a.done) return;
-    __shared__ float s_val[MP_TILE];
-    __shared__ uint32_t s_rowend[MP_TILE];
-    __shared__ float s_rowsum[MP_TILE];
-    __shared__ SegVal s_warp[MP_THREADS / 32];
-    __shared__ double2 s_red[MP_THREADS / 32];
-    const int tid = threadIdx.x;
-    double dsum = 0.0, nsum = 0.0;
-
-    for (uint32_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const uint32_t r0 = a.tile_row[t], r1 = a.tile_row[t + 1];
-        const uint32_t e0 = a.tile_edge[t], e1 = a.tile_edge[t + 1];
-        const uint32_t nrows = r1 - r0, nedges = e1 - e0;
-        for (uint32_t k = tid; k < nrows; k += MP_THREADS) s_rowend[k] = a.rowptr[r0 + k + 1] - e0;
-        for (uint32_t k = tid; k < nedges; k += MP_THREADS) s_val[k] = __ldg(a.c_old + __ldg(a.col + e0 + k));
-        __syncthreads();
-
-        const uint32_t items = nrows + nedges;
-        const uint32_t d0 = min((uint32_t)tid * MP_ITEMS, items);
-        const uint32_t d1 = min(d0 + MP_ITEMS, items);
-        uint32_t ti = mp_search(s_rowend, nrows, nedges, d0);
-        uint32_t tj = d0 - ti;
-        float run = 0.0f, first_part = 0.0f;
-        int first_row = -1;
-        for (uint32_t d = d0; d < d1; ++d) {
-            if (ti < nrows && s_rowend[ti] <= tj) {
-                if (first_row < 0) {
-                    first_row = (int)ti;
-                    first_part = run;
-                } else {
-                    s_rowsum[ti] = run;
-                }
-                run = 0.0f;
-                ++ti;
-            } else {
-                run += s_val[tj];
-                ++tj;
-            }
-        }
-        float tile_tail;
-        float carry = seg_scan_excl(SegVal{first_row >= 0 ? 1 : 0, run}, s_warp, &tile_tail);
-        if (first_row >= 0) s_rowsum[first_row] = carry + first_part;
-        __syncthreads();
-        const bool head_split = a.rowptr[r0] < e0;
-        if (tid == 0) {
-            a.tail_part[t] = tile_tail;
-            if (head_split && nrows > 0) a.head_part[t] = s_rowsum[0];
-        }
-        for (uint32_t k = tid; k < nrows; k += MP_THREADS) {
-            if (k == 0 && head_split) continue;
-            pr_apply(a, r0 + k, s_rowsum[k], dsum, nsum);
-        }
-        __syncthreads();
-    }
-    double2 r = block_sum2(dsum, nsum, s_red);
-    if (tid == 0) a.block_res[blockIdx.x] = r;
-}
-
-__global__ void __launch_bounds__(256) k_pr_fixup(PrArgs a, int sweep) {
-    if (*(volatile int *)a.done) return;
+__global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int const_pass) {
+    if (*(volatile const int *)a.done) return;
     __shared__ double2 s_red[8];
     __shared__ int s_last;
     double dsum = 0.0, nsum = 0.0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntiles; t += gridDim.x * blockDim.x) {
-        uint32_t ts = a.fix_start[t];
-        if (ts == 0xFFFFFFFFu) continue;
-        float sum = a.tail_part[ts];
-        for (uint32_t k = ts + 1; k < t; ++k) sum += a.tail_part[k];
-        sum += a.head_part[t];
-        pr_apply(a, a.tile_row[t], sum, dsum, nsum);
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i < a.nnz; i += nth) {
+        const float rn = pr_value(a, a.nzsum[i]);
+        const float ro = a.r_nz_old[i];
+        const uint32_t od = a.od_nz[i];
+        a.r_nz_new[i] = rn;
+        a.c_new[a.nz_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
+        dsum += fabs((double)rn - (double)ro);
+        nsum += fabs((double)rn);
+    }
+    if (const_pass) {
+        /* vertices without in-edges: value teleport from the first sweep on;
+         * written once into each contrib buffer (sweeps 0 and 1) */
+        const float rn = pr_value(a, 0.0f);
+        for (uint32_t i = tid; i < a.nzero; i += nth) {
+            const uint32_t v = a.zero_rows[i];
+            const float ro = sweep == 0 ? a.r_init[v] : rn;
+            const uint32_t od = a.outdeg[v];
+            a.c_new[a.zero_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
+            dsum += fabs((double)rn - (double)ro);
+            nsum += fabs((double)rn);
+        }
     }
     double2 r = block_sum2(dsum, nsum, s_red);
     if (threadIdx.x == 0) {
-        a.fix_res[blockIdx.x] = r;
+        a.block_res[blockIdx.x] = r;
         __threadfence();
-        unsigned prev = atomicAdd(a.ticket, 1u);
-        s_last = (prev == gridDim.x - 1);
+        s_last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    /* last block: fixed-order reduction of all partials */
     double x = 0.0, y = 0.0;
-    for (uint32_t i = threadIdx.x; i < a.nblock_res; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
         double2 p = __ldcg(a.block_res + i);
         x += p.x;
         y += p.y;
     }
-    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
-        double2 p = __ldcg(a.fix_res + i);
-        x += p.x;
-        y += p.y;
-    }
-    __syncthreads();
     double2 tot = block_sum2(x, y, s_red);
     if (threadIdx.x == 0) {
-        double res = tot.y > 0.0 ? tot.x / tot.y : 0.0;
+        const double norm = tot.y + (const_pass ? 0.0 : a.norm_const);
+        const double res = norm > 0.0 ? tot.x / norm : 0.0;
         a.res_log[sweep] = res;
         *a.last_res = res;
         *a.sweeps_done = sweep + 1;
@@ -214,76 +373,226 @@ __global__ void __launch_bounds__(256) k_pr_fixup(PrArgs a, int sweep) {
     }
 }
 
-__global__ void k_pr_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float init, const float *__restrict__ init_rank,
-                          float *__restrict__ r, float *__restrict__ c) {
+/* r = initial vector (original ids); c = contribs at relabelled ids */
+__global__ void k_pr_init(uint32_t nv, const uint32_t *__restrict__ outdeg, const uint32_t *__restrict__ newid,
+                          float init, const float *__restrict__ init_rank, float *__restrict__ r, float *__restrict__ c) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         float x = init_rank ? init_rank[v] : init;
         r[v] = x;
         uint32_t od = outdeg[v];
-        c[v] = od ? x / (float)od : 0.0f;
+        c[newid[v]] = od ? __fdiv_rn(x, (float)od) : 0.0f;
     }
+}
+
+/* relabelling by out-degree (descending, ties by id): keys sort ascending */
+__global__ void k_outdeg_keys(const uint32_t *__restrict__ outdeg, uint32_t nv, uint32_t maxdeg, uint32_t vbits,
+                              uint64_t *__restrict__ keys) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        keys[v] = ((uint64_t)(maxdeg - outdeg[v]) << vbits) | v;
+}
+
+__global__ void k_newid(const uint64_t *__restrict__ sorted, uint32_t nv, uint32_t vbits, uint32_t *__restrict__ newid) {
+    const uint64_t mask = (1ull << vbits) - 1ull;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        newid[(uint32_t)(sorted[i] & mask)] = i;
+}
+
+__global__ void k_relabel(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
+                          uint32_t *__restrict__ col_r) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x)
+        col_r[e] = newid[col[e]];
+}
+
+__global__ void k_max_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t *out) {
+    uint32_t m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, a[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+/* compact state of the vertices with in-edges */
+__global__ void k_pr_init_nz(uint32_t nnz, const uint32_t *__restrict__ nz_rows, const float *__restrict__ r,
+                             float *__restrict__ r_nz) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x)
+        r_nz[i] = r[nz_rows[i]];
+}
+
+/* assemble the full rank vector after the last sweep */
+__global__ void k_pr_scatter(uint32_t nnz, uint32_t nzero, const uint32_t *__restrict__ nz_rows,
+                             const uint32_t *__restrict__ zero_rows, const float *__restrict__ r_nz, float t,
+                             float *__restrict__ r) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i < nnz; i += nth) r[nz_rows[i]] = r_nz[i];
+    for (uint32_t i = tid; i < nzero; i += nth) r[zero_rows[i]] = t;
+}
+
+__global__ void k_gather_u32(uint32_t n, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ src,
+                             uint32_t *__restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
+inline unsigned grid1d(uint64_t n, uint64_t cap_per_sm = 16) {
+    uint64_t b = (n + 255) / 256;
+    uint64_t cap = (uint64_t)num_sms() * cap_per_sm;
+    return (unsigned)std::max<uint64_t>(1, std::min(b, cap));
 }
 
 }  // namespace
 
-int ensure_plan(gcg_graph *g) {
-    if (g->plan) return GCG_OK;
-    PrPlan *p = new PrPlan();
-    const uint64_t total = (uint64_t)g->nv + g->ne;
-    p->ntiles = (uint32_t)((total + MP_TILE - 1) / MP_TILE);
-    if (p->tile_row.alloc((size_t)p->ntiles + 1) || p->tile_edge.alloc((size_t)p->ntiles + 1) ||
-        p->fix_start.alloc((size_t)p->ntiles + 1)) {
-        delete p;
-        return GCG_ERR_NOMEM;
+/* ---- the chunk plan: built once per graph -------------------------------- */
+/* Sweep workspace of one graph, reused across calls. */
+struct PrWork {
+    dbuf<float> r, c, nzsum, parts, rnz;
+    dbuf<double2> bres;
+    dbuf<uint32_t> ctl;
+    dbuf<double> dres;
+    int *h_flags = nullptr; /* pinned: done flags copied back per chunk of sweeps */
+    ~PrWork() {
+        if (h_flags) cudaFreeHost(h_flags);
     }
-    unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)p->ntiles + 256) / 256, 4096));
-    k_plan<<<blocks, 256, 0, g->stream>>>(g->in_rowptr.get(), g->nv, g->ne, p->ntiles, p->tile_row.get(),
-                                          p->tile_edge.get());
-    k_plan_fix<<<blocks, 256, 0, g->stream>>>(g->in_rowptr.get(), p->ntiles, p->tile_row.get(), p->tile_edge.get(),
-                                              p->fix_start.get());
+};
+
+struct ChunkPlan {
+    PrWork work;
+    uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
+    dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
+    dbuf<uint4> split;
+    /* sources relabelled by out-degree (descending): col_r = newid[col] */
+    uint32_t hub = 0;
+    dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
+};
+
+void free_chunk_plan(ChunkPlan *p) { delete p; }
+
+static int ensure_chunk_plan(gcg_graph *g) {
+    if (g->cplan) return GCG_OK;
+    cudaStream_t s = g->stream;
+    const uint32_t nv = g->nv;
+    const uint64_t ne = g->ne;
+    ChunkPlan *p = new ChunkPlan();
+    auto bail = [&](int st) {
+        delete p;
+        return st;
+    };
+    p->nchunks = (uint32_t)((ne + CH - 1) / CH);
+    tbuf<uint32_t> flags, pos, nz_start, total;
+    if (flags.alloc(std::max<uint64_t>(nv, 1), s) || pos.alloc(std::max<uint64_t>(nv, 1), s) ||
+        total.alloc(1, s) || nz_start.alloc(std::max<uint64_t>(nv, 1), s))
+        return bail(GCG_ERR_NOMEM);
+    k_nonzero_flags<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, flags.get());
+    int st = scan_u32(flags.get(), pos.get(), nv, total.get(), s);
+    if (st) return bail(st);
+    uint32_t nnz = 0;
+    if (cudaMemcpyAsync(&nnz, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
+    p->nnz = nnz;
+    p->nzero = nv - nnz;
+    /* head bitmap covers whole chunks plus one spare word (read of the next chunk's first bit) */
+    const uint64_t words = ((uint64_t)p->nchunks * CH) / 32 + 8;
+    if (p->nz_rows.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_rows.alloc(std::max<uint32_t>(p->nzero, 1)) ||
+        p->od_nz.alloc(std::max<uint32_t>(nnz, 1)) ||
+        p->head_bits.alloc(words) || p->chunk_nz.alloc(std::max<uint32_t>(p->nchunks, 1)))
+        return bail(GCG_ERR_NOMEM);
+    k_split_rows<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, pos.get(), p->nz_rows.get(), nz_start.get(),
+                                            p->zero_rows.get());
+    cudaMemsetAsync(p->head_bits.get(), 0, words * 4, s);
+    if (nnz) {
+        k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), g->outdeg.get(), p->od_nz.get());
+        k_head_bits<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, p->head_bits.get());
+        k_chunk_nz<<<grid1d(p->nchunks), 256, 0, s>>>(nz_start.get(), nnz, p->nchunks, p->chunk_nz.get());
+        k_split_flags<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, ne, flags.get());
+        if ((st = scan_u32(flags.get(), pos.get(), nnz, total.get(), s))) return bail(st);
+        uint32_t nsplit = 0;
+        if (cudaMemcpyAsync(&nsplit, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
+        p->nsplit = nsplit;
+        if (p->split.alloc(std::max<uint32_t>(nsplit, 1))) return bail(GCG_ERR_NOMEM);
+        k_split_list<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, ne, pos.get(), p->split.get());
+    }
+    /* relabel sources by out-degree so the hottest contribs sit at ids [0, hub) */
+    {
+        tbuf<uint32_t> dmax;
+        tbuf<uint64_t> keys, tmp;
+        if (dmax.alloc(1, s) || keys.alloc(std::max<uint32_t>(nv, 1), s) || tmp.alloc(std::max<uint32_t>(nv, 1), s) ||
+            p->newid.alloc(std::max<uint32_t>(nv, 1)) || p->col_r.alloc(std::max<uint64_t>(ne, 1)) ||
+            p->nz_cidx.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_cidx.alloc(std::max<uint32_t>(p->nzero, 1)))
+            return bail(GCG_ERR_NOMEM);
+        cudaMemsetAsync(dmax.get(), 0, 4, s);
+        k_max_u32<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, dmax.get());
+        uint32_t maxdeg = 0;
+        if (cudaMemcpyAsync(&maxdeg, dmax.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
+        uint32_t dbits = 1;
+        while (dbits < 32 && (1ull << dbits) <= maxdeg) ++dbits;
+        k_outdeg_keys<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, maxdeg, g->vbits, keys.get());
+        uint64_t *sorted = nullptr;
+        if ((st = radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + dbits), &sorted, s)))
+            return bail(st);
+        k_newid<<<grid1d(nv), 256, 0, s>>>(sorted, nv, g->vbits, p->newid.get());
+        if (ne) k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, p->newid.get(), p->col_r.get());
+        if (nnz) k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), p->newid.get(), p->nz_cidx.get());
+        if (p->nzero)
+            k_gather_u32<<<grid1d(p->nzero), 256, 0, s>>>(p->nzero, p->zero_rows.get(), p->newid.get(),
+                                                         p->zero_cidx.get());
+        p->hub = std::min<uint32_t>(nv, HUB_MAX);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(GCG_ERR_CUDA, "chunk plan: relabel"));
+    }
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        delete p;
-        return fail(GCG_ERR_CUDA, std::string("merge-path plan: ") + cudaGetErrorString(e));
-    }
-    g->plan = p;
+    if (e != cudaSuccess) return bail(fail(GCG_ERR_CUDA, std::string("chunk plan: ") + cudaGetErrorString(e)));
+    g->cplan = p;
     return GCG_OK;
 }
 
-static int sweep_grid(uint32_t ntiles) {
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_sweep, MP_THREADS, 0) != cudaSuccess ||
-            per_sm <= 0) {
-            cudaGetLastError();
-            per_sm = 4;
-        }
+/* one CTA of EDGE_THREADS per SM (the hub cache takes most of shared memory) */
+static int edge_grid(uint32_t hub_bytes) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_pr_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
+        attr = true;
     }
-    int g = num_sms() * per_sm;
-    if ((uint32_t)g > ntiles) g = (int)std::max<uint32_t>(ntiles, 1);
-    return g;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_edges, EDGE_THREADS, hub_bytes) != cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return num_sms() * per_sm;
 }
 
 static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats) {
-    GCG_TRY(ensure_plan(g));
+    GCG_TRY(ensure_chunk_plan(g));
     cudaStream_t s = g->stream;
-    const PrPlan &pl = *g->plan;
+    const ChunkPlan &pl = *g->cplan;
     const uint32_t nv = g->nv;
     const int max_sweeps = p->max_sweeps;
 
-    tbuf<float> r, c, parts;
-    tbuf<double2> bres, fres;
-    tbuf<uint32_t> ctl;   /* ticket, done, sweeps_done */
-    tbuf<double> dres;    /* res_log[max_sweeps] + last_res */
-    const int g1 = sweep_grid(pl.ntiles);
-    const int g2 = (int)std::max<uint32_t>(1, std::min<uint32_t>((pl.ntiles + 255) / 256, (uint32_t)num_sms() * 4));
-    GCG_TRY(r.alloc((size_t)2 * nv, s));
-    GCG_TRY(c.alloc((size_t)2 * nv, s));
-    GCG_TRY(parts.alloc((size_t)2 * pl.ntiles + 2, s));
-    GCG_TRY(bres.alloc(g1, s));
-    GCG_TRY(fres.alloc(g2, s));
-    GCG_TRY(ctl.alloc(4, s));
-    GCG_TRY(dres.alloc((size_t)max_sweeps + 1, s));
+    const uint32_t hub_bytes = pl.hub * 4u;
+    const int ge = std::max(1, std::min<int>(edge_grid(hub_bytes), (int)((pl.nchunks + 31) / 32)));
+    const int gv = (int)grid1d(std::max<uint64_t>(pl.nnz, pl.nzero), 8);
+    /* the sweep workspace lives with the graph: allocated on the first call,
+     * reused by later calls (no allocation on the repeated-solve path) */
+    PrWork &w = g->cplan->work;
+    /* each contrib buffer starts on a 256-byte boundary (vector loads of the hub) */
+    const size_t cstride = ((size_t)nv + 63) & ~(size_t)63;
+    if (!w.r.get()) {
+        GCG_TRY(w.r.alloc((size_t)nv));
+        GCG_TRY(w.rnz.alloc((size_t)2 * std::max<uint32_t>(pl.nnz, 1)));
+        GCG_TRY(w.c.alloc((size_t)2 * cstride));
+        GCG_TRY(w.nzsum.alloc(std::max<uint32_t>(pl.nnz, 1)));
+        GCG_TRY(w.parts.alloc((size_t)2 * pl.nchunks + 2));
+        GCG_TRY(w.bres.alloc(gv));
+        GCG_TRY(w.ctl.alloc(4));
+        GCG_CUDA(cudaMallocHost((void **)&w.h_flags, 64 * sizeof(int)));
+    }
+    if (w.dres.n < (size_t)max_sweeps + 1) GCG_TRY(w.dres.alloc((size_t)max_sweeps + 1));
+    dbuf<float> &r = w.r, &c = w.c, &nzsum = w.nzsum, &parts = w.parts, &rnz = w.rnz;
+    dbuf<double2> &bres = w.bres;
+    dbuf<uint32_t> &ctl = w.ctl; /* ticket, done, sweeps_done */
+    dbuf<double> &dres = w.dres; /* res_log[max_sweeps] + last_res */
     GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 4 * sizeof(uint32_t), s));
     GCG_CUDA(cudaMemsetAsync(dres.get(), 0, ((size_t)max_sweeps + 1) * sizeof(double), s));
 
@@ -299,24 +608,32 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
             init_dev = init_stage.get();
         }
     }
-    unsigned vb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, (uint64_t)num_sms() * 8));
-    k_pr_init<<<vb, 256, 0, s>>>(nv, g->outdeg.get(), p->init, init_dev, r.get(), c.get());
+    k_pr_init<<<grid1d(nv, 8), 256, 0, s>>>(nv, g->outdeg.get(), pl.newid.get(), p->init, init_dev, r.get(), c.get());
+    k_pr_init_nz<<<grid1d(pl.nnz, 8), 256, 0, s>>>(pl.nnz, pl.nz_rows.get(), r.get(), rnz.get());
     GCG_LAUNCH_CHECK();
 
-    PrArgs a;
-    a.rowptr = g->in_rowptr.get();
-    a.col = g->in_col.get();
+    SweepArgs a;
+    a.col = pl.col_r.get();
+    a.hub = pl.hub;
+    a.nz_cidx = pl.nz_cidx.get();
+    a.zero_cidx = pl.zero_cidx.get();
     a.outdeg = g->outdeg.get();
-    a.tile_row = pl.tile_row.get();
-    a.tile_edge = pl.tile_edge.get();
-    a.fix_start = pl.fix_start.get();
-    a.ntiles = pl.ntiles;
-    a.nv = nv;
+    a.heads = (const uint8_t *)pl.head_bits.get();
+    a.chunk_nz = pl.chunk_nz.get();
+    a.nz_rows = pl.nz_rows.get();
+    a.zero_rows = pl.zero_rows.get();
+    a.split = pl.split.get();
+    a.ne = g->ne;
+    a.nchunks = pl.nchunks;
+    a.nnz = pl.nnz;
+    a.nzero = pl.nzero;
+    a.nsplit = pl.nsplit;
+    a.od_nz = pl.od_nz.get();
+    a.r_init = r.get();
+    a.nzsum = nzsum.get();
     a.head_part = parts.get();
-    a.tail_part = parts.get() + pl.ntiles + 1;
+    a.tail_part = parts.get() + pl.nchunks + 1;
     a.block_res = bres.get();
-    a.nblock_res = (uint32_t)g1;
-    a.fix_res = fres.get();
     a.ticket = ctl.get();
     a.done = (int *)(ctl.get() + 1);
     a.sweeps_done = (int *)(ctl.get() + 2);
@@ -325,20 +642,22 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     a.teleport = p->teleport;
     a.damping = p->damping;
     a.tol = p->tol;
+    /* |r'| of the constant vertices, added to the norm once they are no longer visited */
+    a.norm_const = (double)pl.nzero * fabs((double)(float)p->teleport);
+    const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 4);
 
     cudaEvent_t ev0, ev1;
     GCG_CUDA(cudaEventCreate(&ev0));
     GCG_CUDA(cudaEventCreate(&ev1));
     GCG_CUDA(cudaEventRecord(ev0, s));
     const bool time_sweeps = (p->flags & GCG_PR_TIME_SWEEPS) != 0;
-    std::vector<cudaEvent_t> sweep_ev; /* pairs around each main sweep kernel */
+    std::vector<cudaEvent_t> sweep_ev; /* pairs around each edge kernel */
 
     /* Sweeps are queued in chunks; after each chunk the done flag is copied to
      * pinned memory. The host waits on the chunk before last, so the GPU always
      * has work queued; sweeps queued past convergence return immediately. */
     const int CHUNK = 4;
-    int *h_flags = nullptr;
-    GCG_CUDA(cudaMallocHost((void **)&h_flags, 64 * sizeof(int)));
+    int *h_flags = w.h_flags;
     std::vector<cudaEvent_t> chunk_ev;
     int launched = 0, stop = 0;
     int status = GCG_OK;
@@ -346,23 +665,24 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         int n = std::min(CHUNK, max_sweeps - launched);
         for (int k = 0; k < n; ++k) {
             const int sw = launched + k;
-            a.r_old = r.get() + (size_t)(sw & 1) * nv;
-            a.c_old = c.get() + (size_t)(sw & 1) * nv;
-            a.r_new = r.get() + (size_t)((sw + 1) & 1) * nv;
-            a.c_new = c.get() + (size_t)((sw + 1) & 1) * nv;
+            a.c_old = c.get() + (size_t)(sw & 1) * cstride;
+            a.c_new = c.get() + (size_t)((sw + 1) & 1) * cstride;
+            a.r_nz_old = rnz.get() + (size_t)(sw & 1) * pl.nnz;
+            a.r_nz_new = rnz.get() + (size_t)((sw + 1) & 1) * pl.nnz;
             if (time_sweeps) {
                 cudaEvent_t e0, e1;
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, s);
-                k_pr_sweep<<<g1, MP_THREADS, 0, s>>>(a, sw);
+                k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
                 cudaEventRecord(e1, s);
                 sweep_ev.push_back(e0);
                 sweep_ev.push_back(e1);
             } else {
-                k_pr_sweep<<<g1, MP_THREADS, 0, s>>>(a, sw);
+                k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
             }
-            k_pr_fixup<<<g2, 256, 0, s>>>(a, sw);
+            k_pr_fix<<<fg, 256, 0, s>>>(a);
+            k_pr_vertex<<<gv, 256, 0, s>>>(a, sw, sw < 2 ? 1 : 0);
         }
         launched += n;
         if (cudaGetLastError() != cudaSuccess) {
@@ -387,7 +707,6 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     GCG_CUDA(cudaEventRecord(ev1, s));
     GCG_CUDA(cudaEventSynchronize(ev1));
     for (auto e : chunk_ev) cudaEventDestroy(e);
-    cudaFreeHost(h_flags);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
@@ -416,8 +735,13 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     double last_res = 0.0;
     GCG_CUDA(cudaMemcpy(&last_res, a.last_res, sizeof(double), cudaMemcpyDeviceToHost));
     if (p->residuals && sweeps > 0) GCG_TRY(copy_out(p->residuals, dres.get(), (size_t)sweeps * sizeof(double), s));
-    const float *result = r.get() + (size_t)(sweeps & 1) * nv;
-    if (out_rank) GCG_TRY(copy_out(out_rank, result, (size_t)nv * sizeof(float), s));
+    if (sweeps > 0) {
+        const float t = (float)p->teleport; /* teleport + damping * 0 */
+        k_pr_scatter<<<grid1d(nv, 8), 256, 0, s>>>(pl.nnz, pl.nzero, pl.nz_rows.get(), pl.zero_rows.get(),
+                                                  rnz.get() + (size_t)(sweeps & 1) * pl.nnz, t, r.get());
+        GCG_LAUNCH_CHECK();
+    }
+    if (out_rank) GCG_TRY(copy_out(out_rank, r.get(), (size_t)nv * sizeof(float), s));
     GCG_CUDA(cudaStreamSynchronize(s));
     if (stats) {
         stats->sweeps = sweeps;
@@ -426,7 +750,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         stats->device_ms = ms;
         stats->sweep_kernel_ms = sweep_ms;
         stats->timed_sweeps = timed;
-        stats->kernel_launches = 1 + 2 * launched;
+        stats->kernel_launches = 1 + 3 * launched;
     }
     return GCG_OK;
 }

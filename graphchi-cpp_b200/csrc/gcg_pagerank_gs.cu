@@ -70,7 +70,7 @@ __global__ void k_max_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t *
 __global__ void k_gs_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float reset, float *pr) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         uint32_t oc = outdeg[v];
-        pr[v] = oc > 0 ? 1.0f / (float)oc : reset;
+        pr[v] = oc > 0 ? __fdiv_rn(1.0f, (float)oc) : reset;
     }
 }
 
@@ -87,11 +87,11 @@ __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, u
             const uint32_t u = __ldg(col + j);
             sum += (u < v) ? ((volatile const float *)pr_new)[u] : __ldg(pr_old + u);
         }
+        /* explicit round-to-nearest ops: no FMA contraction, the same rounding as
+         * the reference's separate double multiply and add */
         const int outc = (int)outdeg[v];
-        if (outc > 0)
-            pr_new[v] = (float)((reset + damping * (double)sum) / (double)outc);
-        else
-            pr_new[v] = (float)(reset + damping * (double)sum);
+        const double t = __dadd_rn(reset, __dmul_rn(damping, (double)sum));
+        pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
     }
 }
 
@@ -99,7 +99,7 @@ __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, u
 __global__ void k_gs_final(uint32_t nv, const uint32_t *__restrict__ outdeg, const float *__restrict__ pr, float *out) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         uint32_t oc = outdeg[v];
-        out[v] = oc > 0 ? pr[v] * (float)oc : pr[v];
+        out[v] = oc > 0 ? __fmul_rn(pr[v], (float)oc) : pr[v];
     }
 }
 
