@@ -49,13 +49,13 @@ def load_peaks():
 
 
 def load_traffic_per_edge():
-    """DRAM bytes per edge and per vertex of one k_pr_edges launch, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "pagerank_sweep_rmat.md")
+    """DRAM bytes per edge of one k_pr_edges launch at scale 24, from the committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one launch / E)."""
+    path = os.path.join(ROOT, "profiles", "pagerank_edges_rmat24_traffic.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_edge_and_vertex:"):
-                a, b = line.split(":", 1)[1].split()
-                return float(a), float(b)
+            if line.startswith("dram_bytes_per_edge:"):
+                return float(line.split(":", 1)[1].split()[0])
     except Exception:
         pass
     return None
@@ -227,7 +227,7 @@ def run_ours(args, rank, world):
     achieved = alg_bytes / per_launch_s / 1e9
     peak, peak_kind = load_peaks()
     tr = load_traffic_per_edge()
-    traffic = (tr[0] * E + tr[1] * V) if tr else None
+    traffic = tr * E if (tr and args.scale == 24) else None
 
     # ---- e2e: host buffers through the C ABI ----
     hs = torch.empty(m, dtype=torch.int32, pin_memory=True)
@@ -247,12 +247,12 @@ def run_ours(args, rank, world):
         if i >= args.e2e_warmup:
             e2e_times.append(dt)
             e2e_edges += E * st.sweeps
-    e2e_s = sum(e2e_times)
+    e2e_s = sum(e2e_times) if e2e_times else float("nan")
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = e2e_edges * world / e2e_s / 1e9
+    e2e_value = e2e_edges * world / e2e_s / 1e9 if e2e_times else None
 
     # ---- CPU baseline: the reference's own PageRank on a bounded sample ----
     cpu = None

@@ -149,6 +149,25 @@ struct SweepArgs {
     double teleport, damping, tol, norm_const;
 };
 
+/* columns (streamed), head flags and starting row index of one chunk */
+template <typename A>
+__device__ __forceinline__ void load_chunk(const A &a, uint32_t ch, uint32_t lane, uint64_t pol, uint32_t (&col)[EPL],
+                                           uint32_t &flags, uint32_t &nvalid, uint32_t &base) {
+    const uint64_t e = (uint64_t)ch * CH + (uint64_t)EPL * lane;
+    nvalid = e < a.ne ? (uint32_t)((a.ne - e) < EPL ? (a.ne - e) : EPL) : 0u;
+    if (nvalid == EPL) {
+        uint4 x = ld_stream_v4(a.col + e, pol);
+        uint4 y = ld_stream_v4(a.col + e + 4, pol);
+        col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
+        col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
+    }
+    flags = nvalid ? (uint32_t)a.heads[e >> 3] : 0u;
+    base = a.chunk_nz[ch];
+}
+
 constexpr int EDGE_THREADS = 1024;
 constexpr uint32_t HUB_MAX = 49152; /* 192 KB of shared memory */
 
@@ -171,29 +190,23 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
         __syncthreads();
     }
 
-    for (uint32_t ch = gwarp; ch < a.nchunks; ch += nwarps) {
+    /* Software pipeline: while a chunk's gathers are in flight, the next chunk's
+     * columns, head flags and row base are already being loaded. */
+    uint32_t ch = gwarp;
+    uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
+    if (ch < a.nchunks) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base);
+    for (; ch < a.nchunks; ch += nwarps) {
         const uint64_t e0 = (uint64_t)ch * CH;
-        const uint64_t e = e0 + (uint64_t)EPL * lane;
-        const uint32_t nvalid = e < a.ne ? (uint32_t)((a.ne - e) < EPL ? (a.ne - e) : EPL) : 0u;
-        uint32_t col[EPL];
-        if (nvalid == EPL) {
-            uint4 x = ld_stream_v4(a.col + e, pol_stream);
-            uint4 y = ld_stream_v4(a.col + e + 4, pol_stream);
-            col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
-            col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
-        } else {
-#pragma unroll
-            for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
-        }
-        const uint32_t flags = nvalid ? (uint32_t)a.heads[e >> 3] : 0u;
         float val[EPL];
 #pragma unroll
         for (int j = 0; j < EPL; ++j) {
             const uint32_t x = col[j];
             val[j] = (uint32_t)j >= nvalid ? 0.0f : (x < a.hub ? s_hub[x] : ld_keep_f32(a.c_old + x, pol_keep));
         }
-
-        const uint32_t base = a.chunk_nz[ch];
+        const uint32_t cur_flags = flags, cur_nvalid = nvalid, cur_base = base;
+        if (ch + nwarps < a.nchunks) load_chunk(a, ch + nwarps, lane, pol_stream, col, flags, nvalid, base);
+        {
+        const uint32_t flags = cur_flags, nvalid = cur_nvalid, base = cur_base;
         const uint32_t head0 = __shfl_sync(FULL, flags, 0) & 1u;
         const uint32_t nh_lane = __popc(flags);
         uint32_t incl = nh_lane;
@@ -252,6 +265,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
                 if (ends_here) a.nzsum[idx] = vinc;
                 else a.tail_part[ch] = vinc;
             }
+        }
         }
     }
 }
