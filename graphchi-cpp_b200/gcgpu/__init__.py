@@ -45,7 +45,9 @@ EXPORTED = [
     "gcg_graph_degrees", "gcg_graph_csr", "gcg_graph_write_metadata", "gcg_write_vout",
     "gcg_pr_params_default", "gcg_pagerank", "gcg_connected_components", "gcg_triangle_count",
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
+    "gcg_pagerank_csr_noalloc",
 ]
+NOALLOC_MAX_VERTICES = 1 << 20
 
 
 class GcgError(RuntimeError):
@@ -105,6 +107,8 @@ _cc = _sig("gcg_connected_components", _i, _vp, _vp, C.POINTER(CcStats))
 _tc = _sig("gcg_triangle_count", _i, _vp, _vp, _vp, _vp, C.POINTER(TcStats))
 _gen_rmat = _sig("gcg_generate_rmat", _i, _u32, _u64, C.c_double, C.c_double, C.c_double, _u64, _vp, _vp)
 _gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
+_pr_noalloc = _sig("gcg_pagerank_csr_noalloc", _i, _vp, _vp, _vp, _u32, C.POINTER(PrParams), _vp, _vp,
+                   C.POINTER(PrStats))
 _last_error = _sig("gcg_last_error", C.c_char_p)
 _version = _sig("gcg_version", C.c_char_p)
 
@@ -293,3 +297,18 @@ def write_vout(base, values):
     elem = values.dtype.itemsize if isinstance(values, np.ndarray) else values.element_size()
     n = values.shape[0]
     check(_write_vout(os.fsencode(base), ptr(values), n, elem))
+
+
+def pagerank_csr_noalloc(in_rowptr, in_col, outdeg, out, num_vertices=None, max_sweeps=3, teleport=0.15,
+                         damping=0.85, tol=0.0, init=1.0, stream=0):
+    """gcg_pagerank_csr_noalloc: Jacobi PageRank over a CSR already in device
+    memory (CUDA tensors), with no device allocation by the library.
+    Returns PrStats; the ranks are written into ``out``."""
+    n = int(out.shape[0]) if num_vertices is None else int(num_vertices)
+    p = PrParams()
+    _pr_default(C.byref(p))
+    p.mode, p.max_sweeps, p.teleport, p.damping, p.tol, p.init = (PR_JACOBI, max_sweeps, teleport, damping, tol,
+                                                                  init)
+    st = PrStats()
+    check(_pr_noalloc(ptr(in_rowptr), ptr(in_col), ptr(outdeg), n, C.byref(p), ptr(out), stream, C.byref(st)))
+    return st

@@ -155,6 +155,23 @@ void gcg_pr_params_default(gcg_pr_params *p);
  * out_rank: num_vertices floats, host or device. stats may be NULL. */
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats);
 
+/* No counterpart in the reference. PageRank (GCG_PR_JACOBI only) over an in-edge
+ * CSR the caller already keeps in device memory, for callers that cannot let a
+ * library allocate device memory (a host framework whose own allocator owns the
+ * GPU, or a loop that must not incur cudaMalloc/cudaFree synchronisation). It
+ * allocates nothing: in_rowptr (num_vertices+1), in_col, outdeg (num_vertices),
+ * out_rank (num_vertices) and the optional params->init_rank / residuals must all
+ * be device memory, or the call fails. Its scratch is a fixed static device
+ * array sized for GCG_NOALLOC_MAX_VERTICES vertices (about 12.6 MB, held by every
+ * GPU that loads the library); larger graphs are rejected with
+ * GCG_ERR_UNSUPPORTED. The first call on a device looks up that array's address;
+ * make it before any stream capture. All calls share the array: calls that
+ * overlap on the GPU race. stream: a cudaStream_t (NULL = legacy default). */
+#define GCG_NOALLOC_MAX_VERTICES (1u << 20)
+int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_t *in_col, const uint32_t *outdeg,
+                             uint32_t num_vertices, const gcg_pr_params *params, float *out_rank,
+                             void *stream, gcg_pr_stats *stats);
+
 /* ---- connected components ---------------------------------------------- */
 
 typedef struct {
