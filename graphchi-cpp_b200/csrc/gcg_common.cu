@@ -134,6 +134,7 @@ static void host_parallel_for(uint64_t m, F f) {
 gcg_graph::~gcg_graph() {
     delete plan;
     gcg::free_chunk_plan(cplan);
+    gcg::free_ppr_plan(pplan);
     free(intervals_host);
 }
 

@@ -116,6 +116,8 @@ int num_sms();
 struct PrPlan;
 struct ChunkPlan;
 void free_chunk_plan(ChunkPlan *p);
+struct PprPlan;
+void free_ppr_plan(PprPlan *p);
 
 }  // namespace gcg
 
@@ -139,6 +141,8 @@ struct gcg_graph {
     gcg::PrPlan *plan = nullptr;
     /* 256-edge chunk plan of the in-CSR (PageRank), built on first use */
     gcg::ChunkPlan *cplan = nullptr;
+    /* row segments for batched personalised PageRank, built on first use */
+    gcg::PprPlan *pplan = nullptr;
 
     ~gcg_graph();
 };

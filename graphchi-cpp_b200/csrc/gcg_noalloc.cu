@@ -153,8 +153,8 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
         return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank_csr_noalloc: " + std::to_string(num_vertices) +
                                              " vertices exceed the fixed scratch limit of " +
                                              std::to_string(NA_MAXV) + " (GCG_NOALLOC_MAX_VERTICES)");
-    if (params->mode != GCG_PR_JACOBI)
-        return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank_csr_noalloc: only GCG_PR_JACOBI is available");
+    if (params->mode != GCG_PR_JACOBI || params->source != GCG_NO_SOURCE)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank_csr_noalloc: only plain GCG_PR_JACOBI is available");
     if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_pagerank_csr_noalloc: max_sweeps < 0");
     if (!is_device_ptr(in_rowptr) || !is_device_ptr(in_col) || !is_device_ptr(outdeg) || !is_device_ptr(out_rank) ||
         (params->init_rank && !is_device_ptr(params->init_rank)) ||

@@ -147,6 +147,7 @@ struct SweepArgs {
     int *done, *sweeps_done;
     double *res_log, *last_res;
     double teleport, damping, tol, norm_const;
+    uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
 };
 
 /* columns (streamed), head flags and starting row index of one chunk */
@@ -312,6 +313,11 @@ __global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
 __device__ __forceinline__ float pr_value(const SweepArgs &a, float sum) {
     return (float)__dadd_rn(a.teleport, __dmul_rn(a.damping, (double)sum));
 }
+/* personalised: the teleport term only at the source vertex */
+__device__ __forceinline__ float pr_value_at(const SweepArgs &a, float sum, uint32_t v) {
+    const double tele = (a.source == GCG_NO_SOURCE || v == a.source) ? a.teleport : 0.0;
+    return (float)__dadd_rn(tele, __dmul_rn(a.damping, (double)sum));
+}
 
 __device__ __forceinline__ double2 block_sum2(double x, double y, double2 *s_red) {
 #pragma unroll
@@ -339,7 +345,8 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
     double dsum = 0.0, nsum = 0.0;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < a.nnz; i += nth) {
-        const float rn = pr_value(a, a.nzsum[i]);
+        const float rn = a.source == GCG_NO_SOURCE ? pr_value(a, a.nzsum[i])
+                                                   : pr_value_at(a, a.nzsum[i], a.nz_rows[i]);
         const float ro = a.r_nz_old[i];
         const uint32_t od = a.od_nz[i];
         a.r_nz_new[i] = rn;
@@ -350,9 +357,9 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
     if (const_pass) {
         /* vertices without in-edges: value teleport from the first sweep on;
          * written once into each contrib buffer (sweeps 0 and 1) */
-        const float rn = pr_value(a, 0.0f);
         for (uint32_t i = tid; i < a.nzero; i += nth) {
             const uint32_t v = a.zero_rows[i];
+            const float rn = pr_value_at(a, 0.0f, v);
             const float ro = sweep == 0 ? a.r_init[v] : rn;
             const uint32_t od = a.outdeg[v];
             a.c_new[a.zero_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
@@ -389,9 +396,11 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
 
 /* r = initial vector (original ids); c = contribs at relabelled ids */
 __global__ void k_pr_init(uint32_t nv, const uint32_t *__restrict__ outdeg, const uint32_t *__restrict__ newid,
-                          float init, const float *__restrict__ init_rank, float *__restrict__ r, float *__restrict__ c) {
+                          float init, const float *__restrict__ init_rank, uint32_t source, float *__restrict__ r,
+                          float *__restrict__ c) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        float x = init_rank ? init_rank[v] : init;
+        /* personalised runs start from the indicator of the source */
+        float x = init_rank ? init_rank[v] : (source == GCG_NO_SOURCE ? init : (v == source ? 1.0f : 0.0f));
         r[v] = x;
         uint32_t od = outdeg[v];
         c[newid[v]] = od ? __fdiv_rn(x, (float)od) : 0.0f;
@@ -435,10 +444,13 @@ __global__ void k_pr_init_nz(uint32_t nnz, const uint32_t *__restrict__ nz_rows,
 /* assemble the full rank vector after the last sweep */
 __global__ void k_pr_scatter(uint32_t nnz, uint32_t nzero, const uint32_t *__restrict__ nz_rows,
                              const uint32_t *__restrict__ zero_rows, const float *__restrict__ r_nz, float t,
-                             float *__restrict__ r) {
+                             uint32_t source, float *__restrict__ r) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     for (uint32_t i = tid; i < nnz; i += nth) r[nz_rows[i]] = r_nz[i];
-    for (uint32_t i = tid; i < nzero; i += nth) r[zero_rows[i]] = t;
+    for (uint32_t i = tid; i < nzero; i += nth) {
+        const uint32_t v = zero_rows[i];
+        r[v] = (source == GCG_NO_SOURCE || v == source) ? t : 0.0f;
+    }
 }
 
 __global__ void k_gather_u32(uint32_t n, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ src,
@@ -622,7 +634,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
             init_dev = init_stage.get();
         }
     }
-    k_pr_init<<<grid1d(nv, 8), 256, 0, s>>>(nv, g->outdeg.get(), pl.newid.get(), p->init, init_dev, r.get(), c.get());
+    k_pr_init<<<grid1d(nv, 8), 256, 0, s>>>(nv, g->outdeg.get(), pl.newid.get(), p->init, init_dev, p->source, r.get(),
+                                            c.get());
     k_pr_init_nz<<<grid1d(pl.nnz, 8), 256, 0, s>>>(pl.nnz, pl.nz_rows.get(), r.get(), rnz.get());
     GCG_LAUNCH_CHECK();
 
@@ -657,7 +670,14 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     a.damping = p->damping;
     a.tol = p->tol;
     /* |r'| of the constant vertices, added to the norm once they are no longer visited */
-    a.norm_const = (double)pl.nzero * fabs((double)(float)p->teleport);
+    a.source = p->source;
+    if (p->source == GCG_NO_SOURCE) {
+        a.norm_const = (double)pl.nzero * fabs((double)(float)p->teleport);
+    } else { /* only the source keeps a teleport value, if it has no in-edges */
+        uint32_t sdeg = 0;
+        GCG_CUDA(cudaMemcpy(&sdeg, g->indeg.get() + p->source, 4, cudaMemcpyDeviceToHost));
+        a.norm_const = sdeg == 0 ? fabs((double)(float)p->teleport) : 0.0;
+    }
     const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 4);
 
     cudaEvent_t ev0, ev1;
@@ -752,7 +772,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     if (sweeps > 0) {
         const float t = (float)p->teleport; /* teleport + damping * 0 */
         k_pr_scatter<<<grid1d(nv, 8), 256, 0, s>>>(pl.nnz, pl.nzero, pl.nz_rows.get(), pl.zero_rows.get(),
-                                                  rnz.get() + (size_t)(sweeps & 1) * pl.nnz, t, r.get());
+                                                  rnz.get() + (size_t)(sweeps & 1) * pl.nnz, t, p->source,
+                                                  r.get());
         GCG_LAUNCH_CHECK();
     }
     if (out_rank) GCG_TRY(copy_out(out_rank, r.get(), (size_t)nv * sizeof(float), s));
@@ -786,11 +807,17 @@ void gcg_pr_params_default(gcg_pr_params *p) {
     p->flags = 0u;
     p->init_rank = nullptr;
     p->residuals = nullptr;
+    p->source = GCG_NO_SOURCE;
+    p->reserved2 = 0u;
 }
 
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats) {
     if (!g || !params) return fail(GCG_ERR_INVALID, "gcg_pagerank: null argument");
     if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_pagerank: max_sweeps < 0");
+    if (params->source != GCG_NO_SOURCE && params->source >= g->nv)
+        return fail(GCG_ERR_INVALID, "gcg_pagerank: personalisation source >= num_vertices");
+    if (params->source != GCG_NO_SOURCE && params->mode != GCG_PR_JACOBI)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank: personalisation needs GCG_PR_JACOBI");
     if (params->mode == GCG_PR_JACOBI) return pagerank_jacobi(g, params, out_rank, stats);
     if (params->mode == GCG_PR_GS_EXACT) return pagerank_gs_exact(g, params, out_rank, stats);
     return fail(GCG_ERR_INVALID, "gcg_pagerank: unknown mode");

@@ -45,7 +45,7 @@ EXPORTED = [
     "gcg_graph_degrees", "gcg_graph_csr", "gcg_graph_write_metadata", "gcg_write_vout",
     "gcg_pr_params_default", "gcg_pagerank", "gcg_connected_components", "gcg_triangle_count",
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
-    "gcg_pagerank_csr_noalloc",
+    "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
 ]
 NOALLOC_MAX_VERTICES = 1 << 20
 
@@ -64,7 +64,11 @@ class GraphInfo(C.Structure):
 class PrParams(C.Structure):
     _fields_ = [("mode", C.c_int), ("max_sweeps", C.c_int), ("teleport", C.c_double),
                 ("damping", C.c_double), ("tol", C.c_double), ("init", C.c_float),
-                ("flags", C.c_uint32), ("init_rank", C.c_void_p), ("residuals", C.c_void_p)]
+                ("flags", C.c_uint32), ("init_rank", C.c_void_p), ("residuals", C.c_void_p),
+                ("source", C.c_uint32), ("reserved2", C.c_uint32)]
+
+
+NO_SOURCE = 0xFFFFFFFF
 
 
 class PrStats(C.Structure):
@@ -109,6 +113,7 @@ _gen_rmat = _sig("gcg_generate_rmat", _i, _u32, _u64, C.c_double, C.c_double, C.
 _gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
 _pr_noalloc = _sig("gcg_pagerank_csr_noalloc", _i, _vp, _vp, _vp, _u32, C.POINTER(PrParams), _vp, _vp,
                    C.POINTER(PrStats))
+_ppr = _sig("gcg_ppr_batched", _i, _vp, _vp, _u32, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
 _last_error = _sig("gcg_last_error", C.c_char_p)
 _version = _sig("gcg_version", C.c_char_p)
 
@@ -229,13 +234,14 @@ class Graph:
         check(_write_meta(self._h, os.fsencode(base)))
 
     def pagerank(self, mode=PR_JACOBI, max_sweeps=3, teleport=0.15, damping=0.85, tol=0.0, init=1.0,
-                 init_rank=None, out=None, residuals=None, time_sweeps=False):
+                 init_rank=None, out=None, residuals=None, time_sweeps=False, source=None):
         """Returns (ranks, PrStats). out/init_rank/residuals: numpy or device tensors."""
         p = PrParams()
         _pr_default(C.byref(p))
         p.mode, p.max_sweeps, p.teleport, p.damping, p.tol, p.init = (
             mode, max_sweeps, teleport, damping, tol, init)
         p.flags = PR_TIME_SWEEPS if time_sweeps else 0
+        p.source = NO_SOURCE if source is None else int(source)
         if init_rank is not None:
             init_rank = init_rank if not isinstance(init_rank, np.ndarray) else \
                 np.ascontiguousarray(init_rank, dtype=np.float32)
@@ -246,6 +252,23 @@ class Graph:
             out = np.zeros(self.num_vertices, dtype=np.float32)
         st = PrStats()
         check(_pagerank(self._h, C.byref(p), ptr(out), C.byref(st)))
+        return out, st
+
+    def ppr_batched(self, sources, max_sweeps=100, teleport=0.15, damping=0.85, tol=0.0, out=None,
+                    residuals=None, time_sweeps=False):
+        """Batched personalised PageRank; returns (V x k ranks, PrStats)."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32) if isinstance(sources, (list, np.ndarray)) else sources
+        k = int(src.shape[0])
+        p = PrParams()
+        _pr_default(C.byref(p))
+        p.max_sweeps, p.teleport, p.damping, p.tol = max_sweeps, teleport, damping, tol
+        p.flags = PR_TIME_SWEEPS if time_sweeps else 0
+        if residuals is not None:
+            p.residuals = ptr(residuals)
+        if out is None:
+            out = np.zeros((self.num_vertices, k), dtype=np.float32)
+        st = PrStats()
+        check(_ppr(self._h, ptr(src), k, C.byref(p), ptr(out), C.byref(st)))
         return out, st
 
     def connected_components(self, out=None):

@@ -127,9 +127,13 @@ typedef struct {
     uint32_t flags;         /* GCG_PR_TIME_SWEEPS: time each sweep kernel with CUDA events */
     const float *init_rank; /* optional initial vector (num_vertices, host or device): the warm start */
     double *residuals;      /* optional: per-sweep residual log (max_sweeps doubles, host or device) */
+    uint32_t source;        /* personalisation: teleport (and the initial mass 1) only at this
+                               vertex; GCG_NO_SOURCE = plain PageRank. JACOBI only. */
+    uint32_t reserved2;
 } gcg_pr_params;
 
 #define GCG_PR_TIME_SWEEPS 0x1u
+#define GCG_NO_SOURCE 0xFFFFFFFFu
 
 typedef struct {
     int sweeps;             /* sweeps run */
@@ -154,6 +158,19 @@ void gcg_pr_params_default(gcg_pr_params *p);
  * same final values as pagerank.cpp:140-143 (pr * outdeg).
  * out_rank: num_vertices floats, host or device. stats may be NULL. */
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats);
+
+/* Batched personalised PageRank (the engine's addition beside the reference's
+ * one-vector runs of example_apps/pagerank.cpp): nsources sources solved together
+ * as a vertex-major rank matrix. For source s: r_s starts at the indicator of
+ * sources[s]; each sweep r_s[v] = (float)(params->teleport*[v == sources[s]] +
+ * params->damping * sum_{u->v} r_s[u]/outdeg[u]) (float contributions and sums);
+ * stops after max_sweeps or when the largest per-source normalised L1 change
+ * (FP64) is <= params->tol. mode must be GCG_PR_JACOBI, init_rank NULL and source
+ * GCG_NO_SOURCE. sources: nsources ids, host or device. out: num_vertices x
+ * nsources floats, out[v * nsources + s], host or device. params->residuals (if
+ * set) receives the per-sweep maximum residual. Sources run in groups of 256. */
+int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t nsources, const gcg_pr_params *params,
+                    float *out, gcg_pr_stats *stats);
 
 /* No counterpart in the reference. PageRank (GCG_PR_JACOBI only) over an in-edge
  * CSR the caller already keeps in device memory, for callers that cannot let a
