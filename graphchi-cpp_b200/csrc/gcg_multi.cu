@@ -1,0 +1,757 @@
+/*
+ * Many independent graphs, one persistent launch.
+ *
+ * The engine's addition for batches of uneven graphs (no reference counterpart:
+ * the reference runs one graph per engine). gcg_batch_create concatenates the
+ * graphs' in-CSRs into one block-diagonal union (vertex and edge offsets; each
+ * graph is one interval) and builds the PageRank chunk plan on it, so the
+ * out-degree relabelling and the shared-memory hub cache serve all graphs.
+ *
+ * gcg_batch_pagerank runs every sweep of every graph inside ONE cooperative
+ * persistent kernel (one 1024-thread CTA per SM). Per sweep, four phases split by
+ * a grid barrier:
+ *   A  edges: warps pull 256-edge chunks of the still-active graphs from a device
+ *      work queue (atomic counter over the concatenated chunk ranges) and run the
+ *      same gather / warp reduction as the single-graph kernel;
+ *   B  rows crossing chunks: partials added in chunk order;
+ *   C  vertices: CTAs pull 1024-row tiles of the active graphs from a second
+ *      queue, apply, and write one FP64 residual partial per tile (fixed slot);
+ *   D  one warp per graph adds its tile partials in a fixed order; a graph whose
+ *      residual is <= tol (or that reached max_sweeps) leaves the queues.
+ * The kernel ends when no graph is active. Each graph's ranks are formed with the
+ * same sums in the same order as its single-graph solve (only the FP64 residual
+ * is reduced in a different order). Contributions change between
+ * sweeps inside the kernel, so they are read with L2-coherent loads, never the
+ * non-coherent path.
+ *
+ * Every grid-barrier wait is bounded: after the spin limit the kernel raises an
+ * error flag and returns, and the host reports GCG_ERR_TIMEOUT.
+ */
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gcg_internal.cuh"
+#include "gcg_pr_device.cuh"
+
+namespace gcg {
+namespace {
+
+constexpr uint32_t VT = EDGE_THREADS; /* rows per vertex tile (one per thread) */
+constexpr uint32_t NG_MAX = 1024;     /* graphs per batch */
+
+/* per-graph ranges in the union */
+struct GRange {
+    uint32_t cs, ce;      /* chunks [cs, ce) holding the graph's edges */
+    uint32_t ss, se;      /* split-row list entries */
+    uint32_t ns, ne;      /* rows with in-edges (nz index range) */
+    uint32_t zs, ze;      /* rows without in-edges (zero index range) */
+    uint32_t it_nz, it_z; /* first tile slot of its nz tiles / zero tiles */
+    uint32_t gend;        /* end of the graph's edges in the union (its chunks stop there) */
+    uint32_t pad1;
+};
+
+struct MultiArgs {
+    SweepArgs a;            /* union graph arguments (buffers set per sweep inside) */
+    float *c[2];
+    float *rnz[2];
+    const GRange *gr;
+    uint32_t ng, max_sweeps;
+    double2 *tile_part;     /* per tile slot */
+    const double *norm_const; /* per graph */
+    int *active;            /* per graph */
+    int *gsweeps;           /* per graph: sweeps run */
+    double *gres;           /* per graph: last residual */
+    uint32_t *qctr;         /* [2 parities][2 queues] */
+    uint32_t *bar;          /* [0] arrivals, [1] generation */
+    int *err;
+    long long spin_limit;
+    uint32_t extra_arrivals; /* test hook: the barrier waits for this many more CTAs */
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+/* Grid barrier with a bounded wait; returns false (all CTAs) once any CTA timed out. */
+__device__ bool grid_sync(const MultiArgs &m, uint32_t &gen) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t target = gen + 1;
+        const uint32_t expect = gridDim.x + m.extra_arrivals;
+        if (atomicAdd(m.bar, 1u) == expect - 1) {
+            atomicExch(m.bar, 0u);
+            __threadfence();
+            atomicExch(m.bar + 1, target);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_u32(m.bar + 1) < target) {
+                if (*(volatile int *)m.err || ++spins > m.spin_limit) {
+                    atomicExch(m.err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        gen = target;
+        __threadfence();
+        s_ok = *(volatile int *)m.err == 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+/* prefix over the active graphs of a per-graph count, in shared memory;
+ * *nactive receives the number of active graphs */
+__device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pref, uint32_t *nactive = nullptr) {
+    __shared__ uint32_t s_nact;
+    if (threadIdx.x == 0) {
+        uint32_t t = 0, na = 0;
+        for (uint32_t g = 0; g < m.ng; ++g) {
+            s_pref[g] = t;
+            if (*(volatile int *)(m.active + g)) {
+                const GRange r = m.gr[g];
+                t += which == 0 ? r.ce - r.cs : which == 1 ? r.se - r.ss : 0u;
+                ++na;
+            }
+        }
+        s_pref[m.ng] = t;
+        s_nact = na;
+    }
+    __syncthreads();
+    if (nactive) *nactive = s_nact;
+    return s_pref[m.ng];
+}
+
+/* the active graph whose range holds position x of the concatenation */
+__device__ __forceinline__ uint32_t find_graph(const uint32_t *s_pref, uint32_t ng, uint32_t x) {
+    uint32_t lo = 0, hi = ng; /* largest g with s_pref[g] <= x: its range is non-empty */
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_pref[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m) {
+    extern __shared__ float s_hub[];
+    __shared__ uint32_t s_pref[NG_MAX + 1];
+    __shared__ uint32_t s_item;
+    __shared__ double2 s_red[EDGE_THREADS / 32];
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
+    uint32_t gen = 0;
+    SweepArgs a = m.a;
+
+    for (uint32_t sweep = 0; sweep < m.max_sweeps; ++sweep) {
+        a.c_old = m.c[sweep & 1];
+        a.c_new = m.c[(sweep + 1) & 1];
+        a.r_nz_old = m.rnz[sweep & 1];
+        a.r_nz_new = m.rnz[(sweep + 1) & 1];
+        const int const_pass = sweep < 2;
+        uint32_t *qA = m.qctr + 2 * (sweep & 1), *qC = qA + 1;
+
+        /* ---- A: edge chunks of the active graphs (work queue) ---- */
+        uint32_t nact = 0;
+        const uint32_t totA = active_prefix(m, 0, s_pref, &nact);
+        if (nact == 0) break; /* every graph has stopped: the same answer in every CTA */
+        load_hub(a, s_hub);
+        __syncthreads();
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) item = atomicAdd(qA, 1u);
+            item = __shfl_sync(FULL, item, 0);
+            if (item >= totA) break;
+            const uint32_t g = find_graph(s_pref, m.ng, item);
+            const uint32_t ch = m.gr[g].cs + (item - s_pref[g]);
+            uint32_t col[EPL], flags, nvalid, base;
+            const uint64_t gend = m.gr[g].gend;
+            load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
+            float val[EPL];
+            gather_chunk<true>(a, col, nvalid, s_hub, pol_keep, val);
+            reduce_chunk(a, ch, lane, val, flags, nvalid, base, gend);
+        }
+        if (!grid_sync(m, gen)) return;
+
+        /* ---- B: rows crossing chunk boundaries, summed exactly as the
+         *         single-graph fix-up does (k_pr_fix): short rows by one lane in
+         *         chunk order, long rows by the warp (lane-strided, xor tree) ---- */
+        const uint32_t totB = active_prefix(m, 1, s_pref);
+        for (uint32_t wb = gwarp * 32u; wb < totB; wb += nwarps * 32u) {
+            const uint32_t x = wb + lane;
+            uint4 sp = make_uint4(0, 0, 0, 0);
+            const bool valid = x < totB;
+            if (valid) {
+                const uint32_t g = find_graph(s_pref, m.ng, x);
+                sp = a.split[m.gr[g].ss + (x - s_pref[g])];
+            }
+            const bool lng = valid && (sp.z - sp.y) > 8u;
+            if (valid && !lng) {
+                float s = __ldcg(a.tail_part + sp.y);
+                for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += __ldcg(a.head_part + c);
+                a.nzsum[sp.x] = s;
+            }
+            uint32_t msk = __ballot_sync(FULL, lng);
+            while (msk) {
+                const int srcl = __ffs(msk) - 1;
+                msk &= msk - 1;
+                const uint32_t row = __shfl_sync(FULL, sp.x, srcl);
+                const uint32_t cs = __shfl_sync(FULL, sp.y, srcl);
+                const uint32_t ce = __shfl_sync(FULL, sp.z, srcl);
+                float s = 0.0f;
+                for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) s += __ldcg(a.head_part + c);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+                if (lane == 0) a.nzsum[row] = __ldcg(a.tail_part + cs) + s;
+            }
+        }
+        if (!grid_sync(m, gen)) return;
+
+        /* ---- C: vertex tiles of the active graphs (work queue), one residual
+         *         partial per tile ---- */
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (uint32_t g = 0; g < m.ng; ++g) {
+                s_pref[g] = t;
+                if (*(volatile int *)(m.active + g)) {
+                    const GRange r = m.gr[g];
+                    t += (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
+                }
+            }
+            s_pref[m.ng] = t;
+        }
+        __syncthreads();
+        const uint32_t totC = s_pref[m.ng];
+        for (;;) {
+            if (threadIdx.x == 0) s_item = atomicAdd(qC, 1u);
+            __syncthreads();
+            const uint32_t item = s_item;
+            __syncthreads();
+            if (item >= totC) break;
+            const uint32_t g = find_graph(s_pref, m.ng, item);
+            const GRange r = m.gr[g];
+            const uint32_t t = item - s_pref[g];
+            const uint32_t ntn = (r.ne - r.ns + VT - 1) / VT;
+            double d = 0.0, n = 0.0;
+            uint32_t slot;
+            if (t < ntn) {
+                slot = r.it_nz + t;
+                const uint32_t i = r.ns + t * VT + threadIdx.x;
+                if (i < r.ne) {
+                    const float rn = pr_value(a, __ldcg(a.nzsum + i));
+                    const float ro = __ldcg(a.r_nz_old + i);
+                    const uint32_t od = a.od_nz[i];
+                    a.r_nz_new[i] = rn;
+                    a.c_new[a.nz_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
+                    d = fabs((double)rn - (double)ro);
+                    n = fabs((double)rn);
+                }
+            } else {
+                slot = r.it_z + (t - ntn);
+                const uint32_t i = r.zs + (t - ntn) * VT + threadIdx.x;
+                if (i < r.ze) {
+                    const uint32_t v = a.zero_rows[i];
+                    const float rn = pr_value(a, 0.0f);
+                    const float ro = sweep == 0 ? __ldcg(a.r_init + v) : rn;
+                    const uint32_t od = a.outdeg[v];
+                    a.c_new[a.zero_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
+                    d = fabs((double)rn - (double)ro);
+                    n = fabs((double)rn);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                d += __shfl_down_sync(FULL, d, o);
+                n += __shfl_down_sync(FULL, n, o);
+            }
+            if (lane == 0) s_red[warp] = make_double2(d, n);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double2 tot = make_double2(0.0, 0.0);
+                for (uint32_t w = 0; w < EDGE_THREADS / 32; ++w) {
+                    tot.x += s_red[w].x;
+                    tot.y += s_red[w].y;
+                }
+                m.tile_part[slot] = tot;
+            }
+        }
+        if (!grid_sync(m, gen)) return;
+
+        /* ---- D: per-graph residual and stop ---- */
+        for (uint32_t g = gwarp; g < m.ng; g += nwarps) {
+            if (!*(volatile int *)(m.active + g)) continue;
+            const GRange r = m.gr[g];
+            const uint32_t nt = (r.ne - r.ns + VT - 1) / VT;
+            const uint32_t nz = const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u;
+            double d = 0.0, n = 0.0;
+            for (uint32_t t = lane; t < nt + nz; t += 32u) {
+                const double2 p = __ldcg(m.tile_part + (t < nt ? r.it_nz + t : r.it_z + (t - nt)));
+                d += p.x;
+                n += p.y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                d += __shfl_xor_sync(FULL, d, o);
+                n += __shfl_xor_sync(FULL, n, o);
+            }
+            if (lane == 0) {
+                if (!const_pass) n += m.norm_const[g];
+                const double res = n > 0.0 ? d / n : 0.0;
+                m.gres[g] = res;
+                m.gsweeps[g] = (int)sweep + 1;
+                if ((a.tol > 0.0 && res <= a.tol) || sweep + 1 >= m.max_sweeps) m.active[g] = 0;
+            }
+        }
+        /* the queues of the next sweep's parity were last used a sweep ago */
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            m.qctr[2 * ((sweep + 1) & 1)] = 0u;
+            m.qctr[2 * ((sweep + 1) & 1) + 1] = 0u;
+        }
+        if (!grid_sync(m, gen)) return;
+    }
+}
+
+/* result assembly: ranks of every vertex of every graph, from the buffer of the
+ * sweep count its graph stopped at */
+__global__ void k_multi_scatter(const GRange *__restrict__ gr, uint32_t ng, const int *__restrict__ gsweeps,
+                                const uint32_t *__restrict__ nz_rows, const uint32_t *__restrict__ zero_rows,
+                                const float *__restrict__ rnz0, const float *__restrict__ rnz1, float t,
+                                float *__restrict__ r) {
+    for (uint32_t g = blockIdx.y; g < ng; g += gridDim.y) {
+        const GRange x = gr[g];
+        const int sw = gsweeps[g];
+        if (sw == 0) continue; /* no sweep: the initial vector stays */
+        const float *src = (sw & 1) ? rnz1 : rnz0;
+        for (uint32_t i = x.ns + blockIdx.x * blockDim.x + threadIdx.x; i < x.ne; i += gridDim.x * blockDim.x)
+            r[nz_rows[i]] = src[i];
+        for (uint32_t i = x.zs + blockIdx.x * blockDim.x + threadIdx.x; i < x.ze; i += gridDim.x * blockDim.x)
+            r[zero_rows[i]] = t;
+    }
+}
+
+__global__ void k_concat(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
+                         const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ outdeg, uint32_t nv,
+                         uint64_t ne, uint32_t voff, uint32_t eoff, uint32_t *__restrict__ urowptr,
+                         uint32_t *__restrict__ ucol, uint32_t *__restrict__ uindeg, uint32_t *__restrict__ uoutdeg) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v <= nv; v += nth) {
+        urowptr[voff + v] = rowptr[v] + eoff;
+        if (v < nv) {
+            uindeg[voff + v] = indeg[v];
+            uoutdeg[voff + v] = outdeg[v];
+        }
+    }
+    for (uint64_t e = tid; e < ne; e += nth) ucol[eoff + e] = col[e] + voff;
+}
+
+/* the padding vertex after a graph: in-edges [pe0, pe1) from itself, no out-edges */
+__global__ void k_pad(uint32_t pv, uint32_t pe0, uint32_t pe1, uint32_t *__restrict__ urowptr, uint32_t *__restrict__ ucol,
+                      uint32_t *__restrict__ uindeg, uint32_t *__restrict__ uoutdeg) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (tid == 0) {
+        urowptr[pv] = pe0;
+        urowptr[pv + 1] = pe1;
+        uindeg[pv] = pe1 - pe0;
+        uoutdeg[pv] = 0u;
+    }
+    for (uint32_t e = pe0 + tid; e < pe1; e += nth) ucol[e] = pv;
+}
+
+/* graph g's vertices keep their order at union offset voff[g]; map both ways */
+__global__ void k_expand(const float *__restrict__ src, const uint32_t *__restrict__ roff, const uint32_t *__restrict__ voff,
+                         uint32_t ng, float *__restrict__ dst, int to_union) {
+    for (uint32_t g = blockIdx.y; g < ng; g += gridDim.y) {
+        const uint32_t n = roff[g + 1] - roff[g];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            if (to_union) dst[voff[g] + i] = src[roff[g] + i];
+            else dst[roff[g] + i] = src[voff[g] + i];
+        }
+    }
+}
+
+/* lower bound of each query id in a sorted id list */
+__global__ void k_bounds(const uint32_t *__restrict__ ids, uint32_t n, const uint32_t *__restrict__ q, uint32_t nq,
+                         uint32_t *__restrict__ out) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nq) return;
+    const uint32_t x = q[g];
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (ids[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    out[g] = lo;
+}
+
+/* lower bound of each graph's first nz index in the split-row list */
+__global__ void k_split_bounds(const uint4 *__restrict__ split, uint32_t n, const uint32_t *__restrict__ nzb, uint32_t nq,
+                               uint32_t *__restrict__ out) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nq) return;
+    const uint32_t x = nzb[g];
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (split[mid].x < x) lo = mid + 1; else hi = mid;
+    }
+    out[g] = lo;
+}
+
+}  // namespace
+}  // namespace gcg
+
+/* ---- host side ------------------------------------------------------------ */
+
+struct gcg_batch {
+    uint32_t ng = 0;
+    gcg_graph *u = nullptr; /* the union graph (owned) */
+    std::vector<uint32_t> voff, eoff;   /* union vertex / edge offset of each graph (edges 256-aligned) */
+    std::vector<uint32_t> roff;         /* offset of each graph in the callers' arrays (no padding) */
+    std::vector<gcg::GRange> gr_host;
+    gcg::dbuf<uint32_t> d_roff, d_voff;
+    uint32_t ntiles = 0;
+    gcg::dbuf<gcg::GRange> gr;
+    /* workspace, allocated on the first solve */
+    gcg::dbuf<float> c, rnz, r, nzsum, parts;
+    gcg::dbuf<double2> tile_part;
+    gcg::dbuf<double> norm_const, gres;
+    gcg::dbuf<int> active, gsweeps, err;
+    gcg::dbuf<uint32_t> qctr, bar;
+    ~gcg_batch() { delete u; }
+};
+
+namespace gcg {
+
+static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
+    b->ng = ng;
+    b->voff.assign(ng + 1, 0);
+    b->eoff.assign(ng + 1, 0);
+    b->roff.assign(ng + 1, 0);
+    std::vector<uint32_t> gend(ng);
+    uint64_t V = 0, E = 0, R = 0;
+    for (uint32_t g = 0; g < ng; ++g) {
+        E = (E + CH - 1) / CH * CH; /* the graph starts on a chunk boundary */
+        b->voff[g] = (uint32_t)V;
+        b->eoff[g] = (uint32_t)E;
+        b->roff[g] = (uint32_t)R;
+        V += graphs[g]->nv + 1; /* + its padding vertex */
+        R += graphs[g]->nv;
+        E += graphs[g]->ne;
+        gend[g] = (uint32_t)E;
+        if (V >= 0xFFFFFFFFull || E + CH >= 0xFFFFFFFFull)
+            return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_create: more than 2^32-1 vertices or edges in total");
+    }
+    const uint64_t Etot = (E + CH - 1) / CH * CH;
+    b->voff[ng] = (uint32_t)V;
+    b->eoff[ng] = (uint32_t)Etot;
+    b->roff[ng] = (uint32_t)R;
+    gcg_graph *u = new gcg_graph();
+    b->u = u;
+    u->nv = (uint32_t)V;
+    u->ne = Etot;
+    u->vbits = 1;
+    while (u->vbits < 32 && (1ull << u->vbits) < V) ++u->vbits;
+    if (u->in_rowptr.alloc((size_t)V + 1) || u->in_col.alloc(Etot) || u->indeg.alloc(V) || u->outdeg.alloc(V))
+        return GCG_ERR_NOMEM;
+    for (uint32_t g = 0; g < ng; ++g) {
+        const gcg_graph *x = graphs[g];
+        const uint64_t n = std::max<uint64_t>(x->nv + 1ull, x->ne);
+        const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)num_sms() * 16));
+        k_concat<<<blocks, 256>>>(x->in_rowptr.get(), x->in_col.get(), x->indeg.get(), x->outdeg.get(), x->nv, x->ne,
+                                  b->voff[g], b->eoff[g], u->in_rowptr.get(), u->in_col.get(), u->indeg.get(),
+                                  u->outdeg.get());
+        /* padding vertex: the filler edges up to the next graph's chunk boundary */
+        k_pad<<<8, 256>>>(b->voff[g] + x->nv, gend[g], b->eoff[g + 1], u->in_rowptr.get(), u->in_col.get(),
+                          u->indeg.get(), u->outdeg.get());
+    }
+    GCG_LAUNCH_CHECK();
+    /* each graph (with its padding vertex) is one interval of the union */
+    u->nshards = ng;
+    GCG_TRY(u->intervals_dev.alloc(ng));
+    u->intervals_host = (uint32_t *)malloc((size_t)ng * 4);
+    for (uint32_t g = 0; g < ng; ++g) u->intervals_host[g] = b->voff[g + 1] - 1;
+    GCG_CUDA(cudaMemcpy(u->intervals_dev.get(), u->intervals_host, (size_t)ng * 4, cudaMemcpyHostToDevice));
+    GCG_TRY(ensure_chunk_plan(u));
+    const ChunkPlan &pl = *u->cplan;
+    /* per-graph ranges (padding vertices excluded) by binary search on the device:
+     * query 2g = first vertex of graph g, 2g+1 = its padding vertex */
+    const uint32_t nq = 2 * ng;
+    std::vector<uint32_t> q(nq);
+    for (uint32_t g = 0; g < ng; ++g) {
+        q[2 * g] = b->voff[g];
+        q[2 * g + 1] = b->voff[g] + graphs[g]->nv;
+    }
+    dbuf<uint32_t> dq, nzb, zb, sb;
+    GCG_TRY(dq.alloc(nq));
+    GCG_TRY(nzb.alloc(nq));
+    GCG_TRY(zb.alloc(nq));
+    GCG_TRY(sb.alloc(nq));
+    GCG_CUDA(cudaMemcpy(dq.get(), q.data(), nq * 4, cudaMemcpyHostToDevice));
+    const unsigned gb = (nq + 255) / 256;
+    k_bounds<<<gb, 256>>>(pl.nz_rows.get(), pl.nnz, dq.get(), nq, nzb.get());
+    k_bounds<<<gb, 256>>>(pl.zero_rows.get(), pl.nzero, dq.get(), nq, zb.get());
+    k_split_bounds<<<gb, 256>>>(pl.split.get(), pl.nsplit, nzb.get(), nq, sb.get());
+    GCG_LAUNCH_CHECK();
+    std::vector<uint32_t> hn(nq), hz(nq), hs(nq);
+    GCG_CUDA(cudaMemcpy(hn.data(), nzb.get(), nq * 4, cudaMemcpyDeviceToHost));
+    GCG_CUDA(cudaMemcpy(hz.data(), zb.get(), nq * 4, cudaMemcpyDeviceToHost));
+    GCG_CUDA(cudaMemcpy(hs.data(), sb.get(), nq * 4, cudaMemcpyDeviceToHost));
+    b->gr_host.resize(ng);
+    uint32_t tiles = 0;
+    for (uint32_t g = 0; g < ng; ++g) {
+        GRange &r = b->gr_host[g];
+        r.cs = b->eoff[g] / CH;
+        r.ce = (gend[g] + CH - 1) / CH;
+        r.gend = gend[g];
+        r.ns = hn[2 * g];
+        r.ne = hn[2 * g + 1];
+        r.zs = hz[2 * g];
+        r.ze = hz[2 * g + 1];
+        r.ss = hs[2 * g];
+        r.se = hs[2 * g + 1];
+        r.it_nz = tiles;
+        tiles += (r.ne - r.ns + VT - 1) / VT;
+        r.it_z = tiles;
+        tiles += (r.ze - r.zs + VT - 1) / VT;
+        r.pad1 = 0;
+    }
+    b->ntiles = tiles;
+    GCG_TRY(b->gr.alloc(ng));
+    GCG_CUDA(cudaMemcpy(b->gr.get(), b->gr_host.data(), ng * sizeof(GRange), cudaMemcpyHostToDevice));
+    GCG_TRY(b->d_roff.alloc(ng + 1));
+    GCG_TRY(b->d_voff.alloc(ng + 1));
+    GCG_CUDA(cudaMemcpy(b->d_roff.get(), b->roff.data(), (ng + 1) * 4, cudaMemcpyHostToDevice));
+    GCG_CUDA(cudaMemcpy(b->d_voff.get(), b->voff.data(), (ng + 1) * 4, cudaMemcpyHostToDevice));
+    return GCG_OK;
+}
+
+static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int32_t *sweeps, double *residuals,
+                          gcg_pr_stats *stats) {
+    gcg_graph *u = b->u;
+    const ChunkPlan &pl = *u->cplan;
+    const uint32_t nv = u->nv, ng = b->ng;
+    cudaStream_t s = u->stream;
+    const size_t cstride = ((size_t)nv + 63) & ~(size_t)63;
+    if (!b->c.get()) {
+        GCG_TRY(b->c.alloc(2 * cstride));
+        GCG_TRY(b->rnz.alloc((size_t)2 * std::max<uint32_t>(pl.nnz, 1)));
+        GCG_TRY(b->r.alloc(nv));
+        GCG_TRY(b->nzsum.alloc(std::max<uint32_t>(pl.nnz, 1)));
+        GCG_TRY(b->parts.alloc((size_t)2 * pl.nchunks + 2));
+        GCG_TRY(b->tile_part.alloc(std::max<uint32_t>(b->ntiles, 1)));
+        GCG_TRY(b->norm_const.alloc(ng));
+        GCG_TRY(b->gres.alloc(ng));
+        GCG_TRY(b->active.alloc(ng));
+        GCG_TRY(b->gsweeps.alloc(ng));
+        GCG_TRY(b->err.alloc(1));
+        GCG_TRY(b->qctr.alloc(4));
+        GCG_TRY(b->bar.alloc(2));
+    }
+    /* initial state */
+    const uint32_t nreal = b->roff[ng];
+    const dim3 eg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nreal / ng + 255) / 256, 64)),
+                  std::min<uint32_t>(ng, 1024));
+    tbuf<float> init_stage, init_union;
+    const float *init_dev = nullptr;
+    if (p->init_rank) { /* caller layout (no padding) -> union layout; padding vertices get 0 */
+        const float *src = p->init_rank;
+        if (!is_device_ptr(p->init_rank)) {
+            GCG_TRY(init_stage.alloc(nreal, s));
+            GCG_TRY(copy_in(init_stage.get(), p->init_rank, (size_t)nreal * 4, s));
+            src = init_stage.get();
+        }
+        GCG_TRY(init_union.alloc(nv, s));
+        GCG_CUDA(cudaMemsetAsync(init_union.get(), 0, (size_t)nv * 4, s));
+        k_expand<<<eg, 256, 0, s>>>(src, b->d_roff.get(), b->d_voff.get(), ng, init_union.get(), 1);
+        init_dev = init_union.get();
+    }
+    GCG_TRY(pr_init_state(u, p->init, init_dev, b->r.get(), b->c.get(), b->rnz.get()));
+    std::vector<double> nc(ng);
+    std::vector<int> act(ng, 1);
+    for (uint32_t g = 0; g < ng; ++g)
+        nc[g] = (double)(b->gr_host[g].ze - b->gr_host[g].zs) * fabs((double)(float)p->teleport);
+    GCG_CUDA(cudaMemcpyAsync(b->norm_const.get(), nc.data(), ng * 8, cudaMemcpyHostToDevice, s));
+    GCG_CUDA(cudaMemcpyAsync(b->active.get(), act.data(), ng * 4, cudaMemcpyHostToDevice, s));
+    GCG_CUDA(cudaMemsetAsync(b->gsweeps.get(), 0, ng * 4, s));
+    GCG_CUDA(cudaMemsetAsync(b->gres.get(), 0, ng * 8, s));
+    GCG_CUDA(cudaMemsetAsync(b->err.get(), 0, 4, s));
+    GCG_CUDA(cudaMemsetAsync(b->qctr.get(), 0, 16, s));
+    GCG_CUDA(cudaMemsetAsync(b->bar.get(), 0, 8, s));
+
+    MultiArgs m;
+    SweepArgs &a = m.a;
+    memset(&a, 0, sizeof(a));
+    a.col = pl.col_r.get();
+    a.outdeg = u->outdeg.get();
+    a.heads = (const uint8_t *)pl.head_bits.get();
+    a.chunk_nz = pl.chunk_nz.get();
+    a.nz_rows = pl.nz_rows.get();
+    a.zero_rows = pl.zero_rows.get();
+    a.split = pl.split.get();
+    a.ne = u->ne;
+    a.nchunks = pl.nchunks;
+    a.nnz = pl.nnz;
+    a.nzero = pl.nzero;
+    a.nsplit = pl.nsplit;
+    a.hub = pl.hub;
+    a.nz_cidx = pl.nz_cidx.get();
+    a.zero_cidx = pl.zero_cidx.get();
+    a.od_nz = pl.od_nz.get();
+    a.r_init = b->r.get();
+    a.nzsum = b->nzsum.get();
+    a.head_part = b->parts.get();
+    a.tail_part = b->parts.get() + pl.nchunks + 1;
+    a.teleport = p->teleport;
+    a.damping = p->damping;
+    a.tol = p->tol;
+    a.source = GCG_NO_SOURCE;
+    m.c[0] = b->c.get();
+    m.c[1] = b->c.get() + cstride;
+    m.rnz[0] = b->rnz.get();
+    m.rnz[1] = b->rnz.get() + pl.nnz;
+    m.gr = b->gr.get();
+    m.ng = ng;
+    m.max_sweeps = (uint32_t)p->max_sweeps;
+    m.tile_part = b->tile_part.get();
+    m.norm_const = b->norm_const.get();
+    m.active = b->active.get();
+    m.gsweeps = b->gsweeps.get();
+    m.gres = b->gres.get();
+    m.qctr = b->qctr.get();
+    m.bar = b->bar.get();
+    m.err = b->err.get();
+    const bool test_timeout = (p->flags & GCG_PR_TEST_BARRIER_TIMEOUT) != 0;
+    m.spin_limit = test_timeout ? (1ll << 14) : (1ll << 25);
+    m.extra_arrivals = test_timeout ? 1u : 0u;
+
+    /* one cooperative launch: one CTA per SM, all resident */
+    const uint32_t hub_bytes = pl.hub * 4u;
+    GCG_CUDA(cudaFuncSetAttribute(k_multi_pagerank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4)));
+    int per_sm = 0;
+    GCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multi_pagerank, EDGE_THREADS, hub_bytes));
+    if (per_sm < 1) return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_pagerank: persistent kernel does not fit an SM");
+    const unsigned grid = (unsigned)num_sms();
+    cudaEvent_t ev0, ev1;
+    GCG_CUDA(cudaEventCreate(&ev0));
+    GCG_CUDA(cudaEventCreate(&ev1));
+    GCG_CUDA(cudaEventRecord(ev0, s));
+    void *kargs[] = {&m};
+    cudaError_t le = cudaLaunchCooperativeKernel((const void *)k_multi_pagerank, dim3(grid), dim3(EDGE_THREADS), kargs,
+                                                 hub_bytes, s);
+    if (le != cudaSuccess) {
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        return fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: cooperative launch: ") + cudaGetErrorString(le));
+    }
+    GCG_CUDA(cudaEventRecord(ev1, s));
+    int herr = 0;
+    GCG_CUDA(cudaMemcpyAsync(&herr, b->err.get(), 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (herr) return fail(GCG_ERR_TIMEOUT, "gcg_batch_pagerank: a grid-barrier wait ran out (persistent kernel stopped)");
+    /* assemble the ranks */
+    {
+        dim3 sg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv / ng + 255) / 256, 64)),
+                std::min<uint32_t>(ng, 1024));
+        const float t = (float)p->teleport;
+        k_multi_scatter<<<sg, 256, 0, s>>>(b->gr.get(), ng, b->gsweeps.get(), pl.nz_rows.get(), pl.zero_rows.get(),
+                                           m.rnz[0], m.rnz[1], t, b->r.get());
+        GCG_LAUNCH_CHECK();
+    }
+    std::vector<int> hsw(ng);
+    std::vector<double> hres(ng);
+    GCG_CUDA(cudaMemcpyAsync(hsw.data(), b->gsweeps.get(), ng * 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaMemcpyAsync(hres.data(), b->gres.get(), ng * 8, cudaMemcpyDeviceToHost, s));
+    if (out) { /* union layout -> caller layout */
+        tbuf<float> compact;
+        GCG_TRY(compact.alloc(nreal, s));
+        k_expand<<<eg, 256, 0, s>>>(b->r.get(), b->d_roff.get(), b->d_voff.get(), ng, compact.get(), 0);
+        GCG_LAUNCH_CHECK();
+        GCG_TRY(copy_out(out, compact.get(), (size_t)nreal * 4, s));
+    }
+    GCG_CUDA(cudaStreamSynchronize(s));
+    if (sweeps) memcpy(sweeps, hsw.data(), ng * 4);
+    if (residuals) memcpy(residuals, hres.data(), ng * 8);
+    if (stats) {
+        int mx = 0, conv = 1;
+        double worst = 0.0;
+        for (uint32_t g = 0; g < ng; ++g) {
+            mx = std::max(mx, hsw[g]);
+            worst = std::max(worst, hres[g]);
+            if (!(p->tol > 0.0 && hres[g] <= p->tol)) conv = 0;
+        }
+        stats->sweeps = mx;
+        stats->converged = conv;
+        stats->residual = worst;
+        stats->device_ms = ms;
+        stats->sweep_kernel_ms = ms;
+        stats->timed_sweeps = mx;
+        /* init (3), the persistent kernel, the scatter, and the layout maps */
+        stats->kernel_launches = 5 + (p->init_rank ? 1 : 0) + (out ? 1 : 0);
+    }
+    return GCG_OK;
+}
+
+}  // namespace gcg
+
+using namespace gcg;
+
+extern "C" {
+
+int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out) {
+    if (!graphs || !out) return fail(GCG_ERR_INVALID, "gcg_batch_create: null argument");
+    *out = nullptr;
+    if (ngraphs == 0 || ngraphs > NG_MAX)
+        return fail(GCG_ERR_INVALID, "gcg_batch_create: ngraphs must be 1.." + std::to_string(NG_MAX));
+    for (uint32_t g = 0; g < ngraphs; ++g)
+        if (!graphs[g]) return fail(GCG_ERR_INVALID, "gcg_batch_create: null graph");
+    gcg_batch *b = new gcg_batch();
+    int st = batch_build(graphs, ngraphs, b);
+    if (st != GCG_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return GCG_OK;
+}
+
+int gcg_batch_vertex_offsets(const gcg_batch *b, uint64_t *offsets) {
+    if (!b || !offsets) return fail(GCG_ERR_INVALID, "gcg_batch_vertex_offsets: null argument");
+    for (uint32_t g = 0; g <= b->ng; ++g) offsets[g] = b->roff[g];
+    return GCG_OK;
+}
+
+int gcg_batch_set_stream(gcg_batch *b, void *stream) {
+    if (!b) return fail(GCG_ERR_INVALID, "gcg_batch_set_stream: null batch");
+    b->u->stream = (cudaStream_t)stream;
+    return GCG_OK;
+}
+
+int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ranks, int32_t *sweeps,
+                       double *residuals, gcg_pr_stats *stats) {
+    if (!b || !params) return fail(GCG_ERR_INVALID, "gcg_batch_pagerank: null argument");
+    if (params->mode != GCG_PR_JACOBI || params->source != GCG_NO_SOURCE)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_pagerank: plain Jacobi only");
+    if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_batch_pagerank: max_sweeps < 0");
+    return batch_pagerank(b, params, out_ranks, sweeps, residuals, stats);
+}
+
+int gcg_batch_free(gcg_batch *b) {
+    if (!b) return GCG_OK;
+    cudaStreamSynchronize(b->u ? b->u->stream : 0);
+    delete b;
+    return GCG_OK;
+}
+
+}  // extern "C"

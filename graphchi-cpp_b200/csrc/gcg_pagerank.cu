@@ -33,37 +33,12 @@
 #include <vector>
 
 #include "gcg_internal.cuh"
+#include "gcg_pr_device.cuh"
 
 namespace gcg {
 
 namespace {
 
-constexpr int CH = 256;  /* edges per warp chunk */
-constexpr int EPL = 8;   /* edges per lane */
-
-/* ---- cache-policy loads --------------------------------------------------- */
-__device__ __forceinline__ uint64_t policy_evict_first() {
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint64_t policy_evict_last() {
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint4 ld_stream_v4(const uint32_t *p, uint64_t pol) {
-    uint4 r;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
-        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-        : "l"(p), "l"(pol));
-    return r;
-}
-__device__ __forceinline__ float ld_keep_f32(const float *p, uint64_t pol) {
-    float r;
-    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
-    return r;
-}
 
 /* ---- per-graph plan kernels -------------------------------------------- */
 __global__ void k_nonzero_flags(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t *__restrict__ f) {
@@ -123,151 +98,32 @@ __global__ void k_split_list(const uint32_t *__restrict__ nz_start, uint32_t nnz
     }
 }
 
-/* ---- sweep kernels ------------------------------------------------------ */
-struct SweepArgs {
-    /* graph / plan */
-    const uint32_t *col, *outdeg;
-    const uint8_t *heads;
-    const uint32_t *chunk_nz, *nz_rows, *zero_rows;
-    const uint4 *split;
-    uint64_t ne;
-    uint32_t nchunks, nnz, nzero, nsplit;
-    uint32_t hub; /* contribs of relabelled sources [0, hub) are cached in shared memory */
-    const uint32_t *nz_cidx, *zero_cidx; /* relabelled ids of the nz / zero rows */
-    /* state (contribs indexed by relabelled id) */
-    const float *c_old;
-    float *c_new;
-    const float *r_nz_old; /* ranks of the vertices with in-edges, compact (nz order) */
-    float *r_nz_new;
-    const uint32_t *od_nz; /* their out-degrees, compact */
-    const float *r_init;   /* full initial vector (residual of the first sweep) */
-    float *nzsum, *head_part, *tail_part;
-    double2 *block_res;
-    uint32_t *ticket;
-    int *done, *sweeps_done;
-    double *res_log, *last_res;
-    double teleport, damping, tol, norm_const;
-    uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
-};
 
-/* columns (streamed), head flags and starting row index of one chunk */
-template <typename A>
-__device__ __forceinline__ void load_chunk(const A &a, uint32_t ch, uint32_t lane, uint64_t pol, uint32_t (&col)[EPL],
-                                           uint32_t &flags, uint32_t &nvalid, uint32_t &base) {
-    const uint64_t e = (uint64_t)ch * CH + (uint64_t)EPL * lane;
-    nvalid = e < a.ne ? (uint32_t)((a.ne - e) < EPL ? (a.ne - e) : EPL) : 0u;
-    if (nvalid == EPL) {
-        uint4 x = ld_stream_v4(a.col + e, pol);
-        uint4 y = ld_stream_v4(a.col + e + 4, pol);
-        col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
-        col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
-    } else {
-#pragma unroll
-        for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
-    }
-    flags = nvalid ? (uint32_t)a.heads[e >> 3] : 0u;
-    base = a.chunk_nz[ch];
-}
 
-constexpr int EDGE_THREADS = 1024;
-constexpr uint32_t HUB_MAX = 49152; /* 192 KB of shared memory */
 
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     if (*(volatile const int *)a.done) return;
     extern __shared__ float s_hub[];
-    const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
     /* hub cache: contribs of the highest out-degree sources (relabelled 0..hub-1) */
-    {
-        const uint32_t n4 = a.hub >> 2;
-        const float4 *src4 = (const float4 *)a.c_old;
-        float4 *dst4 = (float4 *)s_hub;
-        for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
-        for (uint32_t i = (n4 << 2) + threadIdx.x; i < a.hub; i += blockDim.x) s_hub[i] = __ldcg(a.c_old + i);
-        __syncthreads();
-    }
+    load_hub(a, s_hub);
+    __syncthreads();
 
     /* Software pipeline: while a chunk's gathers are in flight, the next chunk's
      * columns, head flags and row base are already being loaded. */
     uint32_t ch = gwarp;
     uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
-    if (ch < a.nchunks) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base);
+    if (ch < a.nchunks) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
     for (; ch < a.nchunks; ch += nwarps) {
-        const uint64_t e0 = (uint64_t)ch * CH;
         float val[EPL];
-#pragma unroll
-        for (int j = 0; j < EPL; ++j) {
-            const uint32_t x = col[j];
-            val[j] = (uint32_t)j >= nvalid ? 0.0f : (x < a.hub ? s_hub[x] : ld_keep_f32(a.c_old + x, pol_keep));
-        }
+        gather_chunk(a, col, nvalid, s_hub, pol_keep, val);
         const uint32_t cur_flags = flags, cur_nvalid = nvalid, cur_base = base;
-        if (ch + nwarps < a.nchunks) load_chunk(a, ch + nwarps, lane, pol_stream, col, flags, nvalid, base);
-        {
-        const uint32_t flags = cur_flags, nvalid = cur_nvalid, base = cur_base;
-        const uint32_t head0 = __shfl_sync(FULL, flags, 0) & 1u;
-        const uint32_t nh_lane = __popc(flags);
-        uint32_t incl = nh_lane;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= (uint32_t)o) incl += y;
-        }
-        const uint32_t H = incl - nh_lane; /* heads in earlier lanes of this chunk */
-        const uint32_t Htot = __shfl_sync(FULL, incl, 31);
-        const uint32_t rowbase = base + (head0 ? 0u : 1u) + H; /* row started by this lane's first head */
-
-        /* in-lane segments: rows that start and end inside this lane are final */
-        float run = 0.0f, pre = 0.0f;
-        uint32_t nh = 0;
-#pragma unroll
-        for (int j = 0; j < EPL; ++j) {
-            if ((uint32_t)j < nvalid) {
-                if ((flags >> j) & 1u) {
-                    if (nh == 0) pre = run;
-                    else a.nzsum[rowbase + nh - 1] = run;
-                    ++nh;
-                    run = 0.0f;
-                }
-                run += val[j];
-            }
-        }
-        /* warp segmented inclusive scan of (lane has a head, lane tail sum) */
-        int finc = nh > 0;
-        float vinc = run;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int fu = __shfl_up_sync(FULL, finc, o);
-            float vu = __shfl_up_sync(FULL, vinc, o);
-            if (lane >= (uint32_t)o) {
-                if (!finc) vinc = vu + vinc;
-                finc |= fu;
-            }
-        }
-        const float prev = __shfl_up_sync(FULL, vinc, 1);
-        const float carry = lane ? prev : 0.0f;
-        if (nh > 0) {
-            /* the row that ends at this lane's first head */
-            const float s = carry + pre;
-            if (H == 0 && !head0) a.head_part[ch] = s;          /* began in an earlier chunk */
-            else if (!(lane == 0 && head0)) a.nzsum[rowbase - 1] = s; /* began in an earlier lane */
-        }
-        /* the chunk's last row */
-        const uint32_t L = (a.ne - e0 >= (uint64_t)CH) ? 31u : (uint32_t)((a.ne - 1 - e0) / EPL);
-        if (lane == L) {
-            if (Htot == 0) {
-                a.head_part[ch] = vinc; /* the whole chunk lies inside one row */
-            } else {
-                const bool ends_here = (e0 + CH >= a.ne) || (a.heads[(e0 + CH) >> 3] & 1u);
-                const uint32_t idx = base + (head0 ? 0u : 1u) + Htot - 1;
-                if (ends_here) a.nzsum[idx] = vinc;
-                else a.tail_part[ch] = vinc;
-            }
-        }
-        }
+        if (ch + nwarps < a.nchunks) load_chunk(a, ch + nwarps, lane, pol_stream, col, flags, nvalid, base, a.ne);
+        reduce_chunk(a, ch, lane, val, cur_flags, cur_nvalid, cur_base, a.ne);
     }
 }
 
@@ -308,11 +164,6 @@ __global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
     }
 }
 
-/* separate round-to-nearest multiply and add (no FMA contraction), as the
- * reference computes (float)(teleport + damping * (double)sum) */
-__device__ __forceinline__ float pr_value(const SweepArgs &a, float sum) {
-    return (float)__dadd_rn(a.teleport, __dmul_rn(a.damping, (double)sum));
-}
 /* personalised: the teleport term only at the source vertex */
 __device__ __forceinline__ float pr_value_at(const SweepArgs &a, float sum, uint32_t v) {
     const double tele = (a.source == GCG_NO_SOURCE || v == a.source) ? a.teleport : 0.0;
@@ -467,31 +318,21 @@ inline unsigned grid1d(uint64_t n, uint64_t cap_per_sm = 16) {
 }  // namespace
 
 /* ---- the chunk plan: built once per graph -------------------------------- */
-/* Sweep workspace of one graph, reused across calls. */
-struct PrWork {
-    dbuf<float> r, c, nzsum, parts, rnz;
-    dbuf<double2> bres;
-    dbuf<uint32_t> ctl;
-    dbuf<double> dres;
-    int *h_flags = nullptr; /* pinned: done flags copied back per chunk of sweeps */
-    ~PrWork() {
-        if (h_flags) cudaFreeHost(h_flags);
-    }
-};
-
-struct ChunkPlan {
-    PrWork work;
-    uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
-    dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
-    dbuf<uint4> split;
-    /* sources relabelled by out-degree (descending): col_r = newid[col] */
-    uint32_t hub = 0;
-    dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
-};
-
 void free_chunk_plan(ChunkPlan *p) { delete p; }
 
-static int ensure_chunk_plan(gcg_graph *g) {
+/* initial state of a sweep: full rank vector r, contributions c (relabelled,
+ * buffer 0) and the compact ranks of the vertices with in-edges (buffer 0) */
+int pr_init_state(gcg_graph *g, float init, const float *init_dev, float *r, float *c, float *rnz) {
+    const ChunkPlan &pl = *g->cplan;
+    cudaStream_t s = g->stream;
+    k_pr_init<<<grid1d(g->nv, 8), 256, 0, s>>>(g->nv, g->outdeg.get(), pl.newid.get(), init, init_dev, GCG_NO_SOURCE,
+                                               r, c);
+    k_pr_init_nz<<<grid1d(pl.nnz, 8), 256, 0, s>>>(pl.nnz, pl.nz_rows.get(), r, rnz);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
+int ensure_chunk_plan(gcg_graph *g) {
     if (g->cplan) return GCG_OK;
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;

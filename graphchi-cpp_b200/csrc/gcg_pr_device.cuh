@@ -1,0 +1,233 @@
+/*
+ * Device pieces of the Jacobi PageRank sweep shared by the single-graph engine
+ * (gcg_pagerank.cu) and the multi-graph persistent launch (gcg_multi.cu): the
+ * sweep arguments, cache-policy loads, the chunk loader, the hub-cache gather and
+ * the warp-level chunk reduction, and the apply formula.
+ */
+#ifndef GCG_PR_DEVICE_CUH
+#define GCG_PR_DEVICE_CUH
+
+#include "gcg_internal.cuh"
+
+namespace gcg {
+
+constexpr int CH = 256;  /* edges per warp chunk */
+constexpr int EPL = 8;   /* edges per lane */
+
+/* ---- cache-policy loads --------------------------------------------------- */
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint4 ld_stream_v4(const uint32_t *p, uint64_t pol) {
+    uint4 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
+__device__ __forceinline__ float ld_keep_f32(const float *p, uint64_t pol) {
+    float r;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
+    return r;
+}
+
+/* ---- sweep kernels ------------------------------------------------------ */
+struct SweepArgs {
+    /* graph / plan */
+    const uint32_t *col, *outdeg;
+    const uint8_t *heads;
+    const uint32_t *chunk_nz, *nz_rows, *zero_rows;
+    const uint4 *split;
+    uint64_t ne;
+    uint32_t nchunks, nnz, nzero, nsplit;
+    uint32_t hub; /* contribs of relabelled sources [0, hub) are cached in shared memory */
+    const uint32_t *nz_cidx, *zero_cidx; /* relabelled ids of the nz / zero rows */
+    /* state (contribs indexed by relabelled id) */
+    const float *c_old;
+    float *c_new;
+    const float *r_nz_old; /* ranks of the vertices with in-edges, compact (nz order) */
+    float *r_nz_new;
+    const uint32_t *od_nz; /* their out-degrees, compact */
+    const float *r_init;   /* full initial vector (residual of the first sweep) */
+    float *nzsum, *head_part, *tail_part;
+    double2 *block_res;
+    uint32_t *ticket;
+    int *done, *sweeps_done;
+    double *res_log, *last_res;
+    double teleport, damping, tol, norm_const;
+    uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
+};
+
+/* columns (streamed), head flags and starting row index of one chunk; ne is
+ * the end of the edge range being swept (positions at or beyond it are masked) */
+template <typename A>
+__device__ __forceinline__ void load_chunk(const A &a, uint32_t ch, uint32_t lane, uint64_t pol, uint32_t (&col)[EPL],
+                                           uint32_t &flags, uint32_t &nvalid, uint32_t &base, uint64_t ne) {
+    const uint64_t e = (uint64_t)ch * CH + (uint64_t)EPL * lane;
+    nvalid = e < ne ? (uint32_t)((ne - e) < EPL ? (ne - e) : EPL) : 0u;
+    if (nvalid == EPL) {
+        uint4 x = ld_stream_v4(a.col + e, pol);
+        uint4 y = ld_stream_v4(a.col + e + 4, pol);
+        col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
+        col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
+    }
+    flags = nvalid ? ((uint32_t)a.heads[e >> 3] & ((1u << nvalid) - 1u)) : 0u;
+    base = a.chunk_nz[ch];
+}
+
+/* L2-coherent load (no non-coherent texture path) for data that the same
+ * kernel launch rewrote before a grid barrier */
+__device__ __forceinline__ float ld_cg_keep_f32(const float *p, uint64_t pol) {
+    float r;
+    asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol) : "memory");
+    return r;
+}
+
+/* hub cache: contribs of the highest out-degree sources (relabelled 0..hub-1);
+ * the caller synchronises the block afterwards */
+template <typename A>
+__device__ __forceinline__ void load_hub(const A &a, float *s_hub) {
+    const uint32_t n4 = a.hub >> 2;
+    const float4 *src4 = (const float4 *)a.c_old;
+    float4 *dst4 = (float4 *)s_hub;
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
+    for (uint32_t i = (n4 << 2) + threadIdx.x; i < a.hub; i += blockDim.x) s_hub[i] = __ldcg(a.c_old + i);
+}
+
+/* contribs of a chunk's sources: hub sources from shared memory, the rest from
+ * L2/HBM (kept in L2). COHERENT selects loads that see writes made earlier in
+ * the same launch. */
+template <bool COHERENT = false, typename A>
+__device__ __forceinline__ void gather_chunk(const A &a, const uint32_t (&col)[EPL], uint32_t nvalid,
+                                             const float *s_hub, uint64_t pol_keep, float (&val)[EPL]) {
+#pragma unroll
+    for (int j = 0; j < EPL; ++j) {
+        const uint32_t x = col[j];
+        float v = 0.0f;
+        if ((uint32_t)j < nvalid) {
+            if (x < a.hub) v = s_hub[x];
+            else v = COHERENT ? ld_cg_keep_f32(a.c_old + x, pol_keep) : ld_keep_f32(a.c_old + x, pol_keep);
+        }
+        val[j] = v;
+    }
+}
+
+/* Warp reduction of one chunk into row sums. Rows that start and end inside the
+ * chunk are written to nzsum; a row that began in an earlier chunk leaves its
+ * part in head_part[ch], a row that continues into the next chunk leaves its
+ * part in tail_part[ch] (both completed in chunk order by the fix-up pass).
+ * ne is the end of the edge range being swept. */
+template <typename A>
+__device__ __forceinline__ void reduce_chunk(const A &a, uint32_t ch, uint32_t lane, const float (&val)[EPL],
+                                             uint32_t flags, uint32_t nvalid, uint32_t base, uint64_t ne) {
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint64_t e0 = (uint64_t)ch * CH;
+    const uint32_t head0 = __shfl_sync(FULL, flags, 0) & 1u;
+    const uint32_t nh_lane = __popc(flags);
+    uint32_t incl = nh_lane;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t H = incl - nh_lane; /* heads in earlier lanes of this chunk */
+    const uint32_t Htot = __shfl_sync(FULL, incl, 31);
+    const uint32_t rowbase = base + (head0 ? 0u : 1u) + H; /* row started by this lane's first head */
+
+    /* in-lane segments: rows that start and end inside this lane are final */
+    float run = 0.0f, pre = 0.0f;
+    uint32_t nh = 0;
+#pragma unroll
+    for (int j = 0; j < EPL; ++j) {
+        if ((uint32_t)j < nvalid) {
+            if ((flags >> j) & 1u) {
+                if (nh == 0) pre = run;
+                else a.nzsum[rowbase + nh - 1] = run;
+                ++nh;
+                run = 0.0f;
+            }
+            run += val[j];
+        }
+    }
+    /* warp segmented inclusive scan of (lane has a head, lane tail sum) */
+    int finc = nh > 0;
+    float vinc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int fu = __shfl_up_sync(FULL, finc, o);
+        float vu = __shfl_up_sync(FULL, vinc, o);
+        if (lane >= (uint32_t)o) {
+            if (!finc) vinc = vu + vinc;
+            finc |= fu;
+        }
+    }
+    const float prev = __shfl_up_sync(FULL, vinc, 1);
+    const float carry = lane ? prev : 0.0f;
+    if (nh > 0) {
+        /* the row that ends at this lane's first head */
+        const float s = carry + pre;
+        if (H == 0 && !head0) a.head_part[ch] = s;                /* began in an earlier chunk */
+        else if (!(lane == 0 && head0)) a.nzsum[rowbase - 1] = s; /* began in an earlier lane */
+    }
+    /* the chunk's last row */
+    const uint32_t L = (ne - e0 >= (uint64_t)CH) ? 31u : (uint32_t)((ne - 1 - e0) / EPL);
+    if (lane == L) {
+        if (Htot == 0) {
+            a.head_part[ch] = vinc; /* the whole chunk lies inside one row */
+        } else {
+            const bool ends_here = (e0 + CH >= ne) || (a.heads[(e0 + CH) >> 3] & 1u);
+            const uint32_t idx = base + (head0 ? 0u : 1u) + Htot - 1;
+            if (ends_here) a.nzsum[idx] = vinc;
+            else a.tail_part[ch] = vinc;
+        }
+    }
+}
+
+constexpr int EDGE_THREADS = 1024;
+constexpr uint32_t HUB_MAX = 49152; /* 192 KB of shared memory */
+
+/* Sweep workspace of one graph, reused across calls. */
+struct PrWork {
+    dbuf<float> r, c, nzsum, parts, rnz;
+    dbuf<double2> bres;
+    dbuf<uint32_t> ctl;
+    dbuf<double> dres;
+    int *h_flags = nullptr; /* pinned: done flags copied back per chunk of sweeps */
+    ~PrWork() {
+        if (h_flags) cudaFreeHost(h_flags);
+    }
+};
+
+struct ChunkPlan {
+    PrWork work;
+    uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
+    dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
+    dbuf<uint4> split;
+    /* sources relabelled by out-degree (descending): col_r = newid[col] */
+    uint32_t hub = 0;
+    dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
+};
+
+/* builds (once per graph) the chunk plan and the out-degree relabelling */
+int ensure_chunk_plan(gcg_graph *g);
+int pr_init_state(gcg_graph *g, float init, const float *init_dev, float *r, float *c, float *rnz);
+
+/* separate round-to-nearest multiply and add (no FMA contraction), as the
+ * reference computes (float)(teleport + damping * (double)sum) */
+__device__ __forceinline__ float pr_value(const SweepArgs &a, float sum) {
+    return (float)__dadd_rn(a.teleport, __dmul_rn(a.damping, (double)sum));
+}
+
+}  // namespace gcg
+
+#endif

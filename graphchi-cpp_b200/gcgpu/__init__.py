@@ -46,7 +46,9 @@ EXPORTED = [
     "gcg_pr_params_default", "gcg_pagerank", "gcg_connected_components", "gcg_triangle_count",
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
     "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
+    "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
 ]
+PR_TEST_BARRIER_TIMEOUT = 0x2
 NOALLOC_MAX_VERTICES = 1 << 20
 
 
@@ -114,6 +116,11 @@ _gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
 _pr_noalloc = _sig("gcg_pagerank_csr_noalloc", _i, _vp, _vp, _vp, _u32, C.POINTER(PrParams), _vp, _vp,
                    C.POINTER(PrStats))
 _ppr = _sig("gcg_ppr_batched", _i, _vp, _vp, _u32, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
+_batch_create = _sig("gcg_batch_create", _i, C.POINTER(_vp), _u32, C.POINTER(_vp))
+_batch_offsets = _sig("gcg_batch_vertex_offsets", _i, _vp, _vp)
+_batch_set_stream = _sig("gcg_batch_set_stream", _i, _vp, _vp)
+_batch_pagerank = _sig("gcg_batch_pagerank", _i, _vp, C.POINTER(PrParams), _vp, _vp, _vp, C.POINTER(PrStats))
+_batch_free = _sig("gcg_batch_free", _i, _vp)
 _last_error = _sig("gcg_last_error", C.c_char_p)
 _version = _sig("gcg_version", C.c_char_p)
 
@@ -335,3 +342,58 @@ def pagerank_csr_noalloc(in_rowptr, in_col, outdeg, out, num_vertices=None, max_
     st = PrStats()
     check(_pr_noalloc(ptr(in_rowptr), ptr(in_col), ptr(outdeg), n, C.byref(p), ptr(out), stream, C.byref(st)))
     return st
+
+
+class Batch:
+    """Many graphs solved by one persistent launch (gcg_batch_*)."""
+
+    def __init__(self, graphs):
+        arr = (_vp * len(graphs))(*[g.handle for g in graphs])
+        h = _vp()
+        check(_batch_create(arr, len(graphs), C.byref(h)))
+        self._h = h
+        self.ngraphs = len(graphs)
+        off = np.zeros(len(graphs) + 1, dtype=np.uint64)
+        check(_batch_offsets(h, ptr(off)))
+        self.offsets = off
+
+    def free(self):
+        if self._h:
+            _batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def set_stream(self, stream_ptr):
+        check(_batch_set_stream(self._h, stream_ptr))
+
+    def pagerank(self, max_sweeps=1000, teleport=0.15, damping=0.85, tol=0.0, init=1.0, init_rank=None, out=None,
+                 flags=0):
+        """Returns (ranks of all graphs concatenated, sweeps per graph, residual per graph, PrStats)."""
+        p = PrParams()
+        _pr_default(C.byref(p))
+        p.max_sweeps, p.teleport, p.damping, p.tol, p.init, p.flags = (max_sweeps, teleport, damping, tol, init,
+                                                                       flags)
+        if init_rank is not None:
+            init_rank = np.ascontiguousarray(init_rank, np.float32) if isinstance(init_rank, np.ndarray) else init_rank
+            p.init_rank = ptr(init_rank)
+        if out is None:
+            out = np.zeros(int(self.offsets[-1]), dtype=np.float32)
+        sweeps = np.zeros(self.ngraphs, dtype=np.int32)
+        res = np.zeros(self.ngraphs, dtype=np.float64)
+        st = PrStats()
+        check(_batch_pagerank(self._h, C.byref(p), ptr(out), ptr(sweeps), ptr(res), C.byref(st)))
+        return out, sweeps, res, st
+
+    def split(self, ranks):
+        return [ranks[int(self.offsets[g]):int(self.offsets[g + 1])] for g in range(self.ngraphs)]

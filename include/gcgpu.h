@@ -133,6 +133,10 @@ typedef struct {
 } gcg_pr_params;
 
 #define GCG_PR_TIME_SWEEPS 0x1u
+/* Test hook of gcg_batch_pagerank: the persistent kernel's grid barrier waits for
+ * one CTA that does not exist, so its bounded wait runs out and the call returns
+ * GCG_ERR_TIMEOUT (exercises the failure path without faulting the GPU). */
+#define GCG_PR_TEST_BARRIER_TIMEOUT 0x2u
 #define GCG_NO_SOURCE 0xFFFFFFFFu
 
 typedef struct {
@@ -171,6 +175,28 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * set) receives the per-sweep maximum residual. Sources run in groups of 256. */
 int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t nsources, const gcg_pr_params *params,
                     float *out, gcg_pr_stats *stats);
+
+/* ---- many graphs in one persistent launch -------------------------------- */
+
+/* A batch of independent graphs (the engine's addition: the reference runs one
+ * graph per engine, graphchi_engine.hpp:148). gcg_batch_create concatenates the
+ * graphs' in-edge CSRs into one block-diagonal union on the device (each graph
+ * is one interval of it); the graphs may be freed afterwards. Up to 1024 graphs,
+ * 2^32-1 vertices and edges in total. */
+typedef struct gcg_batch gcg_batch;
+int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out);
+/* First union vertex id of each graph (ngraphs+1 entries, last = total). */
+int gcg_batch_vertex_offsets(const gcg_batch *b, uint64_t *offsets);
+int gcg_batch_set_stream(gcg_batch *b, void *stream);
+/* Jacobi PageRank of every graph (the gcg_pagerank formula and stopping rule per
+ * graph) in ONE cooperative persistent kernel: sweeps proceed together, a graph
+ * leaves the device work queues when its own residual is <= tol. out_ranks: total
+ * vertices, graph g at its vertex offset; sweeps / residuals: per graph (may be
+ * NULL); params->init_rank (total vertices) may seed all graphs. Returns
+ * GCG_ERR_TIMEOUT if a bounded grid-barrier wait runs out. */
+int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ranks, int32_t *sweeps,
+                       double *residuals, gcg_pr_stats *stats);
+int gcg_batch_free(gcg_batch *b);
 
 /* No counterpart in the reference. PageRank (GCG_PR_JACOBI only) over an in-edge
  * CSR the caller already keeps in device memory, for callers that cannot let a

@@ -1,0 +1,74 @@
+"""Many graphs in one persistent launch (gcg_batch_pagerank) through the C ABI:
+each graph's ranks against its own single-graph solve, and the bounded
+grid-barrier wait (failure detection without a GPU fault)."""
+import numpy as np
+import pytest
+
+import gcgpu
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def make_graphs():
+    specs = [("rmat", 12, 1), ("er", 3000, 2), ("rmat", 9, 3), ("empty", 0, 0), ("er", 20000, 4),
+             ("rmat", 14, 5), ("er", 700, 6)]
+    gs = []
+    for kind, n, seed in specs:
+        if kind == "rmat":
+            s, d = O.rmat_numpy(n, 16 << n, seed=seed)
+        elif kind == "er":
+            s, d = O.er_numpy(n, 8 * n, seed=seed)
+        else:
+            s = d = np.zeros(0, np.uint32)
+        gs.append(gcgpu.Graph.from_edges(s, d, dedup=True))
+    return gs
+
+
+def test_batch_fixed_sweeps_equal_single_graph_solves():
+    gs = make_graphs()
+    with gcgpu.Batch(gs) as b:
+        r, sw, res, st = b.pagerank(max_sweeps=20, tol=0.0)
+        assert list(sw) == [20] * len(gs)
+        for g, part in zip(gs, b.split(r)):
+            ref, _ = g.pagerank(max_sweeps=20)
+            assert np.array_equal(part, ref)
+    for g in gs:
+        g.free()
+
+
+def test_batch_to_tolerance_matches_single_graph_solves():
+    gs = make_graphs()
+    with gcgpu.Batch(gs) as b:
+        r, sw, res, st = b.pagerank(max_sweeps=1000, tol=1e-8)
+        assert st.converged == 1 and np.all(res <= 1e-8)
+        for k, (g, part) in enumerate(zip(gs, b.split(r))):
+            ref, rst = g.pagerank(max_sweeps=1000, tol=1e-8)
+            assert abs(int(sw[k]) - rst.sweeps) <= 1, (k, sw[k], rst.sweeps)
+            if int(sw[k]) == rst.sweeps:
+                assert np.array_equal(part, ref)
+            else:
+                assert np.abs(part - ref).sum() / np.abs(ref).sum() <= 1e-6
+        # uneven sizes converge at different sweeps, all in one persistent launch:
+        # init (3), the persistent kernel, the scatter, the layout map to the output
+        assert st.kernel_launches == 6
+        # warm start from the answer: every graph stops within two sweeps
+        r2, sw2, res2, st2 = b.pagerank(max_sweeps=1000, tol=1e-8, init_rank=r)
+        assert np.all(sw2 <= 2) and np.all(res2 <= 1e-8)
+        assert st2.kernel_launches == 7
+    for g in gs:
+        g.free()
+
+
+def test_batch_barrier_timeout_is_reported_and_context_survives():
+    gs = make_graphs()[:3]
+    with gcgpu.Batch(gs) as b:
+        with pytest.raises(gcgpu.GcgError) as e:
+            b.pagerank(max_sweeps=5, flags=gcgpu.PR_TEST_BARRIER_TIMEOUT)
+        assert e.value.status == -7
+        r, sw, res, st = b.pagerank(max_sweeps=5)
+        assert list(sw) == [5, 5, 5]
+        ref, _ = gs[0].pagerank(max_sweeps=5)
+        assert np.array_equal(b.split(r)[0], ref)
+    for g in gs:
+        g.free()
