@@ -47,7 +47,13 @@ EXPORTED = [
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
     "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
+    "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
+    "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
+    "gcg_warm_start_rank",
 ]
+MLP_IN = 8
+MLP_HIDDEN = 64
+MLP_NPARAMS = 64 * 8 + 64 + 64 * 64 + 64 + 64 + 1
 PR_TEST_BARRIER_TIMEOUT = 0x2
 NOALLOC_MAX_VERTICES = 1 << 20
 
@@ -77,6 +83,11 @@ class PrStats(C.Structure):
     _fields_ = [("sweeps", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("device_ms", C.c_double), ("sweep_kernel_ms", C.c_double), ("timed_sweeps", C.c_int),
                 ("kernel_launches", C.c_int)]
+
+
+class MlpTrainParams(C.Structure):
+    _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64)]
 
 
 class CcStats(C.Structure):
@@ -121,6 +132,17 @@ _batch_offsets = _sig("gcg_batch_vertex_offsets", _i, _vp, _vp)
 _batch_set_stream = _sig("gcg_batch_set_stream", _i, _vp, _vp)
 _batch_pagerank = _sig("gcg_batch_pagerank", _i, _vp, C.POINTER(PrParams), _vp, _vp, _vp, C.POINTER(PrStats))
 _batch_free = _sig("gcg_batch_free", _i, _vp)
+_mlp_create = _sig("gcg_mlp_create", _i, _u64, C.POINTER(_vp))
+_mlp_free = _sig("gcg_mlp_free", _i, _vp)
+_mlp_get = _sig("gcg_mlp_get", _i, _vp, _vp, _vp)
+_mlp_set = _sig("gcg_mlp_set", _i, _vp, _vp, _vp)
+_mlp_fit_norm = _sig("gcg_mlp_fit_normalisation", _i, _vp, _vp, _u64)
+_warm_features = _sig("gcg_warm_features", _i, _vp, _vp)
+_mlp_forward = _sig("gcg_mlp_forward", _i, _vp, _vp, _u64, _vp)
+_mlp_gradient = _sig("gcg_mlp_gradient", _i, _vp, _vp, _vp, _u64, _vp, C.POINTER(C.c_double))
+_mlp_train_default = _sig("gcg_mlp_train_params_default", None, C.POINTER(MlpTrainParams))
+_mlp_train = _sig("gcg_mlp_train", _i, _vp, _vp, _vp, _u64, C.POINTER(MlpTrainParams), _vp)
+_warm_start = _sig("gcg_warm_start_rank", _i, _vp, _vp, C.c_double, C.c_double, _vp, C.POINTER(C.c_double))
 _last_error = _sig("gcg_last_error", C.c_char_p)
 _version = _sig("gcg_version", C.c_char_p)
 
@@ -278,6 +300,21 @@ class Graph:
         check(_ppr(self._h, ptr(src), k, C.byref(p), ptr(out), C.byref(st)))
         return out, st
 
+    def warm_features(self, out=None):
+        """(V, 8) float32 raw warm-start features (gcg_warm_features)."""
+        if out is None:
+            out = np.zeros((self.num_vertices, MLP_IN), dtype=np.float32)
+        check(_warm_features(self._h, ptr(out)))
+        return out
+
+    def warm_start_rank(self, mlp, teleport=0.15, damping=0.85, out=None):
+        """Learned initial ranks (gcg_warm_start_rank); returns (ranks, device ms)."""
+        if out is None:
+            out = np.zeros(self.num_vertices, dtype=np.float32)
+        ms = C.c_double(0.0)
+        check(_warm_start(self._h, mlp.handle, teleport, damping, ptr(out), C.byref(ms)))
+        return out, ms.value
+
     def connected_components(self, out=None):
         if out is None:
             out = np.zeros(self.num_vertices, dtype=np.uint32)
@@ -397,3 +434,97 @@ class Batch:
 
     def split(self, ranks):
         return [ranks[int(self.offsets[g]):int(self.offsets[g + 1])] for g in range(self.ngraphs)]
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32) if isinstance(a, np.ndarray) else a
+
+
+class Mlp:
+    """The warm-start network (gcg_mlp_*): FP32 master weights on the device."""
+
+    def __init__(self, seed=1):
+        h = _vp()
+        check(_mlp_create(seed, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if self._h:
+            _mlp_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+    def get(self):
+        """(params[MLP_NPARAMS], norm[16]) as float32 numpy arrays."""
+        p = np.zeros(MLP_NPARAMS, np.float32)
+        n = np.zeros(2 * MLP_IN, np.float32)
+        check(_mlp_get(self._h, ptr(p), ptr(n)))
+        return p, n
+
+    def set(self, params=None, norm=None):
+        params = None if params is None else np.ascontiguousarray(params, np.float32)
+        norm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        check(_mlp_set(self._h, ptr(params), ptr(norm)))
+
+    def fit_normalisation(self, x):
+        x = _f32(x)
+        check(_mlp_fit_norm(self._h, ptr(x), int(x.shape[0])))
+
+    def forward(self, x, out=None):
+        x = _f32(x)
+        n = int(x.shape[0])
+        if out is None:
+            out = np.zeros(n, np.float32)
+        check(_mlp_forward(self._h, ptr(x), n, ptr(out)))
+        return out
+
+    def gradient(self, x, t):
+        """(gradient of mean squared error, mean loss) over all samples."""
+        x, t = _f32(x), _f32(t)
+        g = np.zeros(MLP_NPARAMS, np.float32)
+        loss = C.c_double(0.0)
+        check(_mlp_gradient(self._h, ptr(x), ptr(t), int(x.shape[0]), ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, t, epochs=None, batch=None, lr=None, seed=None):
+        """Minibatch Adam; returns the mean training loss of each epoch."""
+        x, t = _f32(x), _f32(t)
+        p = MlpTrainParams()
+        _mlp_train_default(C.byref(p))
+        if epochs is not None:
+            p.epochs = epochs
+        if batch is not None:
+            p.batch = batch
+        if lr is not None:
+            p.lr = lr
+        if seed is not None:
+            p.seed = seed
+        losses = np.zeros(max(1, p.epochs), np.float32)
+        check(_mlp_train(self._h, ptr(x), ptr(t), int(x.shape[0]), C.byref(p), ptr(losses)))
+        return losses[: p.epochs]
+
+    def save(self, path):
+        p, n = self.get()
+        np.savez(path, params=p, norm=n)
+
+    @classmethod
+    def load(cls, path):
+        z = np.load(path)
+        m = cls(seed=0)
+        m.set(z["params"], z["norm"])
+        return m

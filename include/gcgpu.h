@@ -215,6 +215,74 @@ int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_t *in_col, 
                              uint32_t num_vertices, const gcg_pr_params *params, float *out_rank,
                              void *stream, gcg_pr_stats *stats);
 
+/* ---- learned warm start ------------------------------------------------- */
+
+/* No counterpart in the reference (its PageRank starts from a constant,
+ * example_apps/pagerank.cpp:80-85). A small MLP maps 8 per-vertex degree
+ * features to log(rank / teleport); exp of its output, times teleport, seeds the
+ * Jacobi iteration through gcg_pr_params.init_rank. The iteration then runs to
+ * the same residual as from the uniform start, so the answer keeps its accuracy.
+ *
+ * Features of vertex v (raw, before the model's normalisation), with
+ * L(u) = log(1 + indeg(u)):
+ *   0 log(1 + indeg v)        1 log(1 + outdeg v)
+ *   2 mean of L(u) over in-neighbours u (0 without in-edges)
+ *   3 max of L(u) over in-neighbours u (0 without in-edges)
+ *   4 log(1 + sum of indeg(u) over in-neighbours u)   (2-hop in-degree)
+ *   5 1 / outdeg v (0 without out-edges)
+ *   6, 7 bits B-1 and B-2 of v, B = bits of a vertex id (R-MAT quadrant bits)
+ *
+ * Network: x' = bf16((x - mean) * inv_std); h1 = bf16(relu(W1 x' + b1));
+ * h2 = relu(W2 h1 + b2); y = W3 . h2 + b3, with W1 (64x8), W2 (64x64), W3 (64)
+ * rounded to BF16 and every product summed in FP32. Parameters, flat FP32 in this
+ * order: W1 [64][8] (row = hidden unit), b1 [64], W2 [64][64] (row = output
+ * unit), b2 [64], W3 [64], b3 [1]. Training keeps FP32 master weights and runs
+ * Adam on the loss mean((y - target)^2), gradients passed straight through the
+ * BF16 roundings. */
+#define GCG_MLP_IN 8
+#define GCG_MLP_HIDDEN 64
+#define GCG_MLP_NPARAMS (64 * 8 + 64 + 64 * 64 + 64 + 64 + 1)
+typedef struct gcg_mlp gcg_mlp;
+
+typedef struct {
+    uint32_t epochs;     /* passes over the samples */
+    uint32_t batch;      /* samples per Adam step (multiple of 128) */
+    float lr, beta1, beta2, eps;
+    uint64_t seed;       /* sample order */
+} gcg_mlp_train_params;
+
+/* He-initialised weights (seeded), zero biases, identity normalisation. */
+int gcg_mlp_create(uint64_t seed, gcg_mlp **out);
+int gcg_mlp_free(gcg_mlp *m);
+/* params: GCG_MLP_NPARAMS floats; norm: 16 floats (mean[8], inv_std[8]); either may be NULL. */
+int gcg_mlp_get(const gcg_mlp *m, float *params, float *norm);
+int gcg_mlp_set(gcg_mlp *m, const float *params, const float *norm);
+/* Sets the normalisation from n samples (x: n x 8, row-major, host or device). */
+int gcg_mlp_fit_normalisation(gcg_mlp *m, const float *x, uint64_t n);
+/* Raw features of every vertex: features[v * 8 + i], host or device. */
+int gcg_warm_features(gcg_graph *g, float *features);
+/* Network output y for n samples (training kernel's forward, FP32 CUDA cores). */
+int gcg_mlp_forward(const gcg_mlp *m, const float *x, uint64_t n, float *y);
+/* Gradient of mean((y - t)^2) over n samples w.r.t. the parameters (the training
+ * kernels, without an update): grad GCG_MLP_NPARAMS floats; *loss the mean loss. */
+int gcg_mlp_gradient(const gcg_mlp *m, const float *x, const float *t, uint64_t n, float *grad, double *loss);
+/* Minibatch Adam over n samples; epoch_loss (epochs floats, may be NULL) receives
+ * the mean training loss of each epoch. */
+void gcg_mlp_train_params_default(gcg_mlp_train_params *p);
+int gcg_mlp_train(gcg_mlp *m, const float *x, const float *t, uint64_t n, const gcg_mlp_train_params *p,
+                  float *epoch_loss);
+/* The warm start: features and network fused on the device (tensor-core
+ * inference), p_v = teleport * exp(y_v) for a vertex with in-edges and exactly
+ * teleport for one without (its rank after any sweep). The predictions p are then
+ * scaled by one factor alpha chosen so that a Jacobi sweep keeps the total rank
+ * (with Z = vertices without in-edges, D = without out-edges, M = sum of p
+ * outside Z, M_D = its part on D: alpha = teleport*(n - (1-damping)|Z| -
+ * damping|Z&D|) / ((1-damping)M + damping M_D)); a per-graph bias of the network
+ * would otherwise excite the slowest mode of the iteration. init_rank:
+ * num_vertices, host or device. *device_ms (may be NULL) receives the device time. */
+int gcg_warm_start_rank(gcg_graph *g, const gcg_mlp *m, double teleport, double damping, float *init_rank,
+                        double *device_ms);
+
 /* ---- connected components ---------------------------------------------- */
 
 typedef struct {
