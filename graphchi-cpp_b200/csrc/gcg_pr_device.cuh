@@ -122,75 +122,100 @@ __device__ __forceinline__ void gather_chunk(const A &a, const uint32_t (&col)[E
     }
 }
 
-/* Warp reduction of one chunk into row sums. Rows that start and end inside the
+/* Value types of the chunk reduction: float (PageRank sums) and Agg3 (three
+ * channels: sum, max, sum). vadd is the reduction; for float it is the plain
+ * IEEE sum, so the PageRank instantiation computes exactly a + b. */
+struct Agg3 {
+    float s, m, t;
+};
+__device__ __forceinline__ float vzero(float) { return 0.0f; }
+__device__ __forceinline__ Agg3 vzero(Agg3) { return Agg3{0.0f, 0.0f, 0.0f}; }
+__device__ __forceinline__ float vadd(float x, float y) { return x + y; }
+__device__ __forceinline__ Agg3 vadd(Agg3 x, Agg3 y) { return Agg3{x.s + y.s, fmaxf(x.m, y.m), x.t + y.t}; }
+__device__ __forceinline__ float vshfl_up(float x, int o) { return __shfl_up_sync(0xFFFFFFFFu, x, o); }
+__device__ __forceinline__ Agg3 vshfl_up(Agg3 x, int o) {
+    return Agg3{__shfl_up_sync(0xFFFFFFFFu, x.s, o), __shfl_up_sync(0xFFFFFFFFu, x.m, o),
+                __shfl_up_sync(0xFFFFFFFFu, x.t, o)};
+}
+
+/* Warp reduction of one chunk into row values. Rows that start and end inside the
  * chunk are written to nzsum; a row that began in an earlier chunk leaves its
  * part in head_part[ch], a row that continues into the next chunk leaves its
  * part in tail_part[ch] (both completed in chunk order by the fix-up pass).
- * ne is the end of the edge range being swept. */
-template <typename A>
-__device__ __forceinline__ void reduce_chunk(const A &a, uint32_t ch, uint32_t lane, const float (&val)[EPL],
-                                             uint32_t flags, uint32_t nvalid, uint32_t base, uint64_t ne) {
+ * ne is the end of the edge range being swept. A supplies heads; R supplies
+ * nzsum, head_part and tail_part of value type V. */
+template <typename A, typename R, typename V>
+__device__ __forceinline__ void reduce_chunk_to(const A &a, const R &o, uint32_t ch, uint32_t lane,
+                                                const V (&val)[EPL], uint32_t flags, uint32_t nvalid, uint32_t base,
+                                                uint64_t ne) {
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint64_t e0 = (uint64_t)ch * CH;
     const uint32_t head0 = __shfl_sync(FULL, flags, 0) & 1u;
     const uint32_t nh_lane = __popc(flags);
     uint32_t incl = nh_lane;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(FULL, incl, o);
-        if (lane >= (uint32_t)o) incl += y;
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(FULL, incl, d);
+        if (lane >= (uint32_t)d) incl += y;
     }
     const uint32_t H = incl - nh_lane; /* heads in earlier lanes of this chunk */
     const uint32_t Htot = __shfl_sync(FULL, incl, 31);
     const uint32_t rowbase = base + (head0 ? 0u : 1u) + H; /* row started by this lane's first head */
 
     /* in-lane segments: rows that start and end inside this lane are final */
-    float run = 0.0f, pre = 0.0f;
+    const V zero = vzero(val[0]);
+    V run = zero, pre = zero;
     uint32_t nh = 0;
 #pragma unroll
     for (int j = 0; j < EPL; ++j) {
         if ((uint32_t)j < nvalid) {
             if ((flags >> j) & 1u) {
                 if (nh == 0) pre = run;
-                else a.nzsum[rowbase + nh - 1] = run;
+                else o.nzsum[rowbase + nh - 1] = run;
                 ++nh;
-                run = 0.0f;
+                run = zero;
             }
-            run += val[j];
+            run = vadd(run, val[j]);
         }
     }
-    /* warp segmented inclusive scan of (lane has a head, lane tail sum) */
+    /* warp segmented inclusive scan of (lane has a head, lane tail value) */
     int finc = nh > 0;
-    float vinc = run;
+    V vinc = run;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int fu = __shfl_up_sync(FULL, finc, o);
-        float vu = __shfl_up_sync(FULL, vinc, o);
-        if (lane >= (uint32_t)o) {
-            if (!finc) vinc = vu + vinc;
+    for (int d = 1; d < 32; d <<= 1) {
+        int fu = __shfl_up_sync(FULL, finc, d);
+        V vu = vshfl_up(vinc, d);
+        if (lane >= (uint32_t)d) {
+            if (!finc) vinc = vadd(vu, vinc);
             finc |= fu;
         }
     }
-    const float prev = __shfl_up_sync(FULL, vinc, 1);
-    const float carry = lane ? prev : 0.0f;
+    const V prev = vshfl_up(vinc, 1);
+    const V carry = lane ? prev : zero;
     if (nh > 0) {
         /* the row that ends at this lane's first head */
-        const float s = carry + pre;
-        if (H == 0 && !head0) a.head_part[ch] = s;                /* began in an earlier chunk */
-        else if (!(lane == 0 && head0)) a.nzsum[rowbase - 1] = s; /* began in an earlier lane */
+        const V sv = vadd(carry, pre);
+        if (H == 0 && !head0) o.head_part[ch] = sv;                /* began in an earlier chunk */
+        else if (!(lane == 0 && head0)) o.nzsum[rowbase - 1] = sv; /* began in an earlier lane */
     }
     /* the chunk's last row */
     const uint32_t L = (ne - e0 >= (uint64_t)CH) ? 31u : (uint32_t)((ne - 1 - e0) / EPL);
     if (lane == L) {
         if (Htot == 0) {
-            a.head_part[ch] = vinc; /* the whole chunk lies inside one row */
+            o.head_part[ch] = vinc; /* the whole chunk lies inside one row */
         } else {
             const bool ends_here = (e0 + CH >= ne) || (a.heads[(e0 + CH) >> 3] & 1u);
             const uint32_t idx = base + (head0 ? 0u : 1u) + Htot - 1;
-            if (ends_here) a.nzsum[idx] = vinc;
-            else a.tail_part[ch] = vinc;
+            if (ends_here) o.nzsum[idx] = vinc;
+            else o.tail_part[ch] = vinc;
         }
     }
+}
+
+template <typename A>
+__device__ __forceinline__ void reduce_chunk(const A &a, uint32_t ch, uint32_t lane, const float (&val)[EPL],
+                                             uint32_t flags, uint32_t nvalid, uint32_t base, uint64_t ne) {
+    reduce_chunk_to(a, a, ch, lane, val, flags, nvalid, base, ne);
 }
 
 constexpr int EDGE_THREADS = 1024;

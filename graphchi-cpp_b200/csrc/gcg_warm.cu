@@ -8,12 +8,18 @@
  * teleport * exp(y) then runs to the same residual as from the uniform start.
  *
  * Kernels
- *   k_warm_vstat   per vertex: {log(1+indeg), indeg} packed in 8 bytes
- *   k_warm_agg     per vertex with in-edges, 8 lanes per vertex: mean and max of
- *                  log(1+indeg(u)) over in-neighbours u and log(1 + sum indeg(u))
- *                  (one 8-byte gather per edge, FP64 sum, integer max and sum)
+ *   k_warm_vstat   per vertex: {log(1+indeg), indeg} packed in 8 bytes, stored at
+ *                  the vertex's out-degree rank (the PageRank relabelling)
+ *   k_warm_agg_edges / k_warm_agg_fix   per vertex with in-edges: sum and max of
+ *                  L(u) = log(1+indeg(u)) over in-neighbours u and the sum of
+ *                  indeg(u), on the PageRank chunk plan: one warp per 256 in-edges
+ *                  (edge-balanced whatever the degrees), one 8-byte gather per
+ *                  edge (the 24576 highest out-degree sources from shared memory),
+ *                  a warp segmented reduction of (sum, max, sum), rows crossing
+ *                  chunks completed in chunk order
  *   k_warm_infer   fused features + network on tensor cores (mma.sync m16n8k16,
- *                  BF16 operands, FP32 accumulation): a warp runs 16 vertices,
+ *                  BF16 operands, FP32 accumulation) over the vertices with
+ *                  in-edges (the others are set to teleport): a warp runs 16 vertices,
  *                  layer 1 as 8 MMAs (K = 8 features padded to 16), layer 2 as 32
  *                  MMAs with the layer-1 accumulators re-packed in registers as
  *                  the A operand, layer 3 and exp on the FP32 pipes
@@ -35,6 +41,7 @@
 #include <vector>
 
 #include "gcg_internal.cuh"
+#include "gcg_pr_device.cuh"
 
 namespace gcg {
 namespace {
@@ -68,77 +75,125 @@ __host__ __device__ __forceinline__ uint32_t bf16_bits(float x_rounded) {
 
 /* ---- features ------------------------------------------------------------ */
 
-__global__ void k_warm_vstat(const uint32_t *__restrict__ indeg, uint32_t nv, uint2 *__restrict__ vstat) {
+/* The in-neighbourhood aggregates run on the PageRank chunk plan: 256-edge warp
+ * chunks over the in-CSR with sources relabelled by out-degree, head bits for
+ * row starts, split rows completed in chunk order. Each edge contributes
+ * {L(u), L(u), indeg(u)} to its row's (sum, max, sum). */
+struct AggArgs {
+    const uint32_t *col; /* relabelled sources */
+    const uint8_t *heads;
+    const uint32_t *chunk_nz;
+    uint64_t ne;
+    uint32_t nchunks, hub;
+    const uint2 *vstat; /* {L(u) as float bits, indeg(u)} by relabelled id */
+};
+struct AggOut {
+    Agg3 *nzsum, *head_part, *tail_part;
+};
+constexpr uint32_t AGG_HUB_MAX = 24576; /* 192 KB of {L, indeg} pairs */
+
+__global__ void k_warm_vstat(const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ newid, uint32_t nv,
+                             uint2 *__restrict__ vstat) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         const uint32_t d = indeg[v];
-        const float L = (float)log1p((double)d);
-        vstat[v] = make_uint2(__float_as_uint(L), d);
+        vstat[newid[v]] = make_uint2(__float_as_uint(log1pf((float)d)), d);
     }
 }
 
-/* agg[v] = {mean L(u), log(1 + max indeg(u)), log(1 + sum indeg(u))} over in-neighbours u */
-__global__ void __launch_bounds__(256) k_warm_agg(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
-                                                  const uint2 *__restrict__ vstat, uint32_t nv,
-                                                  float4 *__restrict__ agg) {
-    const uint32_t sub = threadIdx.x & 7u;
-    const uint32_t grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const uint32_t ngrp = (gridDim.x * blockDim.x) >> 3;
-    /* every octet of a warp runs the same number of iterations (the shuffles are octet-local) */
-    for (uint32_t base = grp - (grp & 3u); base < nv; base += ngrp) {
-        const uint32_t v = base + (grp & 3u);
-        double s = 0.0;
-        uint32_t mx = 0;
-        unsigned long long tot = 0;
-        uint32_t b = 0, e = 0;
-        if (v < nv) {
-            b = rowptr[v];
-            e = rowptr[v + 1];
-        }
-        for (uint32_t i = b + sub; i < e; i += 8u) {
-            const uint2 x = vstat[col[i]];
-            s += (double)__uint_as_float(x.x);
-            mx = max(mx, x.y);
-            tot += x.y;
-        }
+__device__ __forceinline__ uint2 ld_keep_u2(const uint2 *p, uint64_t pol) {
+    uint2 r;
+    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;" : "=r"(r.x), "=r"(r.y) : "l"(p), "l"(pol));
+    return r;
+}
+
+__global__ void __launch_bounds__(EDGE_THREADS, 1) k_warm_agg_edges(AggArgs a, AggOut o) {
+    extern __shared__ uint2 s_vs[];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint64_t pol_stream = policy_evict_first(), pol_keep = policy_evict_last();
+    for (uint32_t i = threadIdx.x; i < a.hub; i += blockDim.x) s_vs[i] = a.vstat[i];
+    __syncthreads();
+    uint32_t ch = gwarp;
+    uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
+    if (ch < a.nchunks) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
+    for (; ch < a.nchunks; ch += nwarps) {
+        Agg3 val[EPL];
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
-            s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-            mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-            tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+        for (int j = 0; j < EPL; ++j) {
+            const uint32_t x = col[j];
+            uint2 w = make_uint2(0u, 0u);
+            if ((uint32_t)j < nvalid) w = x < a.hub ? s_vs[x] : ld_keep_u2(a.vstat + x, pol_keep);
+            const float L = __uint_as_float(w.x);
+            val[j] = Agg3{L, L, (float)w.y};
         }
-        if (sub == 0 && v < nv) {
-            const uint32_t d = e - b;
-            float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (d) {
-                r.x = (float)(s / (double)d);
-                r.y = (float)log1p((double)mx);
-                r.z = (float)log1p((double)tot);
-            }
-            agg[v] = r;
+        const uint32_t cf = flags, cn = nvalid, cb = base;
+        if (ch + nwarps < a.nchunks) load_chunk(a, ch + nwarps, lane, pol_stream, col, flags, nvalid, base, a.ne);
+        reduce_chunk_to(a, o, ch, lane, val, cf, cn, cb, a.ne);
+    }
+}
+
+/* rows crossing chunks, in chunk order (the order of the PageRank fix-up) */
+__global__ void __launch_bounds__(256) k_warm_agg_fix(const uint4 *__restrict__ split, uint32_t nsplit, AggOut o) {
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; wb < nsplit; wb += nwarps * 32u) {
+        const uint32_t k = wb + lane;
+        const bool valid = k < nsplit;
+        uint4 sp = make_uint4(0, 0, 0, 0);
+        if (valid) sp = split[k];
+        const bool lng = valid && (sp.z - sp.y) > 8u;
+        if (valid && !lng) {
+            Agg3 v = o.tail_part[sp.y];
+            for (uint32_t c = sp.y + 1; c <= sp.z; ++c) v = vadd(v, o.head_part[c]);
+            o.nzsum[sp.x] = v;
+        }
+        uint32_t m = __ballot_sync(FULL, lng);
+        while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t row = __shfl_sync(FULL, sp.x, src);
+            const uint32_t cs = __shfl_sync(FULL, sp.y, src);
+            const uint32_t ce = __shfl_sync(FULL, sp.z, src);
+            Agg3 v = Agg3{0.0f, 0.0f, 0.0f};
+            for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) v = vadd(v, o.head_part[c]);
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1)
+                v = vadd(v, Agg3{__shfl_xor_sync(FULL, v.s, d), __shfl_xor_sync(FULL, v.m, d),
+                                 __shfl_xor_sync(FULL, v.t, d)});
+            if (lane == 0) o.nzsum[row] = vadd(o.tail_part[cs], v);
         }
     }
 }
 
-/* the 8 raw features of vertex v */
-__device__ __forceinline__ void raw_features(uint32_t v, uint32_t din, uint32_t dout, float4 ag, uint32_t vbits,
-                                             float (&f)[NIN]) {
-    f[0] = (float)log1p((double)din);
-    f[1] = (float)log1p((double)dout);
-    f[2] = ag.x;
-    f[3] = ag.y;
-    f[4] = ag.z;
-    f[5] = dout ? (float)(1.0 / (double)dout) : 0.0f;
-    f[6] = vbits >= 1 ? (float)((v >> (vbits - 1)) & 1u) : 0.0f;
-    f[7] = vbits >= 2 ? (float)((v >> (vbits - 2)) & 1u) : 0.0f;
+/* raw feature k of vertex v (ag: its in-neighbourhood aggregates; zero without in-edges) */
+__device__ __forceinline__ float feature(int k, uint32_t v, uint32_t din, uint32_t dout, Agg3 ag, uint32_t vbits) {
+    switch (k) {
+        case 0: return log1pf((float)din);
+        case 1: return log1pf((float)dout);
+        case 2: return din ? ag.s / (float)din : 0.0f;
+        case 3: return din ? ag.m : 0.0f;
+        case 4: return din ? log1pf(ag.t) : 0.0f;
+        case 5: return dout ? 1.0f / (float)dout : 0.0f;
+        case 6: return vbits >= 1 ? (float)((v >> (vbits - 1)) & 1u) : 0.0f;
+        default: return vbits >= 2 ? (float)((v >> (vbits - 2)) & 1u) : 0.0f;
+    }
 }
 
-__global__ void k_warm_features(const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ outdeg,
-                                const float4 *__restrict__ agg, uint32_t nv, uint32_t vbits, float *__restrict__ out) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        float f[NIN];
-        raw_features(v, indeg[v], outdeg[v], agg[v], vbits, f);
+/* features of every vertex: nz rows from the aggregates, the others without */
+__global__ void k_warm_features(const uint32_t *__restrict__ nz_rows, uint32_t nnz,
+                                const uint32_t *__restrict__ zero_rows, uint32_t nzero,
+                                const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ outdeg,
+                                const Agg3 *__restrict__ agg, uint32_t vbits, float *__restrict__ out) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i < nnz + nzero; i += nth) {
+        const bool nz = i < nnz;
+        const uint32_t v = nz ? nz_rows[i] : zero_rows[i - nnz];
+        const Agg3 ag = nz ? agg[i] : Agg3{0.0f, 0.0f, 0.0f};
+        const uint32_t din = nz ? indeg[v] : 0u, dout = outdeg[v];
 #pragma unroll
-        for (int i = 0; i < NIN; ++i) out[(size_t)v * NIN + i] = f[i];
+        for (int k = 0; k < NIN; ++k) out[(size_t)v * NIN + k] = feature(k, v, din, dout, ag, vbits);
     }
 }
 
@@ -146,6 +201,25 @@ __global__ void k_warm_features(const uint32_t *__restrict__ indeg, const uint32
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return bf16_bits(lo) | (bf16_bits(hi) << 16);
+}
+
+/* normalised BF16 inputs of the vertices with in-edges, 16 bytes per row: word t
+ * holds features 2t and 2t+1, exactly the layer-1 A-operand word of lane t */
+__global__ void k_warm_xfeat(const uint32_t *__restrict__ nz_rows, const uint32_t *__restrict__ od_nz, uint32_t nnz,
+                             const uint32_t *__restrict__ indeg, const Agg3 *__restrict__ agg, uint32_t vbits,
+                             const float *__restrict__ norm, uint4 *__restrict__ xpk) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        const uint32_t v = nz_rows[i], din = indeg[v], dout = od_nz[i];
+        const Agg3 ag = agg[i];
+        uint32_t w[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float f0 = (feature(2 * t, v, din, dout, ag, vbits) - norm[2 * t]) * norm[NIN + 2 * t];
+            const float f1 = (feature(2 * t + 1, v, din, dout, ag, vbits) - norm[2 * t + 1]) * norm[NIN + 2 * t + 1];
+            w[t] = pack_bf16(bf16r(f0), bf16r(f1));
+        }
+        xpk[i] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
 }
 
 /* D += A (16x16, row) * B (16x8, col), BF16 operands, FP32 accumulation */
@@ -159,25 +233,25 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
 }
 
 struct InferArgs {
-    const uint32_t *indeg, *outdeg;
-    const float4 *agg;
-    uint32_t nv, vbits;
+    const uint32_t *nz_rows, *od_nz;
+    const uint32_t *xpk;           /* per nz row: 4 words of packed BF16 inputs */
+    uint32_t nnz;
     const uint32_t *frag1, *frag2; /* B operand fragments, lane-major */
     const float *wb;               /* rounded weights (biases FP32) */
     const float *norm;             /* mean[8], inv_std[8] */
     float teleport;
     float *out;
     double2 *part_mass;            /* per block: sum of the predicted ranks, of those without out-edges */
-    ulonglong2 *part_count;        /* per block: vertices without in-edges, of those also without out-edges */
 };
 
 constexpr int INFER_THREADS = 256;
 
-/* one warp = 16 vertices per step; lane (g = lane/4, t = lane%4) holds rows g and
- * g+8 of every accumulator tile (the m16n8 C layout), which is also the A layout
- * of the next layer once two adjacent n-tiles are packed to BF16 pairs */
+/* one warp = 16 vertices with in-edges per step; lane (g = lane/4, t = lane%4)
+ * holds rows g and g+8 of every accumulator tile (the m16n8 C layout), which is
+ * also the A layout of the next layer once two adjacent n-tiles are packed to
+ * BF16 pairs. Lane t computes features 2t and 2t+1 of its two rows: exactly its
+ * part of the layer-1 A operand. */
 __global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
-    __shared__ float s_x[INFER_THREADS / 32][16][NIN + 1];
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t g = lane >> 2, t = lane & 3u;
@@ -203,61 +277,37 @@ __global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
             B2[ks][nt][1] = f.y;
         }
     const float b3 = a.wb[OB3];
-    float mean[NIN], istd[NIN];
-#pragma unroll
-    for (int i = 0; i < NIN; ++i) {
-        mean[i] = a.norm[i];
-        istd[i] = a.norm[NIN + i];
-    }
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t ntiles = (a.nv + 15u) >> 4;
+    const uint32_t ntiles = (a.nnz + 15u) >> 4;
     double msum = 0.0, mdang = 0.0;
-    unsigned long long cz = 0, czd = 0;
+    /* inputs of the next tile are loaded while the current one computes */
+    uint32_t nx[2] = {0u, 0u}, nv_[2] = {0u, 0u}, nd[2] = {1u, 1u};
+    auto load_tile = [&](uint32_t tile) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const uint32_t i = (tile << 4) + g + 8 * q;
+            nx[q] = 0u;
+            nv_[q] = 0u;
+            nd[q] = 1u;
+            if (tile < ntiles && i < a.nnz) {
+                nx[q] = a.xpk[(size_t)i * 4 + t];
+                nv_[q] = a.nz_rows[i];
+                nd[q] = a.od_nz[i];
+            }
+        }
+    };
+    load_tile(gwarp);
     for (uint32_t tile = gwarp; tile < ntiles; tile += nwarps) {
-        const uint32_t v0 = tile << 4;
-        uint32_t din = 0, dout = 0;
-        if (lane < 16) {
-            const uint32_t v = v0 + lane;
-            float f[NIN];
-            if (v < a.nv) {
-                din = a.indeg[v];
-                dout = a.outdeg[v];
-                raw_features(v, din, dout, a.agg[v], a.vbits, f);
-            } else {
-#pragma unroll
-                for (int i = 0; i < NIN; ++i) f[i] = 0.0f;
-            }
-#pragma unroll
-            for (int i = 0; i < NIN; ++i) s_x[warp][lane][i] = bf16r((f[i] - mean[i]) * istd[i]);
-        }
-        const uint32_t din_g = __shfl_sync(FULL, din, g), din_g8 = __shfl_sync(FULL, din, g + 8);
-        const uint32_t dout_g = __shfl_sync(FULL, dout, g), dout_g8 = __shfl_sync(FULL, dout, g + 8);
-        if (__ballot_sync(FULL, din != 0) == 0) { /* no vertex of the tile has in-edges */
-            if (t == 0) {
-                if (v0 + g < a.nv) {
-                    a.out[v0 + g] = a.teleport;
-                    ++cz;
-                    czd += dout_g == 0;
-                }
-                if (v0 + g + 8 < a.nv) {
-                    a.out[v0 + g + 8] = a.teleport;
-                    ++cz;
-                    czd += dout_g8 == 0;
-                }
-            }
-            __syncwarp();
-            continue;
-        }
-        __syncwarp();
-        const uint32_t x0 = pack_bf16(s_x[warp][g][2 * t], s_x[warp][g][2 * t + 1]);
-        const uint32_t x1 = pack_bf16(s_x[warp][g + 8][2 * t], s_x[warp][g + 8][2 * t + 1]);
+        const uint32_t i0 = tile << 4;
+        const uint32_t xw[2] = {nx[0], nx[1]}, vq[2] = {nv_[0], nv_[1]}, dq[2] = {nd[0], nd[1]};
+        load_tile(tile + nwarps);
         /* layer 1 -> A operand of layer 2 */
         uint32_t A2[4][4];
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
             float c[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_bf16(c, x0, x1, 0u, 0u, B1[nt], 0u);
+            mma_bf16(c, xw[0], xw[1], 0u, 0u, B1[nt], 0u);
             const float h0 = bf16r(fmaxf(c[0] + bias1[nt][0], 0.0f));
             const float h1 = bf16r(fmaxf(c[1] + bias1[nt][1], 0.0f));
             const float h2 = bf16r(fmaxf(c[2] + bias1[nt][0], 0.0f));
@@ -271,7 +321,8 @@ __global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
         for (int nt = 0; nt < 8; ++nt) {
             float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks) mma_bf16(d, A2[ks][0], A2[ks][1], A2[ks][2], A2[ks][3], B2[ks][nt][0], B2[ks][nt][1]);
+            for (int ks = 0; ks < 4; ++ks)
+                mma_bf16(d, A2[ks][0], A2[ks][1], A2[ks][2], A2[ks][3], B2[ks][nt][0], B2[ks][nt][1]);
             yg = fmaf(fmaxf(d[0] + bias2[nt][0], 0.0f), w3[nt][0], yg);
             yg = fmaf(fmaxf(d[1] + bias2[nt][1], 0.0f), w3[nt][1], yg);
             yg8 = fmaf(fmaxf(d[2] + bias2[nt][0], 0.0f), w3[nt][0], yg8);
@@ -282,55 +333,59 @@ __global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
         yg8 += __shfl_xor_sync(FULL, yg8, 1);
         yg8 += __shfl_xor_sync(FULL, yg8, 2);
         if (t == 0) {
-            /* y is clamped so exp stays finite */
             const float y2[2] = {yg, yg8};
-            const uint32_t di[2] = {din_g, din_g8}, dd[2] = {dout_g, dout_g8};
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                const uint32_t v = v0 + g + 8 * q;
-                if (v >= a.nv) continue;
-                if (di[q]) {
-                    const float r = a.teleport * expf(fminf(fmaxf(y2[q] + b3, -30.0f), 30.0f));
-                    a.out[v] = r;
-                    msum += (double)r;
-                    if (dd[q] == 0) mdang += (double)r;
-                } else {
-                    a.out[v] = a.teleport;
-                    ++cz;
-                    czd += dd[q] == 0;
-                }
+                if (i0 + g + 8 * q >= a.nnz) continue;
+                /* y is clamped so exp stays finite */
+                const float r = a.teleport * expf(fminf(fmaxf(y2[q] + b3, -30.0f), 30.0f));
+                a.out[vq[q]] = r;
+                msum += (double)r;
+                if (dq[q] == 0) mdang += (double)r;
             }
         }
-        __syncwarp();
     }
     /* block partials of the mass terms, reduced in a fixed order */
     __shared__ double s_m[INFER_THREADS / 32][2];
-    __shared__ unsigned long long s_c[INFER_THREADS / 32][2];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         msum += __shfl_xor_sync(FULL, msum, o);
         mdang += __shfl_xor_sync(FULL, mdang, o);
-        cz += __shfl_xor_sync(FULL, cz, o);
-        czd += __shfl_xor_sync(FULL, czd, o);
     }
     if (lane == 0) {
         s_m[warp][0] = msum;
         s_m[warp][1] = mdang;
-        s_c[warp][0] = cz;
-        s_c[warp][1] = czd;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double2 m = make_double2(0.0, 0.0);
-        ulonglong2 c = make_ulonglong2(0, 0);
         for (int w = 0; w < INFER_THREADS / 32; ++w) {
             m.x += s_m[w][0];
             m.y += s_m[w][1];
-            c.x += s_c[w][0];
-            c.y += s_c[w][1];
         }
         a.part_mass[blockIdx.x] = m;
-        a.part_count[blockIdx.x] = c;
+    }
+}
+
+/* vertices without in-edges: exactly teleport; per block, how many also lack out-edges */
+__global__ void __launch_bounds__(256) k_warm_zero(const uint32_t *__restrict__ zero_rows, uint32_t nzero,
+                                                   const uint32_t *__restrict__ outdeg, float teleport,
+                                                   float *__restrict__ out, uint32_t *__restrict__ part_zd) {
+    __shared__ uint32_t s_c[8];
+    uint32_t c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nzero; i += gridDim.x * blockDim.x) {
+        const uint32_t v = zero_rows[i];
+        out[v] = teleport;
+        c += outdeg[v] == 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31u) == 0) s_c[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_c[w];
+        part_zd[blockIdx.x] = tot;
     }
 }
 
@@ -340,36 +395,37 @@ __global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
  * and M_D = the part of M on D, the sweep's total is teleport*n +
  * damping*(total - total on D), which equals the total when
  *   alpha = teleport*(n - (1-damping)|Z| - damping|Z & D|) / ((1-damping)M + damping M_D). */
-__global__ void k_warm_alpha(const double2 *__restrict__ pm, const ulonglong2 *__restrict__ pc, uint32_t nblocks,
-                             uint32_t nv, double teleport, double damping, double *__restrict__ alpha) {
+__global__ void k_warm_alpha(const double2 *__restrict__ pm, uint32_t nmass, const uint32_t *__restrict__ pzd,
+                             uint32_t nzd, uint32_t nv, uint32_t nzero, double teleport, double damping,
+                             double *__restrict__ alpha) {
     const uint32_t lane = threadIdx.x;
     double M = 0.0, MD = 0.0;
-    unsigned long long z = 0, zd = 0;
-    for (uint32_t b = lane; b < nblocks; b += 32u) {
+    unsigned long long zd = 0;
+    for (uint32_t b = lane; b < nmass; b += 32u) {
         M += pm[b].x;
         MD += pm[b].y;
-        z += pc[b].x;
-        zd += pc[b].y;
     }
+    for (uint32_t b = lane; b < nzd; b += 32u) zd += pzd[b];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         M += __shfl_xor_sync(0xFFFFFFFFu, M, o);
         MD += __shfl_xor_sync(0xFFFFFFFFu, MD, o);
-        z += __shfl_xor_sync(0xFFFFFFFFu, z, o);
         zd += __shfl_xor_sync(0xFFFFFFFFu, zd, o);
     }
     if (lane == 0) {
         const double den = (1.0 - damping) * M + damping * MD;
-        const double num = teleport * ((double)nv - (1.0 - damping) * (double)z - damping * (double)zd);
+        const double num = teleport * ((double)nv - (1.0 - damping) * (double)nzero - damping * (double)zd);
         *alpha = (den > 0.0 && num > 0.0) ? num / den : 1.0;
     }
 }
 
-__global__ void k_warm_scale(const uint32_t *__restrict__ indeg, uint32_t nv, const double *__restrict__ alpha,
+__global__ void k_warm_scale(const uint32_t *__restrict__ nz_rows, uint32_t nnz, const double *__restrict__ alpha,
                              float *__restrict__ out) {
     const double al = *alpha;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        if (indeg[v]) out[v] = (float)((double)out[v] * al);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        const uint32_t v = nz_rows[i];
+        out[v] = (float)((double)out[v] * al);
+    }
 }
 
 /* B operand fragments of layers 1 and 2 from the rounded weights */
@@ -627,17 +683,43 @@ int set_train_smem() {
     return GCG_OK;
 }
 
-/* per-vertex aggregates of the in-neighbourhood (features 2-4) */
-int warm_aggregates(gcg_graph *g, tbuf<float4> &agg, cudaStream_t s) {
+/* per-nz-row aggregates of the in-neighbourhood (features 2-4), on the chunk plan */
+int warm_aggregates(gcg_graph *g, tbuf<Agg3> &agg, cudaStream_t s) {
+    GCG_TRY(ensure_chunk_plan(g));
+    const ChunkPlan &pl = *g->cplan;
     const uint32_t nv = g->nv;
     tbuf<uint2> vstat;
+    tbuf<Agg3> parts;
     GCG_TRY(vstat.alloc(nv, s));
-    GCG_TRY(agg.alloc(nv, s));
+    GCG_TRY(agg.alloc(std::max<uint32_t>(pl.nnz, 1), s));
+    GCG_TRY(parts.alloc((size_t)2 * pl.nchunks + 2, s));
     const int sms = num_sms();
     const unsigned b1 = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, sms * 8ull));
-    k_warm_vstat<<<b1, 256, 0, s>>>(g->indeg.get(), nv, vstat.get());
-    const unsigned b2 = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 31) / 32, sms * 8ull));
-    k_warm_agg<<<b2, 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), vstat.get(), nv, agg.get());
+    k_warm_vstat<<<b1, 256, 0, s>>>(g->indeg.get(), pl.newid.get(), nv, vstat.get());
+    if (pl.nchunks) {
+        AggArgs a;
+        a.col = pl.col_r.get();
+        a.heads = (const uint8_t *)pl.head_bits.get();
+        a.chunk_nz = pl.chunk_nz.get();
+        a.ne = g->ne;
+        a.nchunks = pl.nchunks;
+        a.hub = std::min<uint32_t>(nv, AGG_HUB_MAX);
+        a.vstat = vstat.get();
+        AggOut o;
+        o.nzsum = agg.get();
+        o.head_part = parts.get();
+        o.tail_part = parts.get() + pl.nchunks + 1;
+        const size_t smem = (size_t)AGG_HUB_MAX * sizeof(uint2);
+        GCG_CUDA(cudaFuncSetAttribute(k_warm_agg_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const unsigned grid = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>(((uint64_t)pl.nchunks * 32 + EDGE_THREADS - 1) / EDGE_THREADS, (uint64_t)sms));
+        k_warm_agg_edges<<<grid, EDGE_THREADS, (size_t)a.hub * sizeof(uint2), s>>>(a, o);
+        if (pl.nsplit) {
+            const unsigned fb = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>(((uint64_t)pl.nsplit + 255) / 256, sms * 8ull));
+            k_warm_agg_fix<<<fb, 256, 0, s>>>(pl.split.get(), pl.nsplit, o);
+        }
+    }
     GCG_LAUNCH_CHECK();
     return GCG_OK;
 }
@@ -744,8 +826,9 @@ int gcg_warm_features(gcg_graph *g, float *features) {
     if (!g || !features) return fail(GCG_ERR_INVALID, "gcg_warm_features: null argument");
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
-    tbuf<float4> agg;
+    tbuf<Agg3> agg;
     GCG_TRY(warm_aggregates(g, agg, s));
+    const ChunkPlan &pl = *g->cplan;
     tbuf<float> stage;
     float *dst = features;
     const bool dev = is_device_ptr(features);
@@ -754,7 +837,8 @@ int gcg_warm_features(gcg_graph *g, float *features) {
         dst = stage.get();
     }
     const unsigned b = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, num_sms() * 8ull));
-    k_warm_features<<<b, 256, 0, s>>>(g->indeg.get(), g->outdeg.get(), agg.get(), nv, g->vbits, dst);
+    k_warm_features<<<b, 256, 0, s>>>(pl.nz_rows.get(), pl.nnz, pl.zero_rows.get(), pl.nzero, g->indeg.get(),
+                                      g->outdeg.get(), agg.get(), g->vbits, dst);
     GCG_LAUNCH_CHECK();
     if (!dev) GCG_TRY(copy_out(features, dst, (size_t)nv * NIN * 4, s));
     GCG_CUDA(cudaStreamSynchronize(s));
@@ -934,52 +1018,56 @@ int gcg_warm_start_rank(gcg_graph *g, const gcg_mlp *m, double teleport, double 
     if (!(damping >= 0.0 && damping < 1.0)) return fail(GCG_ERR_INVALID, "gcg_warm_start_rank: damping must be in [0, 1)");
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
+    GCG_TRY(ensure_chunk_plan(g)); /* shared with PageRank; built once per graph */
     cudaEvent_t ev0, ev1;
     GCG_CUDA(cudaEventCreate(&ev0));
     GCG_CUDA(cudaEventCreate(&ev1));
     GCG_CUDA(cudaEventRecord(ev0, s));
     int rc = GCG_OK;
     {
-        tbuf<float4> agg;
+        const ChunkPlan &pl = *g->cplan;
+        const int sms = num_sms();
+        tbuf<Agg3> agg;
         tbuf<float> stage;
         tbuf<double2> pmass;
-        tbuf<ulonglong2> pcount;
+        tbuf<uint32_t> pzd;
         tbuf<double> alpha;
+        tbuf<uint4> xpk;
         float *dst = init_rank;
         const bool dev = is_device_ptr(init_rank);
+        const uint64_t tiles = ((uint64_t)pl.nnz + 15) / 16;
+        const unsigned ib = (unsigned)std::max<uint64_t>(
+            1, std::min<uint64_t>((tiles + INFER_THREADS / 32 - 1) / (INFER_THREADS / 32), sms * 2ull));
+        const unsigned zb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)pl.nzero + 255) / 256, sms * 4ull));
         rc = warm_aggregates(g, agg, s);
         if (rc == GCG_OK && !dev) {
             rc = stage.alloc(nv, s);
             dst = stage.get();
         }
-        if (rc == GCG_OK) {
+        if (rc == GCG_OK && (rc = pmass.alloc(ib, s)) == GCG_OK && (rc = pzd.alloc(zb, s)) == GCG_OK &&
+            (rc = alpha.alloc(1, s)) == GCG_OK && (rc = xpk.alloc(std::max<uint32_t>(pl.nnz, 1), s)) == GCG_OK) {
+            const unsigned xb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)pl.nnz + 255) / 256, sms * 8ull));
+            k_warm_xfeat<<<xb, 256, 0, s>>>(pl.nz_rows.get(), pl.od_nz.get(), pl.nnz, g->indeg.get(), agg.get(),
+                                            g->vbits, m->norm.get(), xpk.get());
             InferArgs a;
-            a.indeg = g->indeg.get();
-            a.outdeg = g->outdeg.get();
-            a.agg = agg.get();
-            a.nv = nv;
-            a.vbits = g->vbits;
+            a.nz_rows = pl.nz_rows.get();
+            a.od_nz = pl.od_nz.get();
+            a.xpk = (const uint32_t *)xpk.get();
+            a.nnz = pl.nnz;
             a.frag1 = m->frag.get();
             a.frag2 = m->frag.get() + NFRAG1;
             a.wb = m->wb.get();
             a.norm = m->norm.get();
             a.teleport = (float)teleport;
             a.out = dst;
-            const uint64_t warps = ((uint64_t)nv + 15) / 16;
-            const unsigned blocks = (unsigned)std::max<uint64_t>(
-                1, std::min<uint64_t>((warps + INFER_THREADS / 32 - 1) / (INFER_THREADS / 32), num_sms() * 2ull));
-            if ((rc = pmass.alloc(blocks, s)) == GCG_OK && (rc = pcount.alloc(blocks, s)) == GCG_OK &&
-                (rc = alpha.alloc(1, s)) == GCG_OK) {
-                a.part_mass = pmass.get();
-                a.part_count = pcount.get();
-                k_warm_infer<<<blocks, INFER_THREADS, 0, s>>>(a);
-                k_warm_alpha<<<1, 32, 0, s>>>(pmass.get(), pcount.get(), blocks, nv, teleport, damping, alpha.get());
-                const unsigned sb = (unsigned)std::max<uint64_t>(
-                    1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, num_sms() * 8ull));
-                k_warm_scale<<<sb, 256, 0, s>>>(g->indeg.get(), nv, alpha.get(), dst);
-            }
-        }
-        if (rc == GCG_OK) {
+            a.part_mass = pmass.get();
+            k_warm_infer<<<ib, INFER_THREADS, 0, s>>>(a);
+            k_warm_zero<<<zb, 256, 0, s>>>(pl.zero_rows.get(), pl.nzero, g->outdeg.get(), (float)teleport, dst,
+                                           pzd.get());
+            k_warm_alpha<<<1, 32, 0, s>>>(pmass.get(), ib, pzd.get(), zb, nv, pl.nzero, teleport, damping,
+                                          alpha.get());
+            const unsigned sb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)pl.nnz + 255) / 256, sms * 8ull));
+            k_warm_scale<<<sb, 256, 0, s>>>(pl.nz_rows.get(), pl.nnz, alpha.get(), dst);
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = fail(GCG_ERR_CUDA, std::string("gcg_warm_start_rank: ") + cudaGetErrorString(e));
         }

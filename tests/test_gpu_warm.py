@@ -3,7 +3,8 @@ forward pass and gradient, and the tensor-core inference, each against the
 numpy oracle (oracle/warm_oracle.py); then training on the GPU and what the trained
 network gains over the uniform start at the same residual.
 
-Tolerances: features rtol 1e-6 (FP64 sums in another order, then float);
+Tolerances: features rtol 2e-5 (the device sums in FP32 in chunk order, the
+oracle in FP64; the network sees the features rounded to BF16, 4e-3 relative);
 forward |dy| <= 2e-3 (FP32 sums in another order can move a hidden value across
 a BF16 rounding boundary); gradient relative L2 error <= 1e-2 per parameter block
 (same cause); PageRank answers from the two starts within normalised L1 1e-6."""
@@ -41,13 +42,13 @@ def test_features_vs_oracle():
     with g:
         f = g.warm_features()
     assert f.shape == f_ref.shape
-    assert np.allclose(f, f_ref, rtol=1e-6, atol=1e-7)
+    assert np.allclose(f, f_ref, rtol=2e-5, atol=1e-6)
     # an Erdos-Renyi graph with isolated vertices, and a tiny graph
     s, d = O.er_numpy(3000, 6000, seed=4)
     with gcgpu.Graph.from_edges(s, d, dedup=True) as g2:
         rp, col = g2.csr(gcgpu.CSR_IN)
         ref = W.features(g2.num_vertices, rp, col, g2.degrees()[:, 1])
-        assert np.allclose(g2.warm_features(), ref, rtol=1e-6, atol=1e-7)
+        assert np.allclose(g2.warm_features(), ref, rtol=2e-5, atol=1e-6)
 
 
 def test_forward_and_gradient_vs_oracle():
