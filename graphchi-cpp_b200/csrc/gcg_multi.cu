@@ -10,12 +10,13 @@
  * gcg_batch_pagerank runs every sweep of every graph inside ONE cooperative
  * persistent kernel (one 1024-thread CTA per SM). Per sweep, four phases split by
  * a grid barrier:
- *   A  edges: warps pull 256-edge chunks of the still-active graphs from a device
- *      work queue (atomic counter over the concatenated chunk ranges) and run the
- *      same gather / warp reduction as the single-graph kernel;
+ *   A  edges: warps stride over the 256-edge chunks of the still-active graphs
+ *      (their concatenated chunk ranges; equal-sized chunks need no queue) and run
+ *      the same pipelined gather / warp reduction as the single-graph kernel;
  *   B  rows crossing chunks: partials added in chunk order;
- *   C  vertices: CTAs pull 1024-row tiles of the active graphs from a second
- *      queue, apply, and write one FP64 residual partial per tile (fixed slot);
+ *   C  vertices: CTAs pull 1024-row tiles of the active graphs from a device work
+ *      queue (atomic counter), apply, and write one FP64 residual partial per tile
+ *      (fixed slot);
  *   D  one warp per graph adds its tile partials in a fixed order; a graph whose
  *      residual is <= tol (or that reached max_sweeps) leaves the queues.
  * The kernel ends when no graph is active. Each graph's ranks are formed with the
@@ -157,27 +158,39 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         a.r_nz_old = m.rnz[sweep & 1];
         a.r_nz_new = m.rnz[(sweep + 1) & 1];
         const int const_pass = sweep < 2;
-        uint32_t *qA = m.qctr + 2 * (sweep & 1), *qC = qA + 1;
+        uint32_t *qC = m.qctr + 2 * (sweep & 1) + 1;
 
-        /* ---- A: edge chunks of the active graphs (work queue) ---- */
+        /* ---- A: edge chunks of the active graphs, grid-strided over their
+         *         concatenation (chunks are equal-sized), loads one chunk ahead ---- */
         uint32_t nact = 0;
         const uint32_t totA = active_prefix(m, 0, s_pref, &nact);
         if (nact == 0) break; /* every graph has stopped: the same answer in every CTA */
         load_hub(a, s_hub);
         __syncthreads();
-        for (;;) {
-            uint32_t item = 0;
-            if (lane == 0) item = atomicAdd(qA, 1u);
-            item = __shfl_sync(FULL, item, 0);
-            if (item >= totA) break;
-            const uint32_t g = find_graph(s_pref, m.ng, item);
-            const uint32_t ch = m.gr[g].cs + (item - s_pref[g]);
-            uint32_t col[EPL], flags, nvalid, base;
-            const uint64_t gend = m.gr[g].gend;
-            load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
-            float val[EPL];
-            gather_chunk<true>(a, col, nvalid, s_hub, pol_keep, val);
-            reduce_chunk(a, ch, lane, val, flags, nvalid, base, gend);
+        {
+            uint32_t item = gwarp;
+            uint32_t col[EPL], flags = 0, nvalid = 0, base = 0, ch = 0;
+            uint64_t gend = 0;
+            if (item < totA) {
+                const uint32_t g = find_graph(s_pref, m.ng, item);
+                ch = m.gr[g].cs + (item - s_pref[g]);
+                gend = m.gr[g].gend;
+                load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
+            }
+            for (; item < totA; item += nwarps) {
+                float val[EPL];
+                gather_chunk<true>(a, col, nvalid, s_hub, pol_keep, val);
+                const uint32_t cch = ch, cf = flags, cn = nvalid, cb = base;
+                const uint64_t cend = gend;
+                if (item + nwarps < totA) {
+                    const uint32_t nx = item + nwarps;
+                    const uint32_t g = find_graph(s_pref, m.ng, nx);
+                    ch = m.gr[g].cs + (nx - s_pref[g]);
+                    gend = m.gr[g].gend;
+                    load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
+                }
+                reduce_chunk(a, cch, lane, val, cf, cn, cb, cend);
+            }
         }
         if (!grid_sync(m, gen)) return;
 

@@ -167,12 +167,16 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * one-vector runs of example_apps/pagerank.cpp): nsources sources solved together
  * as a vertex-major rank matrix. For source s: r_s starts at the indicator of
  * sources[s]; each sweep r_s[v] = (float)(params->teleport*[v == sources[s]] +
- * params->damping * sum_{u->v} r_s[u]/outdeg[u]) (float contributions and sums);
- * stops after max_sweeps or when the largest per-source normalised L1 change
- * (FP64) is <= params->tol. mode must be GCG_PR_JACOBI, init_rank NULL and source
- * GCG_NO_SOURCE. sources: nsources ids, host or device. out: num_vertices x
- * nsources floats, out[v * nsources + s], host or device. params->residuals (if
- * set) receives the per-sweep maximum residual. Sources run in groups of 256. */
+ * params->damping * sum_{u->v} r_s[u]/outdeg[u]) (float contributions and sums).
+ * Each source stops on its own, as gcg_pagerank with params->source would: after
+ * its first sweep whose normalised L1 change (FP64) is <= params->tol, or after
+ * max_sweeps. Finished sources leave the matrix (it is compacted to the next
+ * narrower width when the rest fit), so late sweeps gather shorter rows.
+ * mode must be GCG_PR_JACOBI, init_rank NULL and source GCG_NO_SOURCE.
+ * sources: nsources ids, host or device. out: num_vertices x nsources floats,
+ * out[v * nsources + s], host or device. params->residuals (if set) receives the
+ * per-sweep maximum residual of the sources still iterating. stats->sweeps is
+ * the largest per-source count. Sources run in groups of 256. */
 int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t nsources, const gcg_pr_params *params,
                     float *out, gcg_pr_stats *stats);
 

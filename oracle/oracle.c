@@ -343,6 +343,7 @@ int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
     float *acc = (float *)malloc((size_t)k * sizeof(float));
     double *dsum = (double *)malloc((size_t)k * sizeof(double));
     double *nsum = (double *)malloc((size_t)k * sizeof(double));
+    int *frozen = (int *)calloc(k, sizeof(int)); /* a source stops after its own first sweep <= tol */
     for (uint32_t s = 0; s < k; ++s) r[(size_t)sources[s] * k + s] = 1.0f;
     int sweeps = 0;
     for (int it = 0; it < max_sweeps; ++it) {
@@ -357,6 +358,7 @@ int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
                 for (uint32_t s = 0; s < k; ++s) acc[s] += cu[s];
             }
             for (uint32_t s = 0; s < k; ++s) {
+                if (frozen[s]) continue;
                 double tele = (sources[s] == v) ? (1.0 - damping) : 0.0;
                 float x = (float)(tele + damping * (double)acc[s]);
                 float *rv = r + (size_t)v * k + s;
@@ -366,14 +368,17 @@ int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
             }
         }
         ++sweeps;
-        double worst = 0;
+        int active = 0;
         for (uint32_t s = 0; s < k; ++s) {
+            if (frozen[s]) continue;
             double q = nsum[s] > 0 ? dsum[s] / nsum[s] : 0.0;
-            if (q > worst) worst = q;
+            if (tol > 0 && q <= tol) frozen[s] = 1;
+            else ++active;
         }
-        if (tol > 0 && worst <= tol) break;
+        if (active == 0) break;
     }
     memcpy(out, r, n * sizeof(float));
+    free(frozen);
     free(r); free(c); free(acc); free(dsum); free(nsum);
     return sweeps;
 }

@@ -93,9 +93,9 @@ uint64_t orc_tc(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
  * of the batched GPU path): r_s starts at e_s; each sweep
  * r_s[v] = (float)((1-damping)*[v==s] + damping*(double)sum_{u->v} c_s[u]) with
  * c_s[u] = r_s[u]/outdeg[u] in float and the float sum in ascending source order.
- * Stops after the first sweep where max over sources of
- * sum|new-old|/sum|new| <= tol, or after max_sweeps. out is vertex-major
- * (out[v*k + s]). Returns the number of sweeps. */
+ * Each source stops (its column is frozen) after its own first sweep where
+ * sum|new-old|/sum|new| <= tol; all stop after max_sweeps. out is vertex-major
+ * (out[v*k + s]). Returns the number of sweeps of the slowest source. */
 int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
             const uint32_t *outdeg, const uint32_t *sources, uint32_t k, double damping,
             int max_sweeps, double tol, float *out);
