@@ -19,7 +19,10 @@
  *      (fixed slot);
  *   D  one warp per graph adds its tile partials in a fixed order; a graph whose
  *      residual is <= tol (or that reached max_sweeps) leaves the queues.
- * The kernel ends when no graph is active. Each graph's ranks are formed with the
+ * The kernel ends when no graph is active. A whole solve (state init, initial
+ * vector, the persistent kernel, rank assembly) is captured once into a CUDA
+ * graph per parameter set and replayed; gcg_batch_autotune picks the hub-cache
+ * size and the edge phase's work distribution by timing the candidates. Each graph's ranks are formed with the
  * same sums in the same order as its single-graph solve (only the FP64 residual
  * is reduced in a different order). Contributions change between
  * sweeps inside the kernel, so they are read with L2-coherent loads, never the
@@ -70,6 +73,8 @@ struct MultiArgs {
     int *err;
     long long spin_limit;
     uint32_t extra_arrivals; /* test hook: the barrier waits for this many more CTAs */
+    uint32_t grab;           /* edge phase: 0 = warps stride over the chunks; g > 0 = warps take runs
+                                of g chunks from a device work queue (an autotuned choice) */
 };
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
@@ -168,27 +173,39 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         load_hub(a, s_hub);
         __syncthreads();
         {
-            uint32_t item = gwarp;
+            /* runs of chunks: [item, item_end) is this warp's current run; the
+             * next chunk is loaded while the current one is gathered */
+            const uint32_t run = m.grab ? m.grab : 1u;
+            uint32_t item, item_end;
+            auto next_run = [&](uint32_t &it, uint32_t &end) {
+                if (m.grab) {
+                    uint32_t x = 0;
+                    if (lane == 0) x = atomicAdd(m.qctr + 2 * (sweep & 1), run);
+                    it = __shfl_sync(FULL, x, 0);
+                } else {
+                    it = (it == 0xFFFFFFFFu) ? gwarp : it + nwarps - 1u; /* it was incremented past its run of 1 */
+                }
+                end = it < totA ? (totA - it < run ? totA : it + run) : it;
+            };
+            item = 0xFFFFFFFFu;
+            next_run(item, item_end);
             uint32_t col[EPL], flags = 0, nvalid = 0, base = 0, ch = 0;
             uint64_t gend = 0;
-            if (item < totA) {
-                const uint32_t g = find_graph(s_pref, m.ng, item);
-                ch = m.gr[g].cs + (item - s_pref[g]);
+            auto load_item = [&](uint32_t it) {
+                const uint32_t g = find_graph(s_pref, m.ng, it);
+                ch = m.gr[g].cs + (it - s_pref[g]);
                 gend = m.gr[g].gend;
                 load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
-            }
-            for (; item < totA; item += nwarps) {
+            };
+            if (item < item_end) load_item(item);
+            while (item < item_end) {
                 float val[EPL];
                 gather_chunk<true>(a, col, nvalid, s_hub, pol_keep, val);
                 const uint32_t cch = ch, cf = flags, cn = nvalid, cb = base;
                 const uint64_t cend = gend;
-                if (item + nwarps < totA) {
-                    const uint32_t nx = item + nwarps;
-                    const uint32_t g = find_graph(s_pref, m.ng, nx);
-                    ch = m.gr[g].cs + (nx - s_pref[g]);
-                    gend = m.gr[g].gend;
-                    load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
-                }
+                ++item;
+                if (item >= item_end) next_run(item, item_end);
+                if (item < item_end) load_item(item);
                 reduce_chunk(a, cch, lane, val, cf, cn, cb, cend);
             }
         }
@@ -378,6 +395,25 @@ __global__ void k_pad(uint32_t pv, uint32_t pe0, uint32_t pe1, uint32_t *__restr
     for (uint32_t e = pe0 + tid; e < pe1; e += nth) ucol[e] = pv;
 }
 
+/* per-graph state at the start of a solve (on the device, so a whole solve can be
+ * captured in a CUDA graph): all graphs active, counters clear, and the rank mass
+ * of the vertices without in-edges (constant after the first sweep) */
+__global__ void k_multi_init(const GRange *__restrict__ gr, uint32_t ng, double teleport,
+                             double *__restrict__ norm_const, int *__restrict__ active, int *__restrict__ gsweeps,
+                             double *__restrict__ gres, int *__restrict__ err, uint32_t *__restrict__ qctr,
+                             uint32_t *__restrict__ bar) {
+    const double t = fabs((double)(float)teleport);
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        norm_const[g] = (double)(gr[g].ze - gr[g].zs) * t;
+        active[g] = 1;
+        gsweeps[g] = 0;
+        gres[g] = 0.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 4) qctr[threadIdx.x] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x < 2) bar[threadIdx.x] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
+}
+
 /* graph g's vertices keep their order at union offset voff[g]; map both ways */
 __global__ void k_expand(const float *__restrict__ src, const uint32_t *__restrict__ roff, const uint32_t *__restrict__ voff,
                          uint32_t ng, float *__restrict__ dst, int to_union) {
@@ -438,7 +474,25 @@ struct gcg_batch {
     gcg::dbuf<double> norm_const, gres;
     gcg::dbuf<int> active, gsweeps, err;
     gcg::dbuf<uint32_t> qctr, bar;
-    ~gcg_batch() { delete u; }
+    gcg::dbuf<float> rout; /* ranks in the callers' layout */
+    /* launch configuration (gcg_batch_autotune): shared-memory hub entries
+     * (UINT32_MAX = the plan's), edge-phase queue run length (0 = strided) */
+    uint32_t tune_hub = 0xFFFFFFFFu, tune_grab = 0;
+    /* the captured solve, replayed while the parameters stay the same */
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_unsupported = false;
+    double key_t = 0, key_d = 0, key_tol = 0;
+    int key_ms = -1;
+    float key_init = 0;
+    uint32_t key_hub = 0, key_grab = 0;
+    /* the batch's own stream (capturable), used until the caller sets one; it
+     * waits for the legacy default stream at the start of every solve */
+    cudaStream_t own = nullptr;
+    ~gcg_batch() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        delete u;
+        if (own) cudaStreamDestroy(own);
+    }
 };
 
 namespace gcg {
@@ -546,13 +600,60 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
     return GCG_OK;
 }
 
+/* Enqueues one whole solve on the batch stream: per-graph state, initial vector,
+ * the cooperative persistent kernel, the rank assembly and the map to the
+ * callers' layout. Stream-ordered only (no host synchronisation), so it can be
+ * captured into a CUDA graph. */
+static int enqueue_solve(gcg_batch *b, MultiArgs &m, const gcg_pr_params *p, const float *init_dev, unsigned grid,
+                         uint32_t hub_bytes) {
+    gcg_graph *u = b->u;
+    const ChunkPlan &pl = *u->cplan;
+    const uint32_t ng = b->ng, nv = u->nv, nreal = b->roff[ng];
+    cudaStream_t s = u->stream;
+    k_multi_init<<<(ng + 255) / 256, 256, 0, s>>>(b->gr.get(), ng, p->teleport, b->norm_const.get(), b->active.get(),
+                                                  b->gsweeps.get(), b->gres.get(), b->err.get(), b->qctr.get(),
+                                                  b->bar.get());
+    GCG_TRY(pr_init_state(u, p->init, init_dev, b->r.get(), b->c.get(), b->rnz.get()));
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(EDGE_THREADS);
+    cfg.dynamicSmemBytes = hub_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t le = cudaLaunchKernelEx(&cfg, k_multi_pagerank, m);
+    if (le != cudaSuccess)
+        return fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: cooperative launch: ") + cudaGetErrorString(le));
+    dim3 sg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv / ng + 255) / 256, 64)),
+            std::min<uint32_t>(ng, 1024));
+    k_multi_scatter<<<sg, 256, 0, s>>>(b->gr.get(), ng, b->gsweeps.get(), pl.nz_rows.get(), pl.zero_rows.get(),
+                                       m.rnz[0], m.rnz[1], (float)p->teleport, b->r.get());
+    const dim3 eg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nreal / ng + 255) / 256, 64)),
+                  std::min<uint32_t>(ng, 1024));
+    k_expand<<<eg, 256, 0, s>>>(b->r.get(), b->d_roff.get(), b->d_voff.get(), ng, b->rout.get(), 0);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
 static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int32_t *sweeps, double *residuals,
-                          gcg_pr_stats *stats) {
+                          gcg_pr_stats *stats, bool allow_graph = true) {
     gcg_graph *u = b->u;
     const ChunkPlan &pl = *u->cplan;
     const uint32_t nv = u->nv, ng = b->ng;
     cudaStream_t s = u->stream;
+    if (s == b->own && s) { /* order after work the caller queued on the legacy default stream */
+        cudaEvent_t ev;
+        GCG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, 0);
+        cudaStreamWaitEvent(s, ev, 0);
+        cudaEventDestroy(ev);
+    }
     const size_t cstride = ((size_t)nv + 63) & ~(size_t)63;
+    const uint32_t nreal = b->roff[ng];
     if (!b->c.get()) {
         GCG_TRY(b->c.alloc(2 * cstride));
         GCG_TRY(b->rnz.alloc((size_t)2 * std::max<uint32_t>(pl.nnz, 1)));
@@ -567,41 +668,11 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
         GCG_TRY(b->err.alloc(1));
         GCG_TRY(b->qctr.alloc(4));
         GCG_TRY(b->bar.alloc(2));
+        GCG_TRY(b->rout.alloc(std::max<uint32_t>(nreal, 1)));
     }
-    /* initial state */
-    const uint32_t nreal = b->roff[ng];
-    const dim3 eg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nreal / ng + 255) / 256, 64)),
-                  std::min<uint32_t>(ng, 1024));
-    tbuf<float> init_stage, init_union;
-    const float *init_dev = nullptr;
-    if (p->init_rank) { /* caller layout (no padding) -> union layout; padding vertices get 0 */
-        const float *src = p->init_rank;
-        if (!is_device_ptr(p->init_rank)) {
-            GCG_TRY(init_stage.alloc(nreal, s));
-            GCG_TRY(copy_in(init_stage.get(), p->init_rank, (size_t)nreal * 4, s));
-            src = init_stage.get();
-        }
-        GCG_TRY(init_union.alloc(nv, s));
-        GCG_CUDA(cudaMemsetAsync(init_union.get(), 0, (size_t)nv * 4, s));
-        k_expand<<<eg, 256, 0, s>>>(src, b->d_roff.get(), b->d_voff.get(), ng, init_union.get(), 1);
-        init_dev = init_union.get();
-    }
-    GCG_TRY(pr_init_state(u, p->init, init_dev, b->r.get(), b->c.get(), b->rnz.get()));
-    std::vector<double> nc(ng);
-    std::vector<int> act(ng, 1);
-    for (uint32_t g = 0; g < ng; ++g)
-        nc[g] = (double)(b->gr_host[g].ze - b->gr_host[g].zs) * fabs((double)(float)p->teleport);
-    GCG_CUDA(cudaMemcpyAsync(b->norm_const.get(), nc.data(), ng * 8, cudaMemcpyHostToDevice, s));
-    GCG_CUDA(cudaMemcpyAsync(b->active.get(), act.data(), ng * 4, cudaMemcpyHostToDevice, s));
-    GCG_CUDA(cudaMemsetAsync(b->gsweeps.get(), 0, ng * 4, s));
-    GCG_CUDA(cudaMemsetAsync(b->gres.get(), 0, ng * 8, s));
-    GCG_CUDA(cudaMemsetAsync(b->err.get(), 0, 4, s));
-    GCG_CUDA(cudaMemsetAsync(b->qctr.get(), 0, 16, s));
-    GCG_CUDA(cudaMemsetAsync(b->bar.get(), 0, 8, s));
-
     MultiArgs m;
     SweepArgs &a = m.a;
-    memset(&a, 0, sizeof(a));
+    memset(&m, 0, sizeof(m));
     a.col = pl.col_r.get();
     a.outdeg = u->outdeg.get();
     a.heads = (const uint8_t *)pl.head_bits.get();
@@ -614,7 +685,7 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
     a.nnz = pl.nnz;
     a.nzero = pl.nzero;
     a.nsplit = pl.nsplit;
-    a.hub = pl.hub;
+    a.hub = std::min(pl.hub, b->tune_hub);
     a.nz_cidx = pl.nz_cidx.get();
     a.zero_cidx = pl.zero_cidx.get();
     a.od_nz = pl.od_nz.get();
@@ -644,55 +715,99 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
     const bool test_timeout = (p->flags & GCG_PR_TEST_BARRIER_TIMEOUT) != 0;
     m.spin_limit = test_timeout ? (1ll << 14) : (1ll << 25);
     m.extra_arrivals = test_timeout ? 1u : 0u;
+    m.grab = b->tune_grab;
 
     /* one cooperative launch: one CTA per SM, all resident */
-    const uint32_t hub_bytes = pl.hub * 4u;
+    const uint32_t hub_bytes = a.hub * 4u;
     GCG_CUDA(cudaFuncSetAttribute(k_multi_pagerank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4)));
     int per_sm = 0;
     GCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multi_pagerank, EDGE_THREADS, hub_bytes));
     if (per_sm < 1) return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_pagerank: persistent kernel does not fit an SM");
     const unsigned grid = (unsigned)num_sms();
+
+    /* initial vector given: caller layout (no padding) -> union layout, padding 0 */
+    tbuf<float> init_stage, init_union;
+    const float *init_dev = nullptr;
+    if (p->init_rank) {
+        const float *src = p->init_rank;
+        if (!is_device_ptr(p->init_rank)) {
+            GCG_TRY(init_stage.alloc(nreal, s));
+            GCG_TRY(copy_in(init_stage.get(), p->init_rank, (size_t)nreal * 4, s));
+            src = init_stage.get();
+        }
+        GCG_TRY(init_union.alloc(nv, s));
+        GCG_CUDA(cudaMemsetAsync(init_union.get(), 0, (size_t)nv * 4, s));
+        const dim3 eg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nreal / ng + 255) / 256, 64)),
+                      std::min<uint32_t>(ng, 1024));
+        k_expand<<<eg, 256, 0, s>>>(src, b->d_roff.get(), b->d_voff.get(), ng, init_union.get(), 1);
+        init_dev = init_union.get();
+    }
+
+    /* the whole solve as a CUDA graph, captured once per parameter set */
+    bool use_graph = allow_graph && !p->init_rank && !test_timeout && !b->graph_unsupported;
+    if (use_graph) {
+        const bool same = b->gexec && b->key_t == p->teleport && b->key_d == p->damping && b->key_tol == p->tol &&
+                          b->key_ms == p->max_sweeps && b->key_init == p->init && b->key_hub == a.hub &&
+                          b->key_grab == m.grab;
+        if (!same) {
+            if (b->gexec) cudaGraphExecDestroy(b->gexec);
+            b->gexec = nullptr;
+            cudaGraph_t graph = nullptr;
+            int rc = GCG_OK;
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                rc = GCG_ERR_CUDA;
+            } else {
+                rc = enqueue_solve(b, m, p, nullptr, grid, hub_bytes);
+                if (cudaStreamEndCapture(s, &graph) != cudaSuccess) rc = GCG_ERR_CUDA;
+            }
+            if (rc == GCG_OK && cudaGraphInstantiate(&b->gexec, graph, 0) != cudaSuccess) rc = GCG_ERR_CUDA;
+            if (graph) cudaGraphDestroy(graph);
+            if (rc != GCG_OK) { /* this runtime cannot capture the solve: launch it directly from now on */
+                cudaGetLastError();
+                if (b->gexec) cudaGraphExecDestroy(b->gexec);
+                b->gexec = nullptr;
+                b->graph_unsupported = true;
+                use_graph = false;
+            } else {
+                b->key_t = p->teleport;
+                b->key_d = p->damping;
+                b->key_tol = p->tol;
+                b->key_ms = p->max_sweeps;
+                b->key_init = p->init;
+                b->key_hub = a.hub;
+                b->key_grab = m.grab;
+            }
+        }
+    }
     cudaEvent_t ev0, ev1;
     GCG_CUDA(cudaEventCreate(&ev0));
     GCG_CUDA(cudaEventCreate(&ev1));
     GCG_CUDA(cudaEventRecord(ev0, s));
-    void *kargs[] = {&m};
-    cudaError_t le = cudaLaunchCooperativeKernel((const void *)k_multi_pagerank, dim3(grid), dim3(EDGE_THREADS), kargs,
-                                                 hub_bytes, s);
-    if (le != cudaSuccess) {
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
-        return fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: cooperative launch: ") + cudaGetErrorString(le));
+    int rc = GCG_OK;
+    if (use_graph) {
+        cudaError_t e = cudaGraphLaunch(b->gexec, s);
+        if (e != cudaSuccess) rc = fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: graph launch: ") + cudaGetErrorString(e));
+    } else {
+        rc = enqueue_solve(b, m, p, init_dev, grid, hub_bytes);
     }
-    GCG_CUDA(cudaEventRecord(ev1, s));
+    cudaEventRecord(ev1, s);
     int herr = 0;
-    GCG_CUDA(cudaMemcpyAsync(&herr, b->err.get(), 4, cudaMemcpyDeviceToHost, s));
-    GCG_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> hsw(ng);
+    std::vector<double> hres(ng);
+    if (rc == GCG_OK) {
+        cudaMemcpyAsync(&herr, b->err.get(), 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(hsw.data(), b->gsweeps.get(), ng * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(hres.data(), b->gres.get(), ng * 8, cudaMemcpyDeviceToHost, s);
+    }
+    cudaError_t se = cudaStreamSynchronize(s);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    if (rc != GCG_OK) return rc;
+    if (se != cudaSuccess) return fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: ") + cudaGetErrorString(se));
     if (herr) return fail(GCG_ERR_TIMEOUT, "gcg_batch_pagerank: a grid-barrier wait ran out (persistent kernel stopped)");
-    /* assemble the ranks */
-    {
-        dim3 sg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv / ng + 255) / 256, 64)),
-                std::min<uint32_t>(ng, 1024));
-        const float t = (float)p->teleport;
-        k_multi_scatter<<<sg, 256, 0, s>>>(b->gr.get(), ng, b->gsweeps.get(), pl.nz_rows.get(), pl.zero_rows.get(),
-                                           m.rnz[0], m.rnz[1], t, b->r.get());
-        GCG_LAUNCH_CHECK();
-    }
-    std::vector<int> hsw(ng);
-    std::vector<double> hres(ng);
-    GCG_CUDA(cudaMemcpyAsync(hsw.data(), b->gsweeps.get(), ng * 4, cudaMemcpyDeviceToHost, s));
-    GCG_CUDA(cudaMemcpyAsync(hres.data(), b->gres.get(), ng * 8, cudaMemcpyDeviceToHost, s));
-    if (out) { /* union layout -> caller layout */
-        tbuf<float> compact;
-        GCG_TRY(compact.alloc(nreal, s));
-        k_expand<<<eg, 256, 0, s>>>(b->r.get(), b->d_roff.get(), b->d_voff.get(), ng, compact.get(), 0);
-        GCG_LAUNCH_CHECK();
-        GCG_TRY(copy_out(out, compact.get(), (size_t)nreal * 4, s));
-    }
+    if (out) GCG_TRY(copy_out(out, b->rout.get(), (size_t)nreal * 4, s));
     GCG_CUDA(cudaStreamSynchronize(s));
     if (sweeps) memcpy(sweeps, hsw.data(), ng * 4);
     if (residuals) memcpy(residuals, hres.data(), ng * 8);
@@ -710,9 +825,56 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
         stats->device_ms = ms;
         stats->sweep_kernel_ms = ms;
         stats->timed_sweeps = mx;
-        /* init (3), the persistent kernel, the scatter, and the layout maps */
-        stats->kernel_launches = 5 + (p->init_rank ? 1 : 0) + (out ? 1 : 0);
+        /* per-graph init, initial vector (2), the persistent kernel, the rank
+         * assembly, the map to the callers' layout, and the map of init_rank */
+        stats->kernel_launches = 6 + (p->init_rank ? 1 : 0);
     }
+    return GCG_OK;
+}
+
+/* Times `sweeps` fixed sweeps of every candidate launch configuration and keeps
+ * the fastest: hub entries (the out-degree rank below which a source's
+ * contribution is read from shared memory: the degree bin of the cache) and the
+ * edge phase's work distribution (strided, or runs of 1, 4 or 16 chunks from
+ * the device queue). */
+static int batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_out, uint32_t *grab_out, double *ms_out) {
+    const ChunkPlan &pl = *b->u->cplan;
+    std::vector<uint32_t> hubs;
+    for (uint32_t h : {0u, 8192u, 16384u, 32768u, HUB_MAX})
+        if (h <= pl.hub && std::find(hubs.begin(), hubs.end(), h) == hubs.end()) hubs.push_back(h);
+    if (std::find(hubs.begin(), hubs.end(), pl.hub) == hubs.end()) hubs.push_back(pl.hub);
+    const uint32_t grabs[] = {0u, 1u, 4u, 16u};
+    gcg_pr_params p;
+    gcg_pr_params_default(&p);
+    p.max_sweeps = sweeps;
+    p.tol = 0.0;
+    double best = 1e300;
+    uint32_t bh = pl.hub, bg = 0;
+    for (uint32_t h : hubs)
+        for (uint32_t g : grabs) {
+            b->tune_hub = h;
+            b->tune_grab = g;
+            gcg_pr_stats st;
+            double t = 1e300;
+            for (int rep = 0; rep < 2; ++rep) { /* the first run warms caches and the pool */
+                GCG_TRY(batch_pagerank(b, &p, nullptr, nullptr, nullptr, &st, false));
+                t = std::min(t, st.device_ms);
+            }
+            if (t < best) {
+                best = t;
+                bh = h;
+                bg = g;
+            }
+        }
+    b->tune_hub = bh;
+    b->tune_grab = bg;
+    if (b->gexec) { /* captured with another configuration */
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+    }
+    if (hub_out) *hub_out = bh;
+    if (grab_out) *grab_out = bg;
+    if (ms_out) *ms_out = best / std::max(sweeps, 1);
     return GCG_OK;
 }
 
@@ -731,11 +893,32 @@ int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out
         if (!graphs[g]) return fail(GCG_ERR_INVALID, "gcg_batch_create: null graph");
     gcg_batch *b = new gcg_batch();
     int st = batch_build(graphs, ngraphs, b);
+    if (st == GCG_OK && cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
+        b->own = nullptr;
+        st = fail(GCG_ERR_CUDA, "gcg_batch_create: cannot create a stream");
+    }
     if (st != GCG_OK) {
         delete b;
         return st;
     }
+    b->u->stream = b->own;
     *out = b;
+    return GCG_OK;
+}
+
+int gcg_batch_set_config(gcg_batch *b, uint32_t hub_entries, uint32_t queue_run) {
+    if (!b) return fail(GCG_ERR_INVALID, "gcg_batch_set_config: null batch");
+    if (queue_run > (1u << 20)) return fail(GCG_ERR_INVALID, "gcg_batch_set_config: queue_run too large");
+    b->tune_hub = hub_entries;
+    b->tune_grab = queue_run;
+    return GCG_OK;
+}
+
+int gcg_batch_get_config(const gcg_batch *b, uint32_t *hub_entries, uint32_t *queue_run, int *graph_ready) {
+    if (!b) return fail(GCG_ERR_INVALID, "gcg_batch_get_config: null batch");
+    if (hub_entries) *hub_entries = std::min(b->u->cplan->hub, b->tune_hub);
+    if (queue_run) *queue_run = b->tune_grab;
+    if (graph_ready) *graph_ready = b->gexec != nullptr;
     return GCG_OK;
 }
 
@@ -747,7 +930,7 @@ int gcg_batch_vertex_offsets(const gcg_batch *b, uint64_t *offsets) {
 
 int gcg_batch_set_stream(gcg_batch *b, void *stream) {
     if (!b) return fail(GCG_ERR_INVALID, "gcg_batch_set_stream: null batch");
-    b->u->stream = (cudaStream_t)stream;
+    b->u->stream = stream ? (cudaStream_t)stream : b->own;
     return GCG_OK;
 }
 
@@ -758,6 +941,12 @@ int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ran
         return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_pagerank: plain Jacobi only");
     if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_batch_pagerank: max_sweeps < 0");
     return batch_pagerank(b, params, out_ranks, sweeps, residuals, stats);
+}
+
+int gcg_batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_entries, uint32_t *queue_run, double *ms_per_sweep) {
+    if (!b) return fail(GCG_ERR_INVALID, "gcg_batch_autotune: null batch");
+    if (sweeps < 1) return fail(GCG_ERR_INVALID, "gcg_batch_autotune: sweeps must be >= 1");
+    return batch_autotune(b, sweeps, hub_entries, queue_run, ms_per_sweep);
 }
 
 int gcg_batch_free(gcg_batch *b) {

@@ -47,6 +47,7 @@ EXPORTED = [
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
     "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
+    "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
     "gcg_warm_start_rank",
@@ -132,6 +133,9 @@ _batch_offsets = _sig("gcg_batch_vertex_offsets", _i, _vp, _vp)
 _batch_set_stream = _sig("gcg_batch_set_stream", _i, _vp, _vp)
 _batch_pagerank = _sig("gcg_batch_pagerank", _i, _vp, C.POINTER(PrParams), _vp, _vp, _vp, C.POINTER(PrStats))
 _batch_free = _sig("gcg_batch_free", _i, _vp)
+_batch_autotune = _sig("gcg_batch_autotune", _i, _vp, _i, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(C.c_double))
+_batch_set_config = _sig("gcg_batch_set_config", _i, _vp, _u32, _u32)
+_batch_get_config = _sig("gcg_batch_get_config", _i, _vp, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_i))
 _mlp_create = _sig("gcg_mlp_create", _i, _u64, C.POINTER(_vp))
 _mlp_free = _sig("gcg_mlp_free", _i, _vp)
 _mlp_get = _sig("gcg_mlp_get", _i, _vp, _vp, _vp)
@@ -431,6 +435,21 @@ class Batch:
         st = PrStats()
         check(_batch_pagerank(self._h, C.byref(p), ptr(out), ptr(sweeps), ptr(res), C.byref(st)))
         return out, sweeps, res, st
+
+    def autotune(self, sweeps=8):
+        """Times the candidate launch configurations; returns (hub entries, queue run, ms per sweep)."""
+        h, q, ms = _u32(0), _u32(0), C.c_double(0.0)
+        check(_batch_autotune(self._h, sweeps, C.byref(h), C.byref(q), C.byref(ms)))
+        return h.value, q.value, ms.value
+
+    def set_config(self, hub_entries, queue_run):
+        check(_batch_set_config(self._h, hub_entries, queue_run))
+
+    def config(self):
+        """(hub entries, queue run, captured solve ready)."""
+        h, q, r = _u32(0), _u32(0), _i(0)
+        check(_batch_get_config(self._h, C.byref(h), C.byref(q), C.byref(r)))
+        return h.value, q.value, bool(r.value)
 
     def split(self, ranks):
         return [ranks[int(self.offsets[g]):int(self.offsets[g + 1])] for g in range(self.ngraphs)]

@@ -193,13 +193,29 @@ int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out
 int gcg_batch_vertex_offsets(const gcg_batch *b, uint64_t *offsets);
 int gcg_batch_set_stream(gcg_batch *b, void *stream);
 /* Jacobi PageRank of every graph (the gcg_pagerank formula and stopping rule per
- * graph) in ONE cooperative persistent kernel: sweeps proceed together, a graph
- * leaves the device work queues when its own residual is <= tol. out_ranks: total
- * vertices, graph g at its vertex offset; sweeps / residuals: per graph (may be
- * NULL); params->init_rank (total vertices) may seed all graphs. Returns
- * GCG_ERR_TIMEOUT if a bounded grid-barrier wait runs out. */
+ * graph, bit-identical results) in ONE cooperative persistent kernel: sweeps
+ * proceed together, a graph leaves the device work queues when its own residual
+ * is <= tol. out_ranks: total vertices, graph g at its vertex offset (may be
+ * NULL); sweeps / residuals: per graph (may be NULL); params->init_rank (total
+ * vertices) may seed all graphs. Without init_rank the whole solve is captured
+ * into a CUDA graph on the first call with a given parameter set and replayed on
+ * later calls. Returns GCG_ERR_TIMEOUT if a bounded grid-barrier wait runs out.
+ * Until gcg_batch_set_stream is called, the batch runs on a stream of its own
+ * that waits for the legacy default stream at the start of every call. */
 int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ranks, int32_t *sweeps,
                        double *residuals, gcg_pr_stats *stats);
+/* Autotuner of the persistent launch: times `sweeps` fixed sweeps of each
+ * candidate configuration and keeps the fastest for later solves (results do not
+ * depend on it). Candidates: shared-memory hub entries (sources whose out-degree
+ * rank is below it are read from shared memory: the degree threshold of the
+ * cache) in {0, 8192, 16384, 32768, 49152, the plan's}, and the edge phase's work
+ * distribution: warps striding over the chunks (queue_run 0) or taking runs of
+ * 1, 4 or 16 chunks from a device work queue. Outputs may be NULL. */
+int gcg_batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_entries, uint32_t *queue_run, double *ms_per_sweep);
+/* Sets the configuration by hand (hub entries are capped at the plan's). */
+int gcg_batch_set_config(gcg_batch *b, uint32_t hub_entries, uint32_t queue_run);
+/* The configuration in use, and whether a captured solve is ready to replay. */
+int gcg_batch_get_config(const gcg_batch *b, uint32_t *hub_entries, uint32_t *queue_run, int *graph_ready);
 int gcg_batch_free(gcg_batch *b);
 
 /* No counterpart in the reference. PageRank (GCG_PR_JACOBI only) over an in-edge

@@ -72,3 +72,25 @@ def test_batch_barrier_timeout_is_reported_and_context_survives():
         assert np.array_equal(b.split(r)[0], ref)
     for g in gs:
         g.free()
+
+
+def test_batch_graph_replay_and_launch_configs_keep_results():
+    gs = make_graphs()
+    with gcgpu.Batch(gs) as b:
+        r1, sw1, res1, st1 = b.pagerank(max_sweeps=1000, tol=1e-8)
+        assert b.config()[2]  # the solve was captured into a CUDA graph
+        r2, sw2, res2, _ = b.pagerank(max_sweeps=1000, tol=1e-8)  # replayed
+        assert np.array_equal(r1, r2) and np.array_equal(sw1, sw2) and np.array_equal(res1, res2)
+        # every launch configuration computes the same sums in the same order
+        for hub, run in [(0, 0), (8192, 1), (100000, 4), (16384, 16)]:
+            b.set_config(hub, run)
+            r3, sw3, res3, _ = b.pagerank(max_sweeps=1000, tol=1e-8)
+            assert np.array_equal(r1, r3) and np.array_equal(sw1, sw3) and np.array_equal(res1, res3), (hub, run)
+        hub, run, ms = b.autotune(sweeps=4)
+        assert ms > 0 and run in (0, 1, 4, 16)
+        h2, q2, ready = b.config()
+        assert (h2, q2) == (hub, run) and not ready
+        r4, sw4, _, _ = b.pagerank(max_sweeps=1000, tol=1e-8)
+        assert np.array_equal(r1, r4) and np.array_equal(sw1, sw4)
+    for g in gs:
+        g.free()
