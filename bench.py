@@ -15,6 +15,9 @@ the device sharder, 64 vertex intervals.
              launch / its CUDA-event launch time, against measured HBM copy GB/s
   cpu_baseline  the reference's own PageRank app (oracle/_ref/pagerank, built
              from the reference sources) on a bounded sample, all host cores
+  extras     the other rows against their plain methods: connected components
+             (+ triangles) on symmetrised R-MAT, the learned warm start, batched
+             personalised PageRank, 64 uneven graphs in one persistent launch
 
 --impl reference times the reference alone (rank 0; other ranks exit).
 Under torchrun (N > 1) every rank solves its own replica (the path does not
@@ -164,6 +167,115 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_extras(args):
+    """The other rows of the workload, each against its plain method on the same
+    device (all device times by CUDA events; rank 0 of a 1-GPU run):
+      cc            connected components, symmetrised R-MAT scale 24 (and 20) + triangles at 20
+      warm_start    learned warm start vs uniform start to 1e-8 on the scale-24 graph
+      batched_ppr   256 personalised sources at once vs single-source solves, scale 22
+      batched_graphs 64 uneven graphs (10k-2M vertices, ER mean degree 8 / R-MAT) in one
+                    autotuned, graph-captured persistent launch vs one solve per graph"""
+    import math
+    import numpy as np
+    import torch
+    import gcgpu
+    import gcgpu.warm as gw
+    out = {}
+    peak, _ = load_peaks()
+
+    def dev_edges(scale, m, seed, abc=(0.57, 0.19, 0.19)):
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty(m, dtype=torch.int32, device="cuda")
+        gcgpu.generate_rmat(scale, m, *abc, seed=seed, src=s, dst=d)
+        return s, d
+
+    # ---- connected components (and triangles at scale 20) ----
+    cc = {}
+    for scale in (24, 20):
+        s, d = dev_edges(scale, args.ef << scale, args.seed)
+        with gcgpu.Graph.from_edges(s, d, dedup=True, symmetrise=True, out_csr=False) as g:
+            del s, d
+            V, E = g.num_vertices, g.num_edges
+            lab = torch.empty(V, dtype=torch.int32, device="cuda")
+            g.connected_components(out=lab)
+            ms = min(g.connected_components(out=lab)[1].device_ms for _ in range(3))
+            alg = 8.0 * E + 12.0 * V
+            row = {"vertices": V, "directed_edges": E, "ms": ms, "GTEPS": E / ms / 1e6,
+                   "achieved_GBs": alg / ms / 1e6, "frac_of_hbm": alg / ms / 1e6 / peak,
+                   "algorithmic_bytes": "8E + 12V (one hooking pass + compress)"}
+            if scale == 20:
+                tri, _, _, tst = g.triangle_count(per_rank=False, vertexmap=False)
+                tms = min(g.triangle_count(per_rank=False, vertexmap=False)[3].device_ms for _ in range(2))
+                row["triangles"] = tri
+                row["tc_ms"] = tms
+            cc[f"rmat{scale}_sym"] = row
+    out["cc"] = cc
+
+    # ---- learned warm start on the headline graph ----
+    s, d = dev_edges(args.scale, args.ef << args.scale, args.seed)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=False) as g, gcgpu.Mlp.load(gw.MODEL_PATH) as m:
+        del s, d
+        rec = min((gw.evaluate(g, m) for _ in range(2)), key=lambda r: r["ms_warm"])
+        out["warm_start"] = {"graph": f"rmat{args.scale}_ef{args.ef}_seed{args.seed}", "model": "gcgpu/warm_start_rmat.npz",
+                             "sweeps_plain": rec["sweeps_plain"], "sweeps_warm": rec["sweeps_warm"],
+                             "ms_plain": rec["ms_plain"], "ms_warm_total": rec["ms_warm"],
+                             "ms_warm_start": rec["ms_warm_start"], "speedup": rec["ms_plain"] / rec["ms_warm"],
+                             "l1_between_answers": rec["l1_between"], "tol": 1e-8}
+
+    # ---- batched personalised PageRank ----
+    s, d = dev_edges(22, args.ef << 22, args.seed + 6)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=False) as g:
+        del s, d
+        n = g.num_vertices
+        src = np.random.default_rng(3).integers(0, n, 256).astype(np.uint32)
+        g.pagerank(max_sweeps=2)
+        mat = torch.empty((n, 256), dtype=torch.float32, device="cuda")
+        bms = min(g.ppr_batched(src, max_sweeps=1000, tol=1e-8, teleport=0.15, out=mat)[1].device_ms for _ in range(2))
+        vec = torch.empty(n, dtype=torch.float32, device="cuda")
+        sample = 32
+        sms = sum(g.pagerank(max_sweeps=1000, tol=1e-8, teleport=0.15, source=int(v), out=vec)[1].device_ms
+                  for v in src[:sample])
+        out["batched_ppr"] = {"graph": "rmat22_ef16", "sources": 256, "ms_batched": bms,
+                              "ms_single_source_x256": sms * 256 / sample,
+                              "single_source_sample": f"{sample} of the 256 sources timed, scaled by 8",
+                              "speedup": sms * 256 / sample / bms}
+        del mat
+
+    # ---- 64 uneven graphs in one persistent launch ----
+    rng = np.random.default_rng(5)
+    ns = np.exp(rng.uniform(math.log(1e4), math.log(2e6), 64)).astype(int)
+    gs = []
+    for i, nn in enumerate(ns):
+        if i % 2 == 0:
+            mm = 8 * int(nn)
+            s = torch.empty(mm, dtype=torch.int32, device="cuda")
+            d = torch.empty(mm, dtype=torch.int32, device="cuda")
+            gcgpu.generate_er(int(nn), mm, 100 + i, s, d)
+            gs.append(gcgpu.Graph.from_edges(s, d, num_vertices=int(nn), dedup=True, out_csr=False))
+        else:
+            sc = max(1, round(math.log2(nn)))
+            s, d = dev_edges(sc, 8 << sc, 100 + i)
+            gs.append(gcgpu.Graph.from_edges(s, d, num_vertices=1 << sc, dedup=True, out_csr=False))
+    seq = 0.0
+    for g in gs:
+        o = torch.empty(g.num_vertices, dtype=torch.float32, device="cuda")
+        g.pagerank(max_sweeps=1000, tol=1e-8, out=o)
+        seq += g.pagerank(max_sweeps=1000, tol=1e-8, out=o)[1].device_ms
+    with gcgpu.Batch(gs) as b:
+        hub, run, _ = b.autotune(sweeps=6)
+        allr = torch.empty(int(b.offsets[-1]), dtype=torch.float32, device="cuda")
+        b.pagerank(max_sweeps=1000, tol=1e-8, out=allr)  # captures the CUDA graph
+        st = min((b.pagerank(max_sweeps=1000, tol=1e-8, out=allr)[3] for _ in range(3)), key=lambda x: x.device_ms)
+        out["batched_graphs"] = {"graphs": 64, "vertices": int(b.offsets[-1]),
+                                 "edges": int(sum(g.num_edges for g in gs)), "ms_one_launch": st.device_ms,
+                                 "ms_one_solve_per_graph": seq, "speedup": seq / st.device_ms,
+                                 "autotuned": {"hub_entries": hub, "queue_run": run}, "cuda_graph": b.config()[2],
+                                 "max_sweeps": st.sweeps}
+    for g in gs:
+        g.free()
+    return out
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -265,6 +377,13 @@ def run_ours(args, rank, world):
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"[:300]}
 
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        try:
+            extras = run_extras(args)
+        except Exception as e:  # noqa: BLE001
+            extras = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -286,6 +405,7 @@ def run_ours(args, rank, world):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "extras": extras,
         }
         print(json.dumps(line))
     g.free()
@@ -308,6 +428,7 @@ def main():
     ap.add_argument("--ref-scale", type=int, default=20)
     ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the CC / warm-start / batched rows")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

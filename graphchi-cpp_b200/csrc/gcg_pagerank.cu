@@ -113,17 +113,24 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     load_hub(a, s_hub);
     __syncthreads();
 
-    /* Software pipeline: while a chunk's gathers are in flight, the next chunk's
+    /* Warp w takes runs of a.run consecutive chunks: runs w, w + nwarps, ...
+     * Software pipeline: while a chunk's gathers are in flight, the next chunk's
      * columns, head flags and row base are already being loaded. */
-    uint32_t ch = gwarp;
+    const uint64_t R = a.run, nch = a.nchunks;
+    uint64_t q = gwarp, ch = q * R, end = ch + R < nch ? ch + R : nch;
     uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
-    if (ch < a.nchunks) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
-    for (; ch < a.nchunks; ch += nwarps) {
+    if (ch < end) load_chunk(a, (uint32_t)ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
+    while (ch < end) {
         float val[EPL];
         gather_chunk(a, col, nvalid, s_hub, pol_keep, val);
-        const uint32_t cur_flags = flags, cur_nvalid = nvalid, cur_base = base;
-        if (ch + nwarps < a.nchunks) load_chunk(a, ch + nwarps, lane, pol_stream, col, flags, nvalid, base, a.ne);
-        reduce_chunk(a, ch, lane, val, cur_flags, cur_nvalid, cur_base, a.ne);
+        const uint32_t cur = (uint32_t)ch, cur_flags = flags, cur_nvalid = nvalid, cur_base = base;
+        if (++ch >= end) {
+            q += nwarps;
+            ch = q * R;
+            end = ch + R < nch ? ch + R : nch;
+        }
+        if (ch < end) load_chunk(a, (uint32_t)ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
+        reduce_chunk(a, cur, lane, val, cur_flags, cur_nvalid, cur_base, a.ne);
     }
 }
 
@@ -415,6 +422,10 @@ int ensure_chunk_plan(gcg_graph *g) {
 }
 
 /* one CTA of EDGE_THREADS per SM (the hub cache takes most of shared memory) */
+static void launch_edges(int ge, uint32_t hub_bytes, cudaStream_t s, const SweepArgs &a) {
+    k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
+}
+
 static int edge_grid(uint32_t hub_bytes) {
     static bool attr = false;
     if (!attr) {
@@ -437,8 +448,9 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     const uint32_t nv = g->nv;
     const int max_sweeps = p->max_sweeps;
 
-    const uint32_t hub_bytes = pl.hub * 4u;
-    const int ge = std::max(1, std::min<int>(edge_grid(hub_bytes), (int)((pl.nchunks + 31) / 32)));
+    const uint32_t hub_bytes = std::min(pl.hub, pl.tune_hub) * 4u;
+    const uint64_t run = std::max(1u, pl.tune_run);
+    const int ge = std::max(1, (int)std::min<uint64_t>((uint64_t)edge_grid(hub_bytes), (pl.nchunks + 32 * run - 1) / (32 * run)));
     const int gv = (int)grid1d(std::max<uint64_t>(pl.nnz, pl.nzero), 8);
     /* the sweep workspace lives with the graph: allocated on the first call,
      * reused by later calls (no allocation on the repeated-solve path) */
@@ -482,7 +494,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
 
     SweepArgs a;
     a.col = pl.col_r.get();
-    a.hub = pl.hub;
+    a.hub = std::min(pl.hub, pl.tune_hub);
+    a.run = std::max(1u, pl.tune_run);
     a.nz_cidx = pl.nz_cidx.get();
     a.zero_cidx = pl.zero_cidx.get();
     a.outdeg = g->outdeg.get();
@@ -549,12 +562,12 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, s);
-                k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
+                launch_edges(ge, hub_bytes, s, a);
                 cudaEventRecord(e1, s);
                 sweep_ev.push_back(e0);
                 sweep_ev.push_back(e1);
             } else {
-                k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
+                launch_edges(ge, hub_bytes, s, a);
             }
             k_pr_fix<<<fg, 256, 0, s>>>(a);
             k_pr_vertex<<<gv, 256, 0, s>>>(a, sw, sw < 2 ? 1 : 0);
@@ -650,6 +663,66 @@ void gcg_pr_params_default(gcg_pr_params *p) {
     p->residuals = nullptr;
     p->source = GCG_NO_SOURCE;
     p->reserved2 = 0u;
+}
+
+int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_run) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_pagerank_set_config: null graph");
+    if (chunk_run == 0 || chunk_run > (1u << 16)) return fail(GCG_ERR_INVALID, "gcg_pagerank_set_config: chunk_run must be 1..65536");
+    GCG_TRY(ensure_chunk_plan(g));
+    g->cplan->tune_hub = hub_entries;
+    g->cplan->tune_run = chunk_run;
+    return GCG_OK;
+}
+
+int gcg_pagerank_get_config(gcg_graph *g, uint32_t *hub_entries, uint32_t *chunk_run) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_pagerank_get_config: null graph");
+    GCG_TRY(ensure_chunk_plan(g));
+    if (hub_entries) *hub_entries = std::min(g->cplan->hub, g->cplan->tune_hub);
+    if (chunk_run) *chunk_run = g->cplan->tune_run;
+    return GCG_OK;
+}
+
+int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint32_t *chunk_run, double *ms_per_sweep) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_pagerank_autotune: null graph");
+    if (sweeps < 1) return fail(GCG_ERR_INVALID, "gcg_pagerank_autotune: sweeps must be >= 1");
+    GCG_TRY(ensure_chunk_plan(g));
+    ChunkPlan &pl = *g->cplan;
+    std::vector<uint32_t> hubs;
+    for (uint32_t h : {0u, 16384u, 32768u, HUB_MAX})
+        if (h <= pl.hub && std::find(hubs.begin(), hubs.end(), h) == hubs.end()) hubs.push_back(h);
+    if (std::find(hubs.begin(), hubs.end(), pl.hub) == hubs.end()) hubs.push_back(pl.hub);
+    const uint32_t runs[] = {1u, 2u, 4u, 16u};
+    gcg_pr_params p;
+    gcg_pr_params_default(&p);
+    p.max_sweeps = sweeps;
+    p.tol = 0.0;
+    p.flags = GCG_PR_TIME_SWEEPS;
+    tbuf<float> out;
+    GCG_TRY(out.alloc(std::max<uint32_t>(g->nv, 1), g->stream));
+    double best = 1e300;
+    uint32_t bh = pl.hub, br = 1;
+    for (uint32_t h : hubs)
+        for (uint32_t r : runs) {
+            pl.tune_hub = h;
+            pl.tune_run = r;
+            double t = 1e300;
+            for (int rep = 0; rep < 2; ++rep) { /* the first run warms caches */
+                gcg_pr_stats st;
+                GCG_TRY(pagerank_jacobi(g, &p, out.get(), &st));
+                if (st.timed_sweeps > 0) t = std::min(t, st.sweep_kernel_ms / st.timed_sweeps);
+            }
+            if (t < best) {
+                best = t;
+                bh = h;
+                br = r;
+            }
+        }
+    pl.tune_hub = bh;
+    pl.tune_run = br;
+    if (hub_entries) *hub_entries = bh;
+    if (chunk_run) *chunk_run = br;
+    if (ms_per_sweep) *ms_per_sweep = best;
+    return GCG_OK;
 }
 
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats) {

@@ -63,6 +63,7 @@ struct SweepArgs {
     double *res_log, *last_res;
     double teleport, damping, tol, norm_const;
     uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
+    uint32_t run;    /* edge kernel: each warp takes runs of this many consecutive chunks (>= 1) */
 };
 
 /* columns (streamed), head flags and starting row index of one chunk; ne is
@@ -241,6 +242,9 @@ struct ChunkPlan {
     /* sources relabelled by out-degree (descending): col_r = newid[col] */
     uint32_t hub = 0;
     dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
+    /* launch configuration of the edge kernel (gcg_pagerank_autotune):
+     * shared-memory hub entries (capped at hub) and chunks per warp run */
+    uint32_t tune_hub = 0xFFFFFFFFu, tune_run = 1;
 };
 
 /* builds (once per graph) the chunk plan and the out-degree relabelling */

@@ -48,6 +48,7 @@ EXPORTED = [
     "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
+    "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
     "gcg_warm_start_rank",
@@ -127,6 +128,9 @@ _gen_rmat = _sig("gcg_generate_rmat", _i, _u32, _u64, C.c_double, C.c_double, C.
 _gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
 _pr_noalloc = _sig("gcg_pagerank_csr_noalloc", _i, _vp, _vp, _vp, _u32, C.POINTER(PrParams), _vp, _vp,
                    C.POINTER(PrStats))
+_pr_set_config = _sig("gcg_pagerank_set_config", _i, _vp, _u32, _u32)
+_pr_get_config = _sig("gcg_pagerank_get_config", _i, _vp, C.POINTER(_u32), C.POINTER(_u32))
+_pr_autotune = _sig("gcg_pagerank_autotune", _i, _vp, _i, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(C.c_double))
 _ppr = _sig("gcg_ppr_batched", _i, _vp, _vp, _u32, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
 _batch_create = _sig("gcg_batch_create", _i, C.POINTER(_vp), _u32, C.POINTER(_vp))
 _batch_offsets = _sig("gcg_batch_vertex_offsets", _i, _vp, _vp)
@@ -286,6 +290,22 @@ class Graph:
         st = PrStats()
         check(_pagerank(self._h, C.byref(p), ptr(out), C.byref(st)))
         return out, st
+
+    def pagerank_config(self, hub_entries=None, chunk_run=None):
+        """Sets (when given) and returns the edge kernel's (hub entries, chunk run)."""
+        if hub_entries is not None or chunk_run is not None:
+            h0, r0 = self.pagerank_config()
+            check(_pr_set_config(self._h, h0 if hub_entries is None else hub_entries,
+                                 r0 if chunk_run is None else chunk_run))
+        h, r = _u32(0), _u32(0)
+        check(_pr_get_config(self._h, C.byref(h), C.byref(r)))
+        return h.value, r.value
+
+    def pagerank_autotune(self, sweeps=8):
+        """Times the edge kernel's candidate configurations; returns (hub entries, chunk run, ms per sweep)."""
+        h, r, ms = _u32(0), _u32(0), C.c_double(0.0)
+        check(_pr_autotune(self._h, sweeps, C.byref(h), C.byref(r), C.byref(ms)))
+        return h.value, r.value, ms.value
 
     def ppr_batched(self, sources, max_sweeps=100, teleport=0.15, damping=0.85, tol=0.0, out=None,
                     residuals=None, time_sweeps=False):

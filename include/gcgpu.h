@@ -163,6 +163,18 @@ void gcg_pr_params_default(gcg_pr_params *p);
  * out_rank: num_vertices floats, host or device. stats may be NULL. */
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats);
 
+/* Launch configuration of the Jacobi edge kernel of one graph (results do not
+ * depend on it): hub_entries = shared-memory contribution cache entries (sources
+ * whose out-degree rank is below it are read from shared memory; capped at the
+ * plan's 49152), chunk_run = consecutive 256-edge chunks a warp takes at a time
+ * (1 = warps stride chunk by chunk). gcg_pagerank_autotune times `sweeps` fixed
+ * sweeps of each candidate (hub entries {0, 16384, 32768, 49152, the plan's} x
+ * runs {1, 2, 4, 16}), keeps the fastest for later calls on this graph and
+ * reports it (outputs may be NULL). */
+int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_run);
+int gcg_pagerank_get_config(gcg_graph *g, uint32_t *hub_entries, uint32_t *chunk_run);
+int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint32_t *chunk_run, double *ms_per_sweep);
+
 /* Batched personalised PageRank (the engine's addition beside the reference's
  * one-vector runs of example_apps/pagerank.cpp): nsources sources solved together
  * as a vertex-major rank matrix. For source s: r_s starts at the indicator of

@@ -149,6 +149,23 @@ def test_pagerank_deterministic():
     assert np.array_equal(a, b)
 
 
+def test_pagerank_launch_configs_and_autotune_keep_results():
+    # the edge kernel's configuration changes which warp runs a chunk and where a
+    # contribution is read from, never the sums: results are bit-identical
+    z, spec, g, go = graph_for("rmat_s16_ef16_seed1")
+    ref, _ = g.pagerank(max_sweeps=20)
+    for hub, run in [(0, 1), (16384, 2), (49152, 4), (1 << 30, 16), (32768, 64)]:
+        g.pagerank_config(hub, run)
+        r, _ = g.pagerank(max_sweeps=20)
+        assert np.array_equal(r, ref), (hub, run)
+    hub, run, ms = g.pagerank_autotune(sweeps=3)
+    assert ms > 0 and run in (1, 2, 4, 16) and g.pagerank_config() == (hub, run)
+    r, _ = g.pagerank(max_sweeps=20)
+    assert np.array_equal(r, ref)
+    with pytest.raises(gcgpu.GcgError):
+        g.pagerank_config(hub, 0)
+
+
 def test_pagerank_zero_sweeps_returns_init():
     z, spec, g, go = graph_for("handmade_components")
     r, st = g.pagerank(max_sweeps=0, init=2.5)
