@@ -13,6 +13,16 @@
  * evenly over the CTAs; one pass suffices because hooking is transitive.
  * The CAS loop has no waits on other threads: each failed CAS moves to a
  * strictly smaller id, so it ends.
+ *
+ * When every vertex's full neighbourhood is at hand (a symmetrised graph: the
+ * in-list; otherwise the in-list plus the out-list), the edge pass samples
+ * instead (the Afforest scheme): two rounds link each vertex to its first two
+ * neighbours, a compress, then 1024 sampled vertices name the most frequent
+ * root (the giant component); only vertices outside it link their remaining
+ * neighbours (a thread per short list, a warp per long one). A skipped vertex of
+ * the giant component loses nothing: each of its other edges is also in the
+ * neighbour's list, and that neighbour links it unless it is in the giant
+ * component too. The same hook keeps the labels (the minimum id per component).
  */
 #include <algorithm>
 
@@ -81,6 +91,97 @@ __global__ void __launch_bounds__(MP_THREADS) k_cc_hook(const uint32_t *__restri
     }
 }
 
+/* neighbour i of v in the concatenation in-list(v) ++ out-list(v) (rout NULL: in-list only) */
+struct Nbrs {
+    const uint32_t *rin, *cin, *rout, *cout;
+};
+__device__ __forceinline__ uint32_t nbr_count(const Nbrs &n, uint32_t v) {
+    uint32_t d = n.rin[v + 1] - n.rin[v];
+    if (n.rout) d += n.rout[v + 1] - n.rout[v];
+    return d;
+}
+__device__ __forceinline__ uint32_t nbr_at(const Nbrs &n, uint32_t v, uint32_t i) {
+    const uint32_t b = n.rin[v], din = n.rin[v + 1] - b;
+    return i < din ? n.cin[b + i] : n.cout[n.rout[v] + (i - din)];
+}
+
+/* sampling round r: link v to its r-th neighbour */
+__global__ void k_cc_round(Nbrs n, uint32_t nv, uint32_t r, uint32_t *parent) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        if (r < nbr_count(n, v)) hook(parent, v, nbr_at(n, v, r));
+}
+
+/* full compress between the rounds (same read-only find as the final pass) */
+__device__ __forceinline__ uint32_t find_root_ro(const uint32_t *parent, uint32_t x);
+__global__ void k_cc_flatten(uint32_t nv, uint32_t *parent) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        ((volatile uint32_t *)parent)[v] = find_root_ro(parent, v);
+}
+
+/* the most frequent root among 1024 sampled vertices (ties: the smaller id);
+ * one block of 1024 threads: bitonic sort in shared memory, then run lengths */
+__global__ void __launch_bounds__(1024) k_cc_sample(const uint32_t *parent, uint32_t nv, uint32_t *giant) {
+    __shared__ uint32_t s[1024];
+    __shared__ unsigned long long s_best;
+    const uint32_t t = threadIdx.x;
+    uint64_t z = (uint64_t)t * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    s[t] = parent[(uint32_t)(z % nv)];
+    if (t == 0) s_best = ~0ull;
+    __syncthreads();
+    for (uint32_t k = 2; k <= 1024; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = t ^ j;
+            if (o > t) {
+                const uint32_t x = s[t], y = s[o];
+                const bool up = (t & k) == 0;
+                if ((x > y) == up) {
+                    s[t] = y;
+                    s[o] = x;
+                }
+            }
+            __syncthreads();
+        }
+    /* run starting at t: key = (1024 - length) << 32 | value, smallest wins */
+    if (t == 0 || s[t] != s[t - 1]) {
+        uint32_t e = t + 1;
+        while (e < 1024 && s[e] == s[t]) ++e;
+        atomicMin(&s_best, ((unsigned long long)(1024u - (e - t)) << 32) | s[t]);
+    }
+    __syncthreads();
+    if (t == 0) *giant = (uint32_t)(s_best & 0xFFFFFFFFull);
+}
+
+constexpr uint32_t CC_ROUNDS = 2;
+constexpr uint32_t CC_THREAD_MAX = 64; /* remaining neighbours a thread links itself */
+
+/* vertices outside the giant component link their remaining neighbours */
+__global__ void k_cc_rest(Nbrs n, uint32_t nv, const uint32_t *giant, uint32_t *parent, uint32_t *work,
+                          uint32_t *nwork) {
+    const uint32_t c = *giant;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        if (((volatile uint32_t *)parent)[v] == c) continue;
+        const uint32_t d = nbr_count(n, v);
+        if (d <= CC_ROUNDS) continue;
+        if (d - CC_ROUNDS <= CC_THREAD_MAX) {
+            for (uint32_t i = CC_ROUNDS; i < d; ++i) hook(parent, v, nbr_at(n, v, i));
+        } else {
+            work[atomicAdd(nwork, 1u)] = v;
+        }
+    }
+}
+
+__global__ void k_cc_rest_long(Nbrs n, const uint32_t *work, const uint32_t *nwork, uint32_t *parent) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = *nwork;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nw; k += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t v = work[k], d = nbr_count(n, v);
+        for (uint32_t i = CC_ROUNDS + lane; i < d; i += 32u) hook(parent, v, nbr_at(n, v, i));
+    }
+}
+
 /* Final pass: every vertex jumps to its root. The find here only reads (no path
  * halving): a halving store racing with another vertex's final store could put
  * a non-root ancestor back. The only stores are parent[v] = root(v) by v's own
@@ -126,8 +227,12 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
         GCG_TRY(parent_tmp.alloc(nv, s));
         parent = parent_tmp.get();
     }
-    GCG_TRY(cnt.alloc(1, s));
-    GCG_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
+    /* sampling needs each vertex's whole neighbourhood: symmetric in-lists, or in + out lists */
+    const bool sampled = nv > 0 && (g->symmetric || g->has_out);
+    tbuf<uint32_t> work;
+    GCG_TRY(cnt.alloc(4, s));
+    GCG_CUDA(cudaMemsetAsync(cnt.get(), 0, 16, s));
+    if (sampled) GCG_TRY(work.alloc(std::max<uint32_t>(nv, 1), s));
     unsigned vb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv + 255) / 256, (uint64_t)num_sms() * 16));
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cc_hook, MP_THREADS, 0) != cudaSuccess || per_sm <= 0) {
@@ -140,8 +245,23 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
     GCG_CUDA(cudaEventCreate(&ev1));
     GCG_CUDA(cudaEventRecord(ev0, s));
     k_cc_init<<<vb, 256, 0, s>>>(nv, parent);
-    k_cc_hook<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(), pl.tile_edge.get(),
-                                       pl.ntiles, parent);
+    if (sampled) {
+        Nbrs nb;
+        nb.rin = g->in_rowptr.get();
+        nb.cin = g->in_col.get();
+        nb.rout = g->symmetric ? nullptr : g->out_rowptr.get();
+        nb.cout = g->symmetric ? nullptr : g->out_col.get();
+        for (uint32_t r = 0; r < CC_ROUNDS; ++r) {
+            k_cc_round<<<vb, 256, 0, s>>>(nb, nv, r, parent);
+            k_cc_flatten<<<vb, 256, 0, s>>>(nv, parent);
+        }
+        k_cc_sample<<<1, 1024, 0, s>>>(parent, nv, cnt.get() + 1);
+        k_cc_rest<<<vb, 256, 0, s>>>(nb, nv, cnt.get() + 1, parent, work.get(), cnt.get() + 2);
+        k_cc_rest_long<<<num_sms() * 8, 256, 0, s>>>(nb, work.get(), cnt.get() + 2, parent);
+    } else {
+        k_cc_hook<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(),
+                                           pl.tile_edge.get(), pl.ntiles, parent);
+    }
     k_cc_compress<<<vb, 256, 0, s>>>(nv, parent, cnt.get());
     GCG_LAUNCH_CHECK();
     GCG_CUDA(cudaEventRecord(ev1, s));
@@ -154,7 +274,7 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (stats) {
-        stats->passes = 1;
+        stats->passes = sampled ? (int)CC_ROUNDS + 1 : 1;
         stats->ncomponents = nroots;
         stats->device_ms = ms;
     }

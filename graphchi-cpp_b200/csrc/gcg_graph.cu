@@ -225,6 +225,7 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
     gcg_graph *g = new gcg_graph();
     g->nv = nv;
     g->vbits = vbits;
+    g->symmetric = sym;
     g->stream = s;
     auto cleanup = [&](int st) {
         delete g;

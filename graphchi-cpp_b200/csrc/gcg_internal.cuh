@@ -133,6 +133,7 @@ struct gcg_graph {
     /* out-edges grouped by source, destinations ascending (shard order by src) */
     gcg::dbuf<uint32_t> out_rowptr, out_col;
     bool has_out = false;
+    bool symmetric = false; /* built with GCG_BUILD_SYMMETRISE: every in-list is the full neighbourhood */
     gcg::dbuf<uint32_t> indeg, outdeg;
     gcg::dbuf<uint32_t> intervals_dev; /* last vid per interval */
     uint32_t *intervals_host = nullptr;
