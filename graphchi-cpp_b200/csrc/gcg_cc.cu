@@ -16,10 +16,10 @@
  *
  * When every vertex's full neighbourhood is at hand (a symmetrised graph: the
  * in-list; otherwise the in-list plus the out-list), the edge pass samples
- * instead (the Afforest scheme): two rounds link each vertex to its first two
- * neighbours, a compress, then 1024 sampled vertices name the most frequent
- * root (the giant component); only vertices outside it link their remaining
- * neighbours (a thread per short list, a warp per long one). A skipped vertex of
+ * instead (the Afforest scheme): one pass links each vertex to its first
+ * neighbour, then the roots of 1024 sampled vertices name the most frequent
+ * one (the giant component); only vertices whose root is not it link their
+ * remaining neighbours (a thread per short list, a warp per long one). A skipped vertex of
  * the giant component loses nothing: each of its other edges is also in the
  * neighbour's list, and that neighbour links it unless it is in the giant
  * component too. The same hook keeps the labels (the minimum id per component).
@@ -105,17 +105,34 @@ __device__ __forceinline__ uint32_t nbr_at(const Nbrs &n, uint32_t v, uint32_t i
     return i < din ? n.cin[b + i] : n.cout[n.rout[v] + (i - din)];
 }
 
-/* sampling round r: link v to its r-th neighbour */
-__global__ void k_cc_round(Nbrs n, uint32_t nv, uint32_t r, uint32_t *parent) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        if (r < nbr_count(n, v)) hook(parent, v, nbr_at(n, v, r));
+/* Link of the sampling scheme: climbs one parent at a time and re-reads the
+ * larger side's parent before the CAS, so a pair already joined by another
+ * thread ends without an atomic (hub roots see many such pairs). Like hook, it
+ * only ever points a root at a smaller id. */
+__device__ __forceinline__ void link(uint32_t *parent, uint32_t u, uint32_t v) {
+    volatile uint32_t *p = parent;
+    uint32_t p1 = p[u], p2 = p[v];
+    while (p1 != p2) {
+        const uint32_t hi = p1 > p2 ? p1 : p2, lo = p1 > p2 ? p2 : p1;
+        const uint32_t ph = p[hi];
+        if (ph == lo) return;
+        if (ph == hi && atomicCAS(parent + hi, hi, lo) == hi) return;
+        p1 = p[p[hi]];
+        p2 = p[lo];
+    }
 }
 
-/* full compress between the rounds (same read-only find as the final pass) */
+/* sampling round: link v to its first CC_ROUNDS neighbours (adjacent in the
+ * list, so one sector of the column array per vertex) */
+constexpr uint32_t CC_ROUNDS = 1;
 __device__ __forceinline__ uint32_t find_root_ro(const uint32_t *parent, uint32_t x);
-__global__ void k_cc_flatten(uint32_t nv, uint32_t *parent) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        ((volatile uint32_t *)parent)[v] = find_root_ro(parent, v);
+__global__ void k_cc_rounds(Nbrs n, uint32_t nv, uint32_t *parent) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const uint32_t d = nbr_count(n, v);
+#pragma unroll
+        for (uint32_t r = 0; r < CC_ROUNDS; ++r)
+            if (r < d) link(parent, v, nbr_at(n, v, r));
+    }
 }
 
 /* the most frequent root among 1024 sampled vertices (ties: the smaller id);
@@ -128,7 +145,7 @@ __global__ void __launch_bounds__(1024) k_cc_sample(const uint32_t *parent, uint
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     z ^= z >> 31;
-    s[t] = parent[(uint32_t)(z % nv)];
+    s[t] = find_root_ro(parent, (uint32_t)(z % nv));
     if (t == 0) s_best = ~0ull;
     __syncthreads();
     for (uint32_t k = 2; k <= 1024; k <<= 1)
@@ -154,7 +171,6 @@ __global__ void __launch_bounds__(1024) k_cc_sample(const uint32_t *parent, uint
     if (t == 0) *giant = (uint32_t)(s_best & 0xFFFFFFFFull);
 }
 
-constexpr uint32_t CC_ROUNDS = 2;
 constexpr uint32_t CC_THREAD_MAX = 64; /* remaining neighbours a thread links itself */
 
 /* vertices outside the giant component link their remaining neighbours */
@@ -162,11 +178,10 @@ __global__ void k_cc_rest(Nbrs n, uint32_t nv, const uint32_t *giant, uint32_t *
                           uint32_t *nwork) {
     const uint32_t c = *giant;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        if (((volatile uint32_t *)parent)[v] == c) continue;
         const uint32_t d = nbr_count(n, v);
-        if (d <= CC_ROUNDS) continue;
+        if (d <= CC_ROUNDS || find_root(parent, v) == c) continue;
         if (d - CC_ROUNDS <= CC_THREAD_MAX) {
-            for (uint32_t i = CC_ROUNDS; i < d; ++i) hook(parent, v, nbr_at(n, v, i));
+            for (uint32_t i = CC_ROUNDS; i < d; ++i) link(parent, v, nbr_at(n, v, i));
         } else {
             work[atomicAdd(nwork, 1u)] = v;
         }
@@ -178,7 +193,7 @@ __global__ void k_cc_rest_long(Nbrs n, const uint32_t *work, const uint32_t *nwo
     const uint32_t nw = *nwork;
     for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < nw; k += (gridDim.x * blockDim.x) >> 5) {
         const uint32_t v = work[k], d = nbr_count(n, v);
-        for (uint32_t i = CC_ROUNDS + lane; i < d; i += 32u) hook(parent, v, nbr_at(n, v, i));
+        for (uint32_t i = CC_ROUNDS + lane; i < d; i += 32u) link(parent, v, nbr_at(n, v, i));
     }
 }
 
@@ -251,10 +266,7 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
         nb.cin = g->in_col.get();
         nb.rout = g->symmetric ? nullptr : g->out_rowptr.get();
         nb.cout = g->symmetric ? nullptr : g->out_col.get();
-        for (uint32_t r = 0; r < CC_ROUNDS; ++r) {
-            k_cc_round<<<vb, 256, 0, s>>>(nb, nv, r, parent);
-            k_cc_flatten<<<vb, 256, 0, s>>>(nv, parent);
-        }
+        k_cc_rounds<<<vb, 256, 0, s>>>(nb, nv, parent);
         k_cc_sample<<<1, 1024, 0, s>>>(parent, nv, cnt.get() + 1);
         k_cc_rest<<<vb, 256, 0, s>>>(nb, nv, cnt.get() + 1, parent, work.get(), cnt.get() + 2);
         k_cc_rest_long<<<num_sms() * 8, 256, 0, s>>>(nb, work.get(), cnt.get() + 2, parent);
@@ -274,7 +286,7 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (stats) {
-        stats->passes = sampled ? (int)CC_ROUNDS + 1 : 1;
+        stats->passes = sampled ? 2 : 1;
         stats->ncomponents = nroots;
         stats->device_ms = ms;
     }
