@@ -184,13 +184,27 @@ def test_cc_bitexact_vs_reference(name):
     assert st.ncomponents == int(z["cc_ncomp"])
 
 
-def test_cc_directed_weak_components_vs_oracle():
+@pytest.mark.parametrize("out_csr", [True, False])
+def test_cc_directed_weak_components_vs_oracle(out_csr):
+    # with the out-CSR the sampled scheme runs over in + out lists; without it,
+    # the one-pass hooking over every edge
     s, d = O.er_numpy(200_000, 150_000, seed=8)  # sparse: many components
     go = O.OracleGraph(s, d)
-    with gcgpu.Graph.from_edges(s, d, dedup=True) as g:
+    with gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=out_csr) as g:
         lab, st = g.connected_components()
     ref, _ = go.cc()
     assert np.array_equal(lab, ref)
+    assert st.passes == (2 if out_csr else 1)
+
+
+def test_cc_sampled_on_rmat_with_giant_component_vs_oracle():
+    for sym in (True, False):
+        s, d = O.rmat_numpy(14, 16 << 14, seed=31)
+        go = O.OracleGraph(s, d, symmetrise=sym)
+        with gcgpu.Graph.from_edges(s, d, dedup=True, symmetrise=sym) as g:
+            lab, st = g.connected_components()
+        ref, n = go.cc()
+        assert np.array_equal(lab, ref) and st.ncomponents == len(np.unique(ref))
 
 
 # ---- triangle counting ----------------------------------------------------
