@@ -18,10 +18,11 @@ int main(int argc, const char **argv) {
         metrics m("connected-components");
         std::string filename = get_option_string("file");
         int niters = get_option_int("niters", 1000);
+        bool scheduler = get_option_int("scheduler", 0) != 0; /* connectedcomponents.cpp:158 */
         int nshards = convert_if_notexists<vid_t>(filename, get_option_string("nshards", "auto"));
         if (get_option_int("onlyresult", 0) == 0) {
             ConnectedComponentsProgram program;
-            graphchi_engine<vid_t, vid_t> engine(filename, nshards, false, m);
+            graphchi_engine<vid_t, vid_t> engine(filename, nshards, scheduler, m);
             engine.run(program, niters);
         }
         m.start_time("label-analysis");

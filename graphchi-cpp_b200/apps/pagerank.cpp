@@ -3,18 +3,21 @@
  * file as example_apps/pagerank.cpp (:148-188). The vertex program is the
  * in-memory Gauss-Seidel program (pagerank.cpp:121-146), run bit-exactly by
  * gcg_pagerank(GCG_PR_GS_EXACT). Options: file, niters (4), nshards (auto),
- * top (20); tol > 0 switches to the Jacobi iteration run to that residual.
+ * top (20); tol > 0 switches to the Jacobi iteration run to that residual;
+ * scheduler=1 (with delta_threshold) to selective scheduling. Jacobi and
+ * scheduled runs write <file>.deltalog.
  */
 #include "graphchi_gpu/graphchi_gpu.hpp"
 
 using namespace graphchi;
 
 struct PagerankProgram : public GraphChiProgram<float, float> {
-    double tol = 0.0;
+    double tol = 0.0, threshold = 0.0;
     device_program device_kind() const override {
         return device_program::pagerank_vertex_api;
     }
     double tolerance() const override { return tol; }
+    double schedule_threshold() const override { return threshold; }
 };
 
 int main(int argc, const char **argv) {
@@ -25,9 +28,14 @@ int main(int argc, const char **argv) {
         int niters = get_option_int("niters", 4);
         int ntop = get_option_int("top", 20);
         int nshards = convert_if_notexists<float>(filename, get_option_string("nshards", "auto"));
-        graphchi_engine<float, float> engine(filename, nshards, false, m);
+        /* scheduler=1: selective scheduling (a vertex whose rank moves by more than
+         * delta_threshold of it schedules its out-neighbours); the reference's app
+         * runs without it (pagerank.cpp:156) */
+        const bool scheduler = get_option_int("scheduler", 0) != 0;
+        graphchi_engine<float, float> engine(filename, nshards, scheduler, m);
         PagerankProgram program;
         program.tol = atof(get_option_string("tol", "0").c_str());
+        program.threshold = atof(get_option_string("delta_threshold", "0.0001").c_str());
         engine.run(program, program.tol > 0 ? get_option_int("niters", 1000) : niters);
         std::vector<vertex_value<float>> top = get_top_vertices<float>(filename, ntop);
         std::cout << "Print top " << ntop << " vertices:" << std::endl;

@@ -292,3 +292,13 @@ extern "C" int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_s
     }
     return GCG_OK;
 }
+
+extern "C" int gcg_connected_components_ex(gcg_graph *g, const gcg_cc_params *p, uint32_t *labels,
+                                           gcg_cc_stats *stats) {
+    if (!g || !p) return fail(GCG_ERR_INVALID, "gcg_connected_components_ex: null argument");
+    if (p->algorithm == GCG_CC_UNION_FIND) return gcg_connected_components(g, labels, stats);
+    if (p->algorithm != GCG_CC_LABEL_PROPAGATION)
+        return fail(GCG_ERR_INVALID, "gcg_connected_components_ex: unknown algorithm");
+    const int iters = p->max_iterations > 0 ? p->max_iterations : 1000;
+    return cc_label_propagation(g, p->scheduler, iters, labels, stats, p->frontier_log);
+}

@@ -177,6 +177,11 @@ int ensure_plan(gcg_graph *g);
 /* exact Gauss-Seidel PageRank (gcg_pagerank_gs.cu) */
 int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats);
 
+/* selective scheduling on a device frontier (gcg_frontier.cu) */
+int pagerank_delta(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats);
+int cc_label_propagation(gcg_graph *g, int scheduler, int max_iters, uint32_t *labels, gcg_cc_stats *stats,
+                         int32_t *frontier_log);
+
 constexpr int MP_THREADS = 256;
 constexpr int MP_ITEMS = 8;
 constexpr int MP_TILE = MP_THREADS * MP_ITEMS;

@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
         const double norm = tot.y + (const_pass ? 0.0 : a.norm_const);
         const double res = norm > 0.0 ? tot.x / norm : 0.0;
         a.res_log[sweep] = res;
+        if (a.delta_log) a.delta_log[sweep] = tot.x;
         *a.last_res = res;
         *a.sweeps_done = sweep + 1;
         if (a.tol > 0.0 && res <= a.tol) *a.done = 1;
@@ -467,13 +468,13 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         GCG_TRY(w.ctl.alloc(4));
         GCG_CUDA(cudaMallocHost((void **)&w.h_flags, 64 * sizeof(int)));
     }
-    if (w.dres.n < (size_t)max_sweeps + 1) GCG_TRY(w.dres.alloc((size_t)max_sweeps + 1));
+    if (w.dres.n < 2 * (size_t)max_sweeps + 1) GCG_TRY(w.dres.alloc(2 * (size_t)max_sweeps + 1));
     dbuf<float> &r = w.r, &c = w.c, &nzsum = w.nzsum, &parts = w.parts, &rnz = w.rnz;
     dbuf<double2> &bres = w.bres;
     dbuf<uint32_t> &ctl = w.ctl; /* ticket, done, sweeps_done */
     dbuf<double> &dres = w.dres; /* res_log[max_sweeps] + last_res */
     GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 4 * sizeof(uint32_t), s));
-    GCG_CUDA(cudaMemsetAsync(dres.get(), 0, ((size_t)max_sweeps + 1) * sizeof(double), s));
+    GCG_CUDA(cudaMemsetAsync(dres.get(), 0, (2 * (size_t)max_sweeps + 1) * sizeof(double), s));
 
     /* initial vector: caller's (warm start) or the constant init */
     tbuf<float> init_stage;
@@ -520,6 +521,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     a.sweeps_done = (int *)(ctl.get() + 2);
     a.res_log = dres.get();
     a.last_res = dres.get() + max_sweeps;
+    a.delta_log = (p->delta_log || p->work_log) ? dres.get() + max_sweeps + 1 : nullptr;
     a.teleport = p->teleport;
     a.damping = p->damping;
     a.tol = p->tol;
@@ -623,6 +625,17 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     double last_res = 0.0;
     GCG_CUDA(cudaMemcpy(&last_res, a.last_res, sizeof(double), cudaMemcpyDeviceToHost));
     if (p->residuals && sweeps > 0) GCG_TRY(copy_out(p->residuals, dres.get(), (size_t)sweeps * sizeof(double), s));
+    if (p->delta_log && sweeps > 0)
+        GCG_TRY(copy_out(p->delta_log, dres.get() + max_sweeps + 1, (size_t)sweeps * sizeof(double), s));
+    if (p->work_log && sweeps > 0) { /* every vertex updated and every in-edge gathered per sweep */
+        std::vector<uint64_t> wl(2 * (size_t)sweeps);
+        for (int i = 0; i < sweeps; ++i) {
+            wl[2 * i] = (uint64_t)nv * (uint64_t)(i + 1);
+            wl[2 * i + 1] = g->ne * (uint64_t)(i + 1);
+        }
+        GCG_TRY(copy_out(p->work_log, wl.data(), wl.size() * sizeof(uint64_t), s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+    }
     if (sweeps > 0) {
         const float t = (float)p->teleport; /* teleport + damping * 0 */
         k_pr_scatter<<<grid1d(nv, 8), 256, 0, s>>>(pl.nnz, pl.nzero, pl.nz_rows.get(), pl.zero_rows.get(),
@@ -663,6 +676,9 @@ void gcg_pr_params_default(gcg_pr_params *p) {
     p->residuals = nullptr;
     p->source = GCG_NO_SOURCE;
     p->reserved2 = 0u;
+    p->delta_log = nullptr;
+    p->work_log = nullptr;
+    p->delta_threshold = 0.0;
 }
 
 int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_run) {
@@ -734,6 +750,7 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
         return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank: personalisation needs GCG_PR_JACOBI");
     if (params->mode == GCG_PR_JACOBI) return pagerank_jacobi(g, params, out_rank, stats);
     if (params->mode == GCG_PR_GS_EXACT) return pagerank_gs_exact(g, params, out_rank, stats);
+    if (params->mode == GCG_PR_DELTA) return pagerank_delta(g, params, out_rank, stats);
     return fail(GCG_ERR_INVALID, "gcg_pagerank: unknown mode");
 }
 

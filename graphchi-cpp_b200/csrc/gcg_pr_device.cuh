@@ -64,6 +64,7 @@ struct SweepArgs {
     double teleport, damping, tol, norm_const;
     uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
     uint32_t run;    /* edge kernel: each warp takes runs of this many consecutive chunks (>= 1) */
+    double *delta_log; /* optional: per sweep, sum |r' - r| (FP64) */
 };
 
 /* columns (streamed), head flags and starting row index of one chunk; ne is

@@ -36,6 +36,7 @@ CSR_IN = 0
 CSR_OUT = 1
 PR_JACOBI = 0
 PR_GS_EXACT = 1
+PR_DELTA = 2
 PR_TIME_SWEEPS = 0x1
 
 # Every symbol include/gcgpu.h declares (checked by the CPU test suite).
@@ -49,6 +50,7 @@ EXPORTED = [
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
+    "gcg_connected_components_ex",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
     "gcg_warm_start_rank",
@@ -75,7 +77,8 @@ class PrParams(C.Structure):
     _fields_ = [("mode", C.c_int), ("max_sweeps", C.c_int), ("teleport", C.c_double),
                 ("damping", C.c_double), ("tol", C.c_double), ("init", C.c_float),
                 ("flags", C.c_uint32), ("init_rank", C.c_void_p), ("residuals", C.c_void_p),
-                ("source", C.c_uint32), ("reserved2", C.c_uint32)]
+                ("source", C.c_uint32), ("reserved2", C.c_uint32), ("delta_log", C.c_void_p),
+                ("work_log", C.c_void_p), ("delta_threshold", C.c_double)]
 
 
 NO_SOURCE = 0xFFFFFFFF
@@ -94,6 +97,15 @@ class MlpTrainParams(C.Structure):
 
 class CcStats(C.Structure):
     _fields_ = [("passes", C.c_int), ("ncomponents", C.c_uint32), ("device_ms", C.c_double)]
+
+
+class CcParams(C.Structure):
+    _fields_ = [("algorithm", C.c_int), ("scheduler", C.c_int), ("max_iterations", C.c_int),
+                ("reserved", C.c_uint32), ("frontier_log", C.c_void_p)]
+
+
+CC_UNION_FIND = 0
+CC_LABEL_PROPAGATION = 1
 
 
 class TcStats(C.Structure):
@@ -123,6 +135,7 @@ _write_vout = _sig("gcg_write_vout", _i, C.c_char_p, _vp, _u32, _u32)
 _pr_default = _sig("gcg_pr_params_default", None, C.POINTER(PrParams))
 _pagerank = _sig("gcg_pagerank", _i, _vp, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
 _cc = _sig("gcg_connected_components", _i, _vp, _vp, C.POINTER(CcStats))
+_cc_ex = _sig("gcg_connected_components_ex", _i, _vp, C.POINTER(CcParams), _vp, C.POINTER(CcStats))
 _tc = _sig("gcg_triangle_count", _i, _vp, _vp, _vp, _vp, C.POINTER(TcStats))
 _gen_rmat = _sig("gcg_generate_rmat", _i, _u32, _u64, C.c_double, C.c_double, C.c_double, _u64, _vp, _vp)
 _gen_er = _sig("gcg_generate_er", _i, _u32, _u64, _u64, _vp, _vp)
@@ -271,12 +284,18 @@ class Graph:
         check(_write_meta(self._h, os.fsencode(base)))
 
     def pagerank(self, mode=PR_JACOBI, max_sweeps=3, teleport=0.15, damping=0.85, tol=0.0, init=1.0,
-                 init_rank=None, out=None, residuals=None, time_sweeps=False, source=None):
-        """Returns (ranks, PrStats). out/init_rank/residuals: numpy or device tensors."""
+                 init_rank=None, out=None, residuals=None, time_sweeps=False, source=None, delta_log=None,
+                 work_log=None, delta_threshold=0.0):
+        """Returns (ranks, PrStats). out/init_rank/residuals/delta_log/work_log: numpy or device tensors."""
         p = PrParams()
         _pr_default(C.byref(p))
         p.mode, p.max_sweeps, p.teleport, p.damping, p.tol, p.init = (
             mode, max_sweeps, teleport, damping, tol, init)
+        p.delta_threshold = delta_threshold
+        if delta_log is not None:
+            p.delta_log = ptr(delta_log)
+        if work_log is not None:
+            p.work_log = ptr(work_log)
         p.flags = PR_TIME_SWEEPS if time_sweeps else 0
         p.source = NO_SOURCE if source is None else int(source)
         if init_rank is not None:
@@ -339,11 +358,17 @@ class Graph:
         check(_warm_start(self._h, mlp.handle, teleport, damping, ptr(out), C.byref(ms)))
         return out, ms.value
 
-    def connected_components(self, out=None):
+    def connected_components(self, out=None, algorithm=None, scheduler=False, max_iterations=0,
+                             frontier_log=None):
+        """Labels (minimum id per weak component) and CcStats; algorithm None = union-find."""
         if out is None:
             out = np.zeros(self.num_vertices, dtype=np.uint32)
         st = CcStats()
-        check(_cc(self._h, ptr(out), C.byref(st)))
+        if algorithm is None:
+            check(_cc(self._h, ptr(out), C.byref(st)))
+        else:
+            p = CcParams(algorithm, 1 if scheduler else 0, max_iterations, 0, ptr(frontier_log))
+            check(_cc_ex(self._h, C.byref(p), ptr(out), C.byref(st)))
         return out, st
 
     def triangle_count(self, per_rank=True, vertexmap=True):

@@ -210,7 +210,9 @@ struct graphchi_context {
     uint64_t nedges = 0;
     std::string filename;
     double last_residual = 0.0;
+    double last_deltasum = 0.0; /* sum |change| of the last iteration (graphchi_context::get_delta) */
     void set_last_iteration(int it) { last_iteration = it; }
+    double get_delta() const { return last_deltasum; }
 };
 
 template <typename VertexDataType, typename EdgeDataType>
@@ -226,6 +228,9 @@ struct GraphChiProgram {
     virtual device_program device_kind() const = 0;
     /* Optional convergence tolerance for PageRank (0 = run niters). */
     virtual double tolerance() const { return 0.0; }
+    /* With selective scheduling: a PageRank vertex whose value moves by more than
+     * this (relative) schedules its out-neighbours (GCG_PR_DELTA). */
+    virtual double schedule_threshold() const { return 0.0; }
 };
 
 /* ---- engine ---------------------------------------------------------------- */
@@ -236,11 +241,24 @@ class graphchi_engine {
     metrics &m_;
     graphchi_context ctx_;
     int membudget_mb_;
+    bool scheduling_;
     std::shared_ptr<gpu_graph_entry> entry_;
 
+    /* <base>.deltalog, one "iteration,nupdates,work,delta" line per iteration as
+     * graphchi_engine::write_delta_log (graphchi_engine.hpp:593-599): cumulative
+     * vertex updates and edges processed, the iteration's sum of |change| */
+    void write_delta_log(const std::vector<double> &delta, const std::vector<uint64_t> &work, int n) {
+        FILE *f = fopen((base_ + ".deltalog").c_str(), "w");
+        if (!f) return;
+        for (int i = 0; i < n; ++i)
+            fprintf(f, "%d,%lu,%lu,%lf\n", i, (unsigned long)work[2 * i], (unsigned long)work[2 * i + 1], delta[i]);
+        fclose(f);
+    }
+
 public:
-    graphchi_engine(std::string base, int nshards, bool /*selective_scheduling*/, metrics &m)
-        : base_(std::move(base)), nshards_(nshards), m_(m), membudget_mb_(get_option_int("membudget_mb", 1024)) {
+    graphchi_engine(std::string base, int nshards, bool selective_scheduling, metrics &m)
+        : base_(std::move(base)), nshards_(nshards), m_(m), membudget_mb_(get_option_int("membudget_mb", 1024)),
+          scheduling_(selective_scheduling) {
         auto it = gpu_graphs().find(base_);
         if (it == gpu_graphs().end()) {
             gpu_convert(base_, std::to_string(nshards_ > 0 ? nshards_ : 1), sizeof(EdgeDataType));
@@ -298,19 +316,40 @@ public:
                 p.teleport = vapi ? 0.15 : 0.15 / (double)nv;
                 p.tol = program.tolerance();
                 if (p.tol > 0) p.mode = GCG_PR_JACOBI;
+                if (scheduling_) { /* selective scheduling on the device frontier */
+                    p.mode = GCG_PR_DELTA;
+                    p.delta_threshold = program.schedule_threshold();
+                }
                 std::vector<float> r(nv);
+                const bool logged = p.mode != GCG_PR_GS_EXACT;
+                std::vector<double> dl(logged ? std::max(1, p.max_sweeps) : 0);
+                std::vector<uint64_t> wl(logged ? 2 * (size_t)std::max(1, p.max_sweeps) : 0);
+                if (logged) {
+                    p.delta_log = dl.data();
+                    p.work_log = wl.data();
+                }
                 gcg_pr_stats st;
                 gcg_check(gcg_pagerank(entry_->g, &p, r.data(), &st), "pagerank");
                 for (uint32_t v = 0; v < nv; ++v) values[v] = (VertexDataType)r[v];
                 last = st.sweeps;
                 ctx_.last_residual = st.residual;
+                if (logged && st.sweeps > 0) {
+                    write_delta_log(dl, wl, st.sweeps);
+                    ctx_.last_deltasum = dl[st.sweeps - 1];
+                }
                 m_.add_time("device_sweeps", st.device_ms / 1000.0);
                 break;
             }
             case device_program::connected_components: {
                 std::vector<uint32_t> lab(nv);
                 gcg_cc_stats st;
-                gcg_check(gcg_connected_components(entry_->g, lab.data(), &st), "connected components");
+                if (scheduling_) { /* the reference's label propagation with its scheduler, on a device frontier */
+                    gcg_cc_params cp = {GCG_CC_LABEL_PROPAGATION, 1, std::max(1, niters), 0u, nullptr};
+                    gcg_check(gcg_connected_components_ex(entry_->g, &cp, lab.data(), &st), "connected components");
+                    last = st.passes - 1;
+                } else {
+                    gcg_check(gcg_connected_components(entry_->g, lab.data(), &st), "connected components");
+                }
                 for (uint32_t v = 0; v < nv; ++v) values[v] = (VertexDataType)lab[v];
                 m_.add_time("device_cc", st.device_ms / 1000.0);
                 break;

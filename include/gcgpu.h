@@ -116,6 +116,11 @@ int gcg_write_vout(const char *base, const void *values, uint32_t num_vertices, 
 
 #define GCG_PR_JACOBI 0   /* bulk-synchronous (functional engine, sync mode) */
 #define GCG_PR_GS_EXACT 1 /* vertex-API Gauss-Seidel in id order, bit-exact */
+#define GCG_PR_DELTA 2    /* selective scheduling: Jacobi sweeps over a device frontier
+                             (bitset_scheduler.hpp:38-104): sweep 0 updates every vertex; a vertex
+                             whose rank moved by more than delta_threshold x its rank schedules its
+                             out-neighbours for the next sweep; stops when nothing is scheduled, at
+                             tol or at max_sweeps. Needs the out-edge CSR. */
 
 typedef struct {
     int mode;               /* GCG_PR_JACOBI or GCG_PR_GS_EXACT */
@@ -130,6 +135,16 @@ typedef struct {
     uint32_t source;        /* personalisation: teleport (and the initial mass 1) only at this
                                vertex; GCG_NO_SOURCE = plain PageRank. JACOBI only. */
     uint32_t reserved2;
+    /* optional per-sweep progress log, the reference's write_delta_log line
+     * "iteration,nupdates,work,delta" (graphchi_engine.hpp:593-599): delta_log[i] = sum over
+     * vertices of |r' - r| in sweep i (FP64; graphchi_context::log_change, graphchi_context.hpp:82-106);
+     * work_log[2i], [2i+1] = vertex updates and in-edges gathered up to and including sweep i.
+     * max_sweeps entries (2 x for work_log), host or device. JACOBI and DELTA modes. */
+    double *delta_log;
+    uint64_t *work_log;
+    /* GCG_PR_DELTA: a vertex whose rank moved by more than delta_threshold x its new rank
+     * schedules its out-neighbours for the next sweep */
+    double delta_threshold;
 } gcg_pr_params;
 
 #define GCG_PR_TIME_SWEEPS 0x1u
@@ -328,6 +343,23 @@ typedef struct {
  * min-label propagation over in- and out-edges, i.e. the minimum vertex id of
  * each weakly connected component. labels: num_vertices, host or device. */
 int gcg_connected_components(gcg_graph *g, uint32_t *labels, gcg_cc_stats *stats);
+
+#define GCG_CC_UNION_FIND 0        /* hook-and-compress (gcg_connected_components) */
+#define GCG_CC_LABEL_PROPAGATION 1 /* the reference's update rule, iterated to its fixpoint */
+typedef struct {
+    int algorithm;      /* GCG_CC_UNION_FIND or GCG_CC_LABEL_PROPAGATION */
+    int scheduler;      /* label propagation: 1 = selective scheduling on a device frontier, as the
+                           reference's scheduler=1 (bitset_scheduler.hpp:38-104): only vertices whose
+                           label may drop are updated; 0 = every vertex every iteration */
+    int max_iterations; /* label propagation: cap (0 = 1000, connectedcomponents.cpp:165) */
+    uint32_t reserved;
+    int32_t *frontier_log; /* optional: per iteration, vertices updated (max_iterations ints, host or device) */
+} gcg_cc_params;
+/* Same labels as gcg_connected_components (the minimum id per weak component)
+ * by the chosen algorithm; label propagation needs whole neighbourhoods (a graph
+ * built with GCG_BUILD_SYMMETRISE, or with its out-edge CSR). stats->passes =
+ * iterations run. */
+int gcg_connected_components_ex(gcg_graph *g, const gcg_cc_params *p, uint32_t *labels, gcg_cc_stats *stats);
 
 /* ---- triangle counting ------------------------------------------------- */
 
