@@ -218,6 +218,21 @@ int gcg_graph_free(gcg_graph *g) {
     return GCG_OK;
 }
 
+int gcg_graph_get_device_view(const gcg_graph *g, gcg_graph_device_view *v) {
+    if (!g || !v) return fail(GCG_ERR_INVALID, "gcg_graph_get_device_view: null argument");
+    v->in_rowptr = g->in_rowptr.get();
+    v->in_col = g->in_col.get();
+    v->out_rowptr = g->has_out ? g->out_rowptr.get() : nullptr;
+    v->out_col = g->has_out ? g->out_col.get() : nullptr;
+    v->indeg = g->indeg.get();
+    v->outdeg = g->outdeg.get();
+    v->num_vertices = g->nv;
+    v->reserved = 0;
+    v->num_edges = g->ne;
+    v->stream = (void *)g->stream;
+    return GCG_OK;
+}
+
 int gcg_graph_get_info(const gcg_graph *g, gcg_graph_info *info) {
     if (!g || !info) return fail(GCG_ERR_INVALID, "gcg_graph_get_info: null argument");
     info->num_vertices = g->nv;

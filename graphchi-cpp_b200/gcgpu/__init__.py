@@ -50,7 +50,7 @@ EXPORTED = [
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
-    "gcg_connected_components_ex",
+    "gcg_connected_components_ex", "gcg_graph_get_device_view",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
     "gcg_warm_start_rank",

@@ -41,6 +41,14 @@
 
 #include "gcgpu.h"
 
+/* functions a functional kernel's methods may carry: callable from device code
+ * when the including file is compiled by nvcc (graphchi_gpu/functional_gpu.cuh) */
+#ifdef __CUDACC__
+#define GCG_HD __host__ __device__
+#else
+#define GCG_HD
+#endif
+
 namespace graphchi {
 
 typedef uint32_t vid_t;
@@ -202,17 +210,43 @@ enum class device_program {
     triangle_counting     /* example_apps/trianglecounting.cpp */
 };
 
+/* graphchi_context (graphchi_context.hpp:45-106): plain data, so that device
+ * code of a functional kernel can read it (the filename is borrowed) */
 struct graphchi_context {
     int iteration = 0;
     int num_iterations = 0;
     int last_iteration = -1;
     uint64_t nvertices = 0;
     uint64_t nedges = 0;
-    std::string filename;
+    const char *filename = nullptr;
     double last_residual = 0.0;
     double last_deltasum = 0.0; /* sum |change| of the last iteration (graphchi_context::get_delta) */
-    void set_last_iteration(int it) { last_iteration = it; }
-    double get_delta() const { return last_deltasum; }
+    GCG_HD void set_last_iteration(int it) { last_iteration = it; }
+    GCG_HD double get_delta() const { return last_deltasum; }
+};
+
+/* vertex_info of the functional API (functional_defs.hpp:36-40) */
+struct vertex_info {
+    vid_t vertexid;
+    int indegree;
+    int outdegree;
+};
+
+/* Base of a functional (gather-apply-scatter) kernel (functional_api.hpp:54-75).
+ * A kernel defines, with GCG_HD on each so the device can call them:
+ *   VT initial_value(graphchi_context&, vertex_info&)           iteration 0
+ *   VT reset()                                                   before the gather
+ *   ET op_neighborval(graphchi_context&, vertex_info&, vid_t nb, ET nbval)   gather
+ *   VT plus(VT curval, ET toadd)                                 sum
+ *   VT compute_vertexvalue(graphchi_context&, vertex_info&, VT sum)          apply
+ *   ET value_to_neighbor(graphchi_context&, vertex_info&, vid_t nb, VT val)  scatter
+ * and runs with run_functional_unweighted_synchronous<KERNEL> from
+ * graphchi_gpu/functional_gpu.cuh. The methods are called on the kernel's own type
+ * (no virtual dispatch), so the device runs them directly. */
+template <typename FVertexDataType, typename FEdgeDataType>
+struct functional_kernel {
+    typedef FVertexDataType VertexDataType;
+    typedef FEdgeDataType EdgeDataType;
 };
 
 template <typename VertexDataType, typename EdgeDataType>
@@ -297,7 +331,7 @@ public:
     void run(GraphChiProgram<VertexDataType, EdgeDataType> &program, int niters) {
         m_.start_time("runtime");
         const uint32_t nv = (uint32_t)num_vertices();
-        ctx_.filename = base_;
+        ctx_.filename = base_.c_str();
         ctx_.num_iterations = niters;
         ctx_.nvertices = nv;
         ctx_.nedges = num_edges();

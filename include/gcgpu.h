@@ -101,6 +101,21 @@ int gcg_graph_degrees(const gcg_graph *g, int32_t *pairs);
 /* Copies a CSR: rowptr (num_vertices+1) and col (num_edges), host or device. */
 int gcg_graph_csr(const gcg_graph *g, int which, uint32_t *rowptr, uint32_t *col);
 
+/* Borrowed device pointers to a graph's resident arrays, for callers that run
+ * their own kernels over it (the functional plug-in of graphchi_gpu does). Valid
+ * until gcg_graph_free; read-only; out_rowptr/out_col are NULL when the graph was
+ * built without its out-edge CSR. No counterpart in the reference (its shards are
+ * files). */
+typedef struct {
+    const uint32_t *in_rowptr, *in_col;   /* in-edges by destination, sources ascending */
+    const uint32_t *out_rowptr, *out_col; /* out-edges by source, destinations ascending */
+    const uint32_t *indeg, *outdeg;
+    uint32_t num_vertices, reserved;
+    uint64_t num_edges;
+    void *stream; /* the graph's stream (cudaStream_t) */
+} gcg_graph_device_view;
+int gcg_graph_get_device_view(const gcg_graph *g, gcg_graph_device_view *view);
+
 /* Writes the sharder's metadata files for `base`: <base>.<P>.intervals,
  * <base>.numvertices and <base>_degs.bin (sharder.hpp:909-926, :996-1006), so the
  * reference's readers (load_vertex_intervals, degree_data) accept the graph. */

@@ -65,3 +65,16 @@ def test_trianglecounting_app(edgelist):
     total, _, _ = go.tc()
     out = run("trianglecounting", f"file={path}", f"assertequals={int(total)}")
     assert str(int(total)) in out
+
+
+@pytest.mark.parametrize("mode", ["sync", "semisync"])
+def test_pagerank_functional_app_runs_the_kernel_on_the_device(edgelist, mode):
+    # the reference's functional kernel (gather / apply / scatter methods) compiled
+    # with nvcc and run by graphchi_gpu/functional_gpu.cuh: bulk-synchronous
+    # PageRank with teleport 0.15/N, as pagerank_functional --mode sync
+    path, go = edgelist
+    run("pagerank_functional", f"file={path}", "niters=10", f"mode={mode}")
+    got = O.read_vout(path, np.float32)[:go.nv].astype(np.float64)
+    ref, _, _ = go.pagerank_jacobi(teleport=0.15 / go.nv, damping=0.85, init=1.0, max_sweeps=9)
+    ref = np.asarray(ref, np.float64)
+    assert np.abs(got - ref).sum() / np.abs(ref).sum() <= 1e-6
