@@ -106,30 +106,56 @@ __global__ void k_degree(const uint32_t *__restrict__ rowptr, uint32_t nv, uint3
         deg[v] = rowptr[v + 1] - rowptr[v];
 }
 
-__global__ void k_outdeg_hist(const uint32_t *__restrict__ col, uint64_t n, uint32_t *__restrict__ outdeg) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(outdeg + col[i], 1u);
+/* Out-degrees as a histogram of the sources. Counts of ids below OUTDEG_WIN go
+ * to per-block shared-memory counters first (the most-cited sources of power-law
+ * graphs, R-MAT's among them, have small ids; this takes their contention off
+ * the global atomics) and are added to the global counts once per block. */
+constexpr uint32_t OUTDEG_WIN = 32768;
+__global__ void __launch_bounds__(1024) k_outdeg_hist(const uint32_t *__restrict__ col, uint64_t n,
+                                                      uint32_t win, uint32_t *__restrict__ outdeg) {
+    extern __shared__ uint32_t s_cnt[];
+    for (uint32_t i = threadIdx.x; i < win; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t u = col[i];
+        if (u < win) atomicAdd(s_cnt + u, 1u);
+        else atomicAdd(outdeg + u, 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < win; i += blockDim.x)
+        if (s_cnt[i]) atomicAdd(outdeg + i, s_cnt[i]);
 }
 
+/* largest r in [0, nv) with rowptr[r] <= x (the non-empty row holding edge x);
+ * called by a whole warp: 32 probes per step, about log32(nv) dependent loads */
 __device__ uint32_t row_of(const uint32_t *rowptr, uint32_t nv, uint32_t x) {
-    /* largest r in [0, nv) with rowptr[r] <= x (the non-empty row holding edge x) */
+    const uint32_t lane = threadIdx.x & 31u;
     uint32_t lo = 0, hi = nv; /* answer in [lo, hi) */
     while (hi - lo > 1) {
-        uint32_t mid = lo + (hi - lo) / 2;
-        if (rowptr[mid] <= x) lo = mid; else hi = mid;
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t probe = lo + lane * step; /* probe 0 is lo itself, and rowptr[lo] <= x */
+        const bool ok = probe < hi && rowptr[probe] <= x;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok) | 1u;
+        const uint32_t nlo = lo + (31u - __clz(m)) * step; /* the largest probe <= x */
+        hi = nlo + step < hi ? nlo + step : hi;
+        lo = nlo;
     }
     return lo;
 }
 
-/* One thread: the k-way merge sink's interval cuts (sharder.hpp:861-892, :962). */
+/* One warp: the k-way merge sink's interval cuts (sharder.hpp:861-892, :962).
+ * Every lane follows the same cuts (the searches are warp-wide); lane 0 writes. */
 __global__ void k_intervals(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t P, uint32_t *last,
                             uint32_t *count) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const bool lead = threadIdx.x == 0;
     const uint64_t E = rowptr[nv];
     const uint32_t max_vid = nv - 1;
     if (E == 0 || P <= 1) {
-        last[0] = max_vid;
-        *count = 1;
+        if (lead) {
+            last[0] = max_vid;
+            *count = 1;
+        }
         return;
     }
     uint64_t eps = E / P + 1, base = 0;
@@ -140,12 +166,17 @@ __global__ void k_intervals(const uint32_t *__restrict__ rowptr, uint32_t nv, ui
         uint32_t r = row_of(rowptr, nv, (uint32_t)target);
         uint64_t j = (rowptr[r] == target) ? target : (uint64_t)rowptr[r + 1];
         if (j >= E) break;
-        last[shard++] = row_of(rowptr, nv, (uint32_t)(j - 1));
+        const uint32_t cut = row_of(rowptr, nv, (uint32_t)(j - 1));
+        if (lead) last[shard] = cut;
+        ++shard;
         eps = (E - j) / (P - shard);
         base = j;
     }
-    last[shard] = (shard == P - 1) ? max_vid : row_of(rowptr, nv, (uint32_t)(E - 1));
-    *count = shard + 1;
+    const uint32_t fin = (shard == P - 1) ? max_vid : row_of(rowptr, nv, (uint32_t)(E - 1));
+    if (lead) {
+        last[shard] = fin;
+        *count = shard + 1;
+    }
 }
 
 }  // namespace
@@ -284,7 +315,13 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         cudaMemsetAsync(g->outdeg.get(), 0, (size_t)nv * 4, s);
         if (ne > 0) {
             /* sources are the low halves of the sorted keys; take them from in_col */
-            k_outdeg_hist<<<grid_for(ne), 256, 0, s>>>(g->in_col.get(), ne, g->outdeg.get());
+            const uint32_t win = std::min<uint32_t>(nv, OUTDEG_WIN);
+            static bool attr = false;
+            if (!attr) {
+                cudaFuncSetAttribute(k_outdeg_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(OUTDEG_WIN * 4));
+                attr = true;
+            }
+            k_outdeg_hist<<<num_sms(), 1024, (size_t)win * 4, s>>>(g->in_col.get(), ne, win, g->outdeg.get());
         }
     }
     /* intervals */

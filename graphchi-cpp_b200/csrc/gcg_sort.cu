@@ -4,12 +4,14 @@
  * shard_flushinfo::flush sharder.hpp:192 and finish_shard sharder.hpp:640).
  *
  * Design (HBM-bound integer work, no tensor cores):
- *   per 8-bit digit pass: upsweep (per-tile digit histogram, warp-aggregated with
- *   __match_any_sync, no atomics) -> exclusive scan of the digit-major count table
- *   -> downsweep (stable in-tile ranking in 16 rounds of 256 keys, keys regrouped
- *   by digit in shared memory, then written so that each digit run of a tile is a
- *   contiguous, coalesced store).
- * Tiles are 4096 keys (256 threads x 16); keys are read with striped, coalesced loads.
+ *   per 8-bit digit pass: upsweep (per-tile digit histogram, per-warp shared-memory
+ *   counters) -> exclusive scan of the digit-major count table -> downsweep (each
+ *   warp ranks its own contiguous 512 keys with warp-private digit counters and
+ *   __match_any_sync, one digit-major scan over (digit, warp) gives every key its
+ *   place in the tile, keys are regrouped by digit in shared memory and written so
+ *   that each digit run of a tile is a contiguous, coalesced store).
+ * Tiles are 4096 keys (256 threads x 16); each warp reads its 512 keys as 16
+ * coalesced rounds of 32.
  */
 #include "gcg_internal.cuh"
 
@@ -28,27 +30,29 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+/* Warp w of a tile owns the contiguous keys [w*WSEG, (w+1)*WSEG) of the tile and
+ * reads them as RS_ITEMS coalesced rounds of 32; keeping each warp's keys
+ * contiguous lets the downsweep rank them with warp-private counters and stay
+ * stable (tile order = warp order, then round, then lane). */
+constexpr int RS_WSEG = RS_TILE / RS_WARPS;
+
 __global__ void __launch_bounds__(RS_THREADS) rs_upsweep(const uint64_t *__restrict__ keys, uint64_t n,
                                                          int shift, uint32_t dmask, uint32_t ntiles,
                                                          uint32_t *__restrict__ counts) {
     __shared__ uint32_t hist[RS_WARPS][256];
     for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS) (&hist[0][0])[i] = 0;
     __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t wbase = (uint64_t)blockIdx.x * RS_TILE + (uint64_t)warp * RS_WSEG;
     uint32_t dig[RS_ITEMS];
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
-        uint64_t i = base + (uint64_t)k * RS_THREADS + threadIdx.x;
+        const uint64_t i = wbase + (uint64_t)k * 32 + lane;
         dig[k] = (i < n) ? (uint32_t)((__ldg(keys + i) >> shift) & dmask) : 256u;
     }
 #pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
-        uint32_t d = dig[k];
-        uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        if (d < 256u && lane == __ffs(peers) - 1) hist[warp][d] += __popc(peers);
-        __syncwarp();
-    }
+    for (int k = 0; k < RS_ITEMS; ++k)
+        if (dig[k] < 256u) atomicAdd(&hist[warp][dig[k]], 1u);
     __syncthreads();
     uint32_t s = 0;
 #pragma unroll
@@ -89,50 +93,64 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint64_t *__res
     __shared__ uint64_t s_keys[RS_TILE];
     __shared__ uint32_t s_gofs[256];
     __shared__ uint32_t s_lstart[256];
-    __shared__ uint16_t s_wcnt[RS_WARPS][256];
-    __shared__ uint16_t s_wpre[RS_WARPS][256];
+    __shared__ uint32_t s_wcnt[RS_WARPS][256]; /* per warp: keys of each digit (then the warp's offset) */
     __shared__ uint32_t s_scan[RS_WARPS];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
     const uint32_t tile_n = (n - base) < (uint64_t)RS_TILE ? (uint32_t)(n - base) : (uint32_t)RS_TILE;
+    const uint64_t wbase = base + (uint64_t)warp * RS_WSEG;
 
     uint64_t key[RS_ITEMS];
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
-        uint64_t i = base + (uint64_t)k * RS_THREADS + tid;
+        const uint64_t i = wbase + (uint64_t)k * 32 + lane;
         key[k] = (i < n) ? __ldg(keys_in + i) : 0ull;
     }
-    s_gofs[tid] = offsets[(uint64_t)tid * ntiles + blockIdx.x];
-    uint32_t h = counts[(uint64_t)tid * ntiles + blockIdx.x];
     for (int w = 0; w < RS_WARPS; ++w) s_wcnt[w][tid] = 0;
-    uint32_t lstart = block_excl_scan(h, s_scan);
+    s_gofs[tid] = offsets[(uint64_t)tid * ntiles + blockIdx.x];
+    const uint32_t h = counts[(uint64_t)tid * ntiles + blockIdx.x];
+    const uint32_t lstart = block_excl_scan(h, s_scan); /* synchronises: s_wcnt is clear */
     s_lstart[tid] = lstart;
-    uint32_t run = 0; /* owner thread tid keeps the running count of digit tid */
-    __syncthreads();
 
-#pragma unroll 1
+    /* warp-private ranking over the warp's 16 rounds, in key order */
+    uint16_t lrank[RS_ITEMS];
+#pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
-        const bool valid = (uint64_t)k * RS_THREADS + tid < tile_n;
+        const uint64_t i = wbase + (uint64_t)k * 32 + lane;
+        const bool valid = i < n;
         const uint32_t d = valid ? (uint32_t)((key[k] >> shift) & dmask) : 256u;
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t rank = __popc(peers & lanemask_lt());
-        if (valid && lane == __ffs(peers) - 1) s_wcnt[warp][d] = (uint16_t)__popc(peers);
-        __syncthreads();
+        const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
+        lrank[k] = (uint16_t)(before + __popc(peers & lanemask_lt()));
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) s_wcnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    /* digit-major offsets: digit d's keys of warp w start after those of warps < w */
+    {
+        uint32_t run = s_lstart[tid];
 #pragma unroll
         for (int w = 0; w < RS_WARPS; ++w) {
-            uint32_t c = s_wcnt[w][tid];
-            s_wpre[w][tid] = (uint16_t)run;
-            s_wcnt[w][tid] = 0;
+            const uint32_t c = s_wcnt[w][tid];
+            s_wcnt[w][tid] = run;
             run += c;
         }
-        __syncthreads();
-        if (valid) s_keys[s_lstart[d] + s_wpre[warp][d] + rank] = key[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const uint64_t i = wbase + (uint64_t)k * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)((key[k] >> shift) & dmask);
+            s_keys[s_wcnt[warp][d] + lrank[k]] = key[k];
+        }
     }
     __syncthreads();
     for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
-        uint64_t kk = s_keys[i];
-        uint32_t d = (uint32_t)((kk >> shift) & dmask);
+        const uint64_t kk = s_keys[i];
+        const uint32_t d = (uint32_t)((kk >> shift) & dmask);
         keys_out[(uint64_t)s_gofs[d] + (i - s_lstart[d])] = kk;
     }
 }
