@@ -127,21 +127,24 @@ def reference_pagerank_sample(scale, ef, seed, niters, threads, steps=1, warmup=
     s, d = gcgpu.generate_rmat(scale, ef << scale, seed=seed)
     cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
     E = int(cs.shape[0])
-    vals = []
+    vals, walls = [], []
     with O.RefWorkdir(prefix="gcg_bench_ref_") as w:
         el = w.file("g.el")
         O.write_edgelist(el, cs, cd)
-        # sharding (untimed preparation): a 1-iteration run creates the shards
-        O.run_ref("pagerank", el, {"niters": 1, "nshards": "auto"}, threads)
+        # sharding (timed separately): a 1-iteration run converts the edge list into shards
+        _, shard_wall = O.run_ref("pagerank", el, {"niters": 1, "nshards": "auto"}, threads)
         for i in range(warmup + steps):
             out, wall = O.run_ref("pagerank", el, {"niters": niters, "nshards": "auto"}, threads)
             rt = O.ref_runtime(out) or wall
             if i >= warmup:
                 vals.append(E * niters / rt / 1e9)
+                walls.append(wall)
     sample = (f"oracle/_ref/pagerank (example_apps/pagerank.cpp, in-memory vertex program) on R-MAT scale {scale} "
               f"ef {ef} seed {seed} ({E} edges after dedup), {niters} iterations, engine 'runtime' metric, "
               f"GTEPS = edges x iterations / runtime, shards prepared untimed, membudget 800 MB")
-    return vals, E, sample
+    extra = {"first_run_wall_s_with_sharding": shard_wall, "run_wall_s": walls,
+             "engine_runtime_s": [E * niters / v / 1e9 for v in vals]}
+    return vals, E, sample, extra
 
 
 def run_reference(args, rank, world):
@@ -149,8 +152,8 @@ def run_reference(args, rank, world):
         return
     threads = os.cpu_count() or 1
     try:
-        vals, E, sample = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters, threads,
-                                                    steps=args.steps, warmup=args.warmup)
+        vals, E, sample, _ = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters, threads,
+                                                       steps=args.steps, warmup=args.warmup)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"[:300]}))
         return
@@ -188,6 +191,24 @@ def run_extras(args):
         d = torch.empty(m, dtype=torch.int32, device="cuda")
         gcgpu.generate_rmat(scale, m, *abc, seed=seed, src=s, dst=d)
         return s, d
+
+    # ---- the device sharder on the headline input (edges already on the device) ----
+    m = args.ef << args.scale
+    s, d = dev_edges(args.scale, m, args.seed)
+    t_build = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gb = gcgpu.Graph.from_edges(s, d, dedup=True, nshards=args.nshards, out_csr=False)
+        torch.cuda.synchronize()
+        t_build.append((time.perf_counter() - t0) * 1e3)
+        gb.free()
+    del s, d
+    bms = min(t_build[1:])
+    out["sharder"] = {"raw_edges": m, "ms": bms, "first_call_ms": t_build[0], "sort_bytes_16E": 16.0 * m,
+                      "frac_of_16E_at_hbm_peak": 16.0 * m / peak / 1e6 / bms,
+                      "note": "dedup + in-CSR + degrees + 64 intervals; the LSD sort makes 2b/8 passes of "
+                              "24 bytes per key (b = bits of a vertex id), so 16E is a one-pass lower bound"}
 
     # ---- connected components (and triangles at scale 20) ----
     cc = {}
@@ -372,9 +393,14 @@ def run_ours(args, rank, world):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            vals, Es, sample = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters,
-                                                         os.cpu_count() or 1)
+            vals, Es, sample, extra = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters,
+                                                                os.cpu_count() or 1)
             cpu = {"value": vals[0], "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": sample}
+            cpu.update(extra)
+            # the headline workload at the sample's rate: edges x sweeps of one solve / edges per second
+            cpu["estimated_s_to_tol_at_headline_size"] = E * sweeps[0] / (vals[0] * 1e9)
+            cpu["estimate_note"] = ("per-iteration rate of the sample x the sweeps the headline solve needs; "
+                                    "the reference's PageRank has no residual stop (pagerank.cpp)")
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"[:300]}
