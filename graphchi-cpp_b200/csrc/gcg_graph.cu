@@ -257,6 +257,8 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
     g->nv = nv;
     g->vbits = vbits;
     g->symmetric = sym;
+    g->build_flags = flags;
+    g->nshards_req = nshards ? nshards : 1;
     g->stream = s;
     auto cleanup = [&](int st) {
         delete g;
@@ -343,11 +345,215 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
 }
 
 }  // namespace
+namespace {
+
+/* ---- edge updates (dynamic graphs) ------------------------------------------ */
+
+/* every edge of the in-CSR as (src, dst): a warp per row */
+__global__ void k_edges_of(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
+                           uint32_t *__restrict__ src, uint32_t *__restrict__ dst) {
+    const uint32_t lane = threadIdx.x & 31u, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarps)
+        for (uint32_t i = rowptr[v] + lane; i < rowptr[v + 1]; i += 32u) {
+            src[i] = col[i];
+            dst[i] = v;
+        }
+}
+
+/* the added edges after the existing ones; both directions for a symmetric graph */
+__global__ void k_append_edges(const uint32_t *__restrict__ s, const uint32_t *__restrict__ d, uint64_t m, int both,
+                               uint64_t off, uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
+                               uint32_t *__restrict__ maxid) {
+    uint32_t mx = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = s[i], b = d[i];
+        src[off + i] = a;
+        dst[off + i] = b;
+        if (both) {
+            src[off + m + i] = b;
+            dst[off + m + i] = a;
+        }
+        mx = max(mx, max(a, b));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if ((threadIdx.x & 31u) == 0) atomicMax(maxid, mx);
+}
+
+/* keys (dst << vbits | src) of the edges to delete; ids outside the graph can
+ * match nothing and become the all-ones key */
+__global__ void k_delete_keys(const uint32_t *__restrict__ s, const uint32_t *__restrict__ d, uint64_t m, int both,
+                              uint32_t nv, uint32_t vbits, uint64_t *__restrict__ keys) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = s[i], b = d[i];
+        const bool ok = a < nv && b < nv;
+        keys[i] = ok ? (((uint64_t)b << vbits) | a) : ~0ull;
+        if (both) keys[m + i] = ok ? (((uint64_t)a << vbits) | b) : ~0ull;
+    }
+}
+
+/* keep[i] = 1 unless edge i's key is in the sorted delete list */
+__global__ void k_keep_flags(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
+                             const uint64_t *__restrict__ del, uint64_t nd, uint32_t vbits, uint32_t *__restrict__ keep) {
+    const uint32_t lane = threadIdx.x & 31u, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarps)
+        for (uint32_t i = rowptr[v] + lane; i < rowptr[v + 1]; i += 32u) {
+            const uint64_t key = ((uint64_t)v << vbits) | col[i];
+            uint64_t lo = 0, hi = nd;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (del[mid] < key) lo = mid + 1; else hi = mid;
+            }
+            keep[i] = (lo < nd && del[lo] == key) ? 0u : 1u;
+        }
+}
+
+__global__ void k_compact_edges(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
+                                const uint32_t *__restrict__ keep, const uint32_t *__restrict__ pos,
+                                uint32_t *__restrict__ src, uint32_t *__restrict__ dst) {
+    const uint32_t lane = threadIdx.x & 31u, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < nv; v += nwarps)
+        for (uint32_t i = rowptr[v] + lane; i < rowptr[v + 1]; i += 32u)
+            if (keep[i]) {
+                src[pos[i]] = col[i];
+                dst[pos[i]] = v;
+            }
+}
+
+/* g takes over ng's arrays, plans and sizes (its handle and stream stay); ng
+ * leaves with g's old ones and is deleted by the caller */
+void swap_graph(gcg_graph *g, gcg_graph *ng) {
+    std::swap(g->nv, ng->nv);
+    std::swap(g->ne, ng->ne);
+    std::swap(g->nshards, ng->nshards);
+    std::swap(g->vbits, ng->vbits);
+    auto sw = [](dbuf<uint32_t> &a, dbuf<uint32_t> &b) {
+        std::swap(a.p, b.p);
+        std::swap(a.n, b.n);
+    };
+    sw(g->in_rowptr, ng->in_rowptr);
+    sw(g->in_col, ng->in_col);
+    sw(g->out_rowptr, ng->out_rowptr);
+    sw(g->out_col, ng->out_col);
+    sw(g->indeg, ng->indeg);
+    sw(g->outdeg, ng->outdeg);
+    sw(g->intervals_dev, ng->intervals_dev);
+    std::swap(g->has_out, ng->has_out);
+    std::swap(g->intervals_host, ng->intervals_host);
+    std::swap(g->plan, ng->plan);
+    std::swap(g->cplan, ng->cplan);
+    std::swap(g->pplan, ng->pplan);
+}
+
+int rebuild_from(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t nv) {
+    if (m > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "edge update: more than 2^32-1 edges");
+    gcg_graph *ng = nullptr;
+    /* the edge list already holds both directions of a symmetric graph */
+    GCG_TRY(build_graph(src, dst, m, nv, g->build_flags & ~GCG_BUILD_SYMMETRISE, g->nshards_req, &ng));
+    cudaStreamSynchronize(g->stream);
+    swap_graph(g, ng);
+    delete ng; /* the old arrays and the plans built for them */
+    return GCG_OK;
+}
+
+int add_edges(gcg_graph *g, const uint32_t *s_u, const uint32_t *d_u, uint64_t m) {
+    cudaStream_t s = 0;
+    GCG_CUDA(cudaStreamSynchronize(g->stream));
+    tbuf<uint32_t> sb, db, src, dst, mx;
+    const uint32_t *sa = s_u, *da = d_u;
+    if (m > 0 && !is_device_ptr(s_u)) {
+        GCG_TRY(sb.alloc(m, s));
+        GCG_TRY(copy_in(sb.get(), s_u, m * 4, s));
+        sa = sb.get();
+    }
+    if (m > 0 && !is_device_ptr(d_u)) {
+        GCG_TRY(db.alloc(m, s));
+        GCG_TRY(copy_in(db.get(), d_u, m * 4, s));
+        da = db.get();
+    }
+    const int both = g->symmetric ? 1 : 0;
+    const uint64_t total = g->ne + (both ? 2 * m : m);
+    if (total > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: more than 2^32-1 edges");
+    GCG_TRY(src.alloc(std::max<uint64_t>(total, 1), s));
+    GCG_TRY(dst.alloc(std::max<uint64_t>(total, 1), s));
+    GCG_TRY(mx.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(mx.get(), 0, 4, s));
+    if (g->ne) k_edges_of<<<grid_for((uint64_t)g->nv * 32), 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), g->nv,
+                                                                         src.get(), dst.get());
+    if (m) k_append_edges<<<grid_for(m), 256, 0, s>>>(sa, da, m, both, g->ne, src.get(), dst.get(), mx.get());
+    GCG_LAUNCH_CHECK();
+    uint32_t maxid = 0;
+    GCG_CUDA(cudaMemcpyAsync(&maxid, mx.get(), 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    const uint64_t nv = std::max<uint64_t>(g->nv, m ? (uint64_t)maxid + 1 : 0);
+    if (nv > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: vertex id 2^32-1 is reserved");
+    return rebuild_from(g, src.get(), dst.get(), total, (uint32_t)nv);
+}
+
+int delete_edges(gcg_graph *g, const uint32_t *s_u, const uint32_t *d_u, uint64_t m) {
+    cudaStream_t s = 0;
+    GCG_CUDA(cudaStreamSynchronize(g->stream));
+    if (m == 0 || g->ne == 0) return GCG_OK;
+    tbuf<uint32_t> sb, db, keep, src, dst, total;
+    tbuf<uint64_t> keys, tmp;
+    const uint32_t *sa = s_u, *da = d_u;
+    if (!is_device_ptr(s_u)) {
+        GCG_TRY(sb.alloc(m, s));
+        GCG_TRY(copy_in(sb.get(), s_u, m * 4, s));
+        sa = sb.get();
+    }
+    if (!is_device_ptr(d_u)) {
+        GCG_TRY(db.alloc(m, s));
+        GCG_TRY(copy_in(db.get(), d_u, m * 4, s));
+        da = db.get();
+    }
+    const int both = g->symmetric ? 1 : 0;
+    const uint64_t nd = both ? 2 * m : m;
+    GCG_TRY(keys.alloc(nd, s));
+    GCG_TRY(tmp.alloc(nd, s));
+    k_delete_keys<<<grid_for(m), 256, 0, s>>>(sa, da, m, both, g->nv, g->vbits, keys.get());
+    GCG_LAUNCH_CHECK();
+    uint64_t *sorted = nullptr;
+    GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nd, 0, 64, &sorted, s));
+    const uint64_t ne = g->ne;
+    GCG_TRY(keep.alloc(ne, s));
+    GCG_TRY(total.alloc(1, s));
+    const unsigned wb = grid_for((uint64_t)g->nv * 32);
+    k_keep_flags<<<wb, 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), g->nv, sorted, nd, g->vbits, keep.get());
+    GCG_LAUNCH_CHECK();
+    tbuf<uint32_t> pos;
+    GCG_TRY(pos.alloc(ne, s));
+    GCG_TRY(scan_u32(keep.get(), pos.get(), ne, total.get(), s));
+    uint32_t kept = 0;
+    GCG_CUDA(cudaMemcpyAsync(&kept, total.get(), 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    if (kept == ne) return GCG_OK; /* nothing listed was present */
+    GCG_TRY(src.alloc(std::max<uint32_t>(kept, 1), s));
+    GCG_TRY(dst.alloc(std::max<uint32_t>(kept, 1), s));
+    k_compact_edges<<<wb, 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), g->nv, keep.get(), pos.get(), src.get(),
+                                       dst.get());
+    GCG_LAUNCH_CHECK();
+    return rebuild_from(g, src.get(), dst.get(), kept, g->nv);
+}
+
+}  // namespace
+
 }  // namespace gcg
 
 using namespace gcg;
 
 extern "C" {
+
+int gcg_graph_add_edges(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_graph_add_edges: null graph");
+    if (m > 0 && (!src || !dst)) return fail(GCG_ERR_INVALID, "gcg_graph_add_edges: null edge arrays");
+    return add_edges(g, src, dst, m);
+}
+
+int gcg_graph_delete_edges(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_graph_delete_edges: null graph");
+    if (m > 0 && (!src || !dst)) return fail(GCG_ERR_INVALID, "gcg_graph_delete_edges: null edge arrays");
+    return delete_edges(g, src, dst, m);
+}
 
 int gcg_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t num_vertices,
                          uint32_t flags, uint32_t nshards, gcg_graph **out) {

@@ -134,6 +134,7 @@ struct gcg_graph {
     gcg::dbuf<uint32_t> out_rowptr, out_col;
     bool has_out = false;
     bool symmetric = false; /* built with GCG_BUILD_SYMMETRISE: every in-list is the full neighbourhood */
+    uint32_t build_flags = 0, nshards_req = 1; /* how it was built (edge updates rebuild the same way) */
     gcg::dbuf<uint32_t> indeg, outdeg;
     gcg::dbuf<uint32_t> intervals_dev; /* last vid per interval */
     uint32_t *intervals_host = nullptr;

@@ -50,7 +50,7 @@ EXPORTED = [
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
-    "gcg_connected_components_ex", "gcg_graph_get_device_view",
+    "gcg_connected_components_ex", "gcg_graph_get_device_view", "gcg_graph_add_edges", "gcg_graph_delete_edges",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
     "gcg_warm_start_rank",
@@ -125,6 +125,8 @@ _graph_from_edges = _sig("gcg_graph_from_edges", _i, _vp, _vp, _u64, _u32, _u32,
 _graph_from_file = _sig("gcg_graph_from_edgelist_file", _i, C.c_char_p, _u32, _u32, C.POINTER(_vp))
 _parse_file = _sig("gcg_parse_edgelist_file", _i, C.c_char_p, _vp, _vp, _u64, C.POINTER(_u64))
 _graph_free = _sig("gcg_graph_free", _i, _vp)
+_graph_add = _sig("gcg_graph_add_edges", _i, _vp, _vp, _vp, _u64)
+_graph_del = _sig("gcg_graph_delete_edges", _i, _vp, _vp, _vp, _u64)
 _graph_set_stream = _sig("gcg_graph_set_stream", _i, _vp, _vp)
 _graph_info = _sig("gcg_graph_get_info", _i, _vp, C.POINTER(GraphInfo))
 _graph_intervals = _sig("gcg_graph_intervals", _i, _vp, _vp)
@@ -248,6 +250,16 @@ class Graph:
 
     def set_stream(self, stream_ptr: int):
         check(_graph_set_stream(self._h, stream_ptr))
+
+    def add_edges(self, src, dst):
+        """gcg_graph_add_edges: the graph becomes its edges plus these (rebuilt on the device)."""
+        src, dst = _u32_host(src), _u32_host(dst)
+        check(_graph_add(self._h, ptr(src), ptr(dst), int(src.shape[0])))
+
+    def delete_edges(self, src, dst):
+        """gcg_graph_delete_edges: removes every copy of each listed edge."""
+        src, dst = _u32_host(src), _u32_host(dst)
+        check(_graph_del(self._h, ptr(src), ptr(dst), int(src.shape[0])))
 
     def info(self) -> GraphInfo:
         i = GraphInfo()

@@ -101,6 +101,21 @@ int gcg_graph_degrees(const gcg_graph *g, int32_t *pairs);
 /* Copies a CSR: rowptr (num_vertices+1) and col (num_edges), host or device. */
 int gcg_graph_csr(const gcg_graph *g, int which, uint32_t *rowptr, uint32_t *col);
 
+/* Dynamic graphs: replaces graphchi_dynamicgraph_engine's add_edge and edge
+ * deletion (src/engine/dynamic_graphs/graphchi_dynamicgraph_engine.hpp:289-606:
+ * added edges are buffered and merged into the shards, deleted edges are flagged
+ * and dropped when a shard is rewritten). Here a batch of updates rebuilds the
+ * resident graph on the device: afterwards it is exactly what gcg_graph_from_edges
+ * would build, with the graph's own build flags and interval count, from its
+ * edges plus the added ones (add) or minus every copy of the listed ones
+ * (delete; absent edges are ignored). For a graph built with
+ * GCG_BUILD_SYMMETRISE each edge is added or removed in both directions. Added
+ * ids may exceed the vertex count, which then grows to max id + 1; deletion keeps
+ * it. Cached plans (PageRank, CC) are rebuilt on their next use; the handle and
+ * its stream stay. src/dst: m entries, host or device. */
+int gcg_graph_add_edges(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m);
+int gcg_graph_delete_edges(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m);
+
 /* Borrowed device pointers to a graph's resident arrays, for callers that run
  * their own kernels over it (the functional plug-in of graphchi_gpu does). Valid
  * until gcg_graph_free; read-only; out_rowptr/out_col are NULL when the graph was
