@@ -6,8 +6,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <thread>
 #include <vector>
@@ -66,6 +70,208 @@ void pool_keep_memory() {
     cudaGetLastError();
     done[dev] = true;
 }
+
+/* ---- block cache ----------------------------------------------------------
+ * Graph builds, chunk plans and solver workspaces ask for the same sizes again
+ * and again (a loop that builds, solves and frees a graph per input), and
+ * cudaMalloc/cudaFree cost 0.3-5 ms apiece at these sizes. A freed block waits
+ * in an idle list keyed by (device, size class) for the next request of its
+ * class. Before a block enters the list its device is synchronised, which is
+ * what cudaFree did, so no kernel still touches a block that is handed out
+ * again. Classes: 512-byte multiples up to 1 MiB, 2 MiB multiples above. */
+namespace {
+
+constexpr int CACHE_DEVS = 64;
+constexpr int HOST_DEV = -1;
+
+struct BlockCache {
+    std::mutex mu;
+    std::unordered_map<void *, std::pair<size_t, int>> live; /* ptr -> (class bytes, device or HOST_DEV) */
+    std::multimap<std::pair<int, size_t>, void *> idle;
+    size_t idle_dev[CACHE_DEVS] = {0};
+    size_t cap_dev[CACHE_DEVS] = {0};
+    bool cap_known[CACHE_DEVS] = {false};
+    size_t idle_host = 0, cap_host = 0;
+    bool host_cap_known = false;
+};
+
+/* never destroyed: blocks may be returned by static destructors after main */
+BlockCache &cache() {
+    static BlockCache *c = new BlockCache();
+    return *c;
+}
+
+size_t size_class(size_t b) {
+    if (b == 0) b = 1;
+    if (b <= ((size_t)1 << 20)) return (b + 511) & ~(size_t)511;
+    const size_t g = (size_t)2 << 20;
+    return (b + g - 1) & ~(g - 1);
+}
+
+size_t env_mb(const char *name, size_t dflt) {
+    const char *v = getenv(name);
+    if (!v || !*v) return dflt;
+    char *end = nullptr;
+    unsigned long long mb = strtoull(v, &end, 10);
+    if (end == v) return dflt;
+    return (size_t)mb << 20;
+}
+
+/* under the lock */
+size_t device_cap(BlockCache &c, int dev) {
+    if (!c.cap_known[dev]) {
+        size_t freeb = 0, total = 0;
+        if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+            cudaGetLastError();
+            total = 0;
+        }
+        c.cap_dev[dev] = env_mb("GCG_DEVICE_CACHE_MB", total / 4);
+        c.cap_known[dev] = true;
+    }
+    return c.cap_dev[dev];
+}
+
+size_t host_cap(BlockCache &c) {
+    if (!c.host_cap_known) {
+        c.cap_host = env_mb("GCG_HOST_CACHE_MB", (size_t)256 << 20);
+        c.host_cap_known = true;
+    }
+    return c.cap_host;
+}
+
+/* frees idle blocks: of device dev_sel (>= 0), of every device (ALL_DEVS) or of
+ * none (NO_DEVS), and the host's with host; returns the bytes released */
+constexpr int ALL_DEVS = -1, NO_DEVS = -2;
+uint64_t drain(int dev_sel, bool host) {
+    BlockCache &c = cache();
+    std::vector<std::pair<int, void *>> victims;
+    uint64_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (auto it = c.idle.begin(); it != c.idle.end();) {
+            const int d = it->first.first;
+            const bool take = d == HOST_DEV ? host : (dev_sel == ALL_DEVS || d == dev_sel);
+            if (!take) {
+                ++it;
+                continue;
+            }
+            bytes += it->first.second;
+            if (d == HOST_DEV)
+                c.idle_host -= it->first.second;
+            else
+                c.idle_dev[d] -= it->first.second;
+            victims.emplace_back(d, it->second);
+            it = c.idle.erase(it);
+        }
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto &v : victims) {
+        if (v.first == HOST_DEV) {
+            cudaFreeHost(v.second);
+        } else {
+            if (v.first != cur) cudaSetDevice(v.first);
+            cudaFree(v.second);
+            if (v.first != cur) cudaSetDevice(cur);
+        }
+    }
+    cudaGetLastError();
+    return bytes;
+}
+
+cudaError_t cached_alloc(void **p, size_t bytes, bool host) {
+    *p = nullptr;
+    int dev = HOST_DEV;
+    if (!host) {
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= CACHE_DEVS) return cudaMalloc(p, bytes);
+    }
+    const size_t cls = size_class(bytes);
+    BlockCache &c = cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (!host) device_cap(c, dev); /* read while dev is the current device */
+        auto it = c.idle.find({dev, cls});
+        if (it != c.idle.end()) {
+            *p = it->second;
+            c.idle.erase(it);
+            if (host)
+                c.idle_host -= cls;
+            else
+                c.idle_dev[dev] -= cls;
+            c.live[*p] = {cls, dev};
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = host ? cudaMallocHost(p, cls) : cudaMalloc(p, cls);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        drain(host ? NO_DEVS : dev, host);
+        e = host ? cudaMallocHost(p, cls) : cudaMalloc(p, cls);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return e;
+    }
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.live[*p] = {cls, dev};
+    return cudaSuccess;
+}
+
+void cached_free(void *p, bool host) {
+    if (!p) return;
+    BlockCache &c = cache();
+    size_t cls = 0;
+    int dev = HOST_DEV;
+    bool keep = false;
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.live.find(p);
+        if (it != c.live.end()) {
+            cls = it->second.first;
+            dev = it->second.second;
+            c.live.erase(it);
+            const size_t cap = dev == HOST_DEV ? host_cap(c) : device_cap(c, dev);
+            const size_t held = dev == HOST_DEV ? c.idle_host : c.idle_dev[dev];
+            keep = held + cls <= cap;
+        } else {
+            dev = host ? HOST_DEV : -2; /* not ours: hand straight back */
+        }
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    const int sync_dev = dev >= 0 ? dev : cur;
+    if (sync_dev != cur) cudaSetDevice(sync_dev);
+    if (keep) {
+        /* what cudaFree/cudaFreeHost would wait for: no kernel or copy still uses p */
+        keep = cudaDeviceSynchronize() == cudaSuccess;
+        if (keep) {
+            std::lock_guard<std::mutex> lk(c.mu);
+            c.idle.insert({{dev, cls}, p});
+            if (dev == HOST_DEV)
+                c.idle_host += cls;
+            else
+                c.idle_dev[dev] += cls;
+        }
+    }
+    if (!keep) {
+        if (host)
+            cudaFreeHost(p);
+        else
+            cudaFree(p);
+    }
+    if (sync_dev != cur) cudaSetDevice(cur);
+    cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t dev_alloc(void **p, size_t bytes) { return cached_alloc(p, bytes, false); }
+void dev_free(void *p) { cached_free(p, false); }
+cudaError_t host_alloc(void **p, size_t bytes) { return cached_alloc(p, bytes, true); }
+void host_free(void *p) { cached_free(p, true); }
 
 int num_sms() {
     static int cached = 0;
@@ -208,6 +414,22 @@ int gcg_write_vout(const char *base, const void *values, uint32_t num_vertices, 
 int gcg_graph_set_stream(gcg_graph *g, void *stream) {
     if (!g) return fail(GCG_ERR_INVALID, "gcg_graph_set_stream: null graph");
     g->stream = (cudaStream_t)stream;
+    return GCG_OK;
+}
+
+int gcg_cached_memory(uint64_t *idle_device_bytes, uint64_t *idle_host_bytes) {
+    BlockCache &c = cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    uint64_t d = 0;
+    for (int i = 0; i < CACHE_DEVS; ++i) d += c.idle_dev[i];
+    if (idle_device_bytes) *idle_device_bytes = d;
+    if (idle_host_bytes) *idle_host_bytes = c.idle_host;
+    return GCG_OK;
+}
+
+int gcg_release_cached_memory(uint64_t *released_bytes) {
+    const uint64_t b = drain(ALL_DEVS, true);
+    if (released_bytes) *released_bytes = b;
     return GCG_OK;
 }
 

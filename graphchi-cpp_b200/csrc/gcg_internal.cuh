@@ -36,6 +36,13 @@ int fail(int status, const std::string &msg);
 
 #define GCG_LAUNCH_CHECK() GCG_CUDA(cudaGetLastError())
 
+/* ---- block cache (gcg_common.cu): freed device blocks and small pinned host
+ *      blocks are kept per device and size class for the next allocation ---- */
+cudaError_t dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+cudaError_t host_alloc(void **p, size_t bytes);
+void host_free(void *p);
+
 /* ---- device buffers ----------------------------------------------------- */
 template <typename T>
 struct dbuf {
@@ -48,7 +55,7 @@ struct dbuf {
     int alloc(size_t count) {
         release();
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        cudaError_t e = dev_alloc((void **)&p, count * sizeof(T));
         if (e != cudaSuccess) {
             p = nullptr;
             return fail(GCG_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
@@ -58,7 +65,7 @@ struct dbuf {
         return GCG_OK;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }

@@ -466,7 +466,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         GCG_TRY(w.parts.alloc((size_t)2 * pl.nchunks + 2));
         GCG_TRY(w.bres.alloc(gv));
         GCG_TRY(w.ctl.alloc(4));
-        GCG_CUDA(cudaMallocHost((void **)&w.h_flags, 64 * sizeof(int)));
+        GCG_CUDA(host_alloc((void **)&w.h_flags, 64 * sizeof(int)));
     }
     if (w.dres.n < 2 * (size_t)max_sweeps + 1) GCG_TRY(w.dres.alloc(2 * (size_t)max_sweeps + 1));
     dbuf<float> &r = w.r, &c = w.c, &nzsum = w.nzsum, &parts = w.parts, &rnz = w.rnz;

@@ -231,7 +231,7 @@ struct PrWork {
     dbuf<double> dres;
     int *h_flags = nullptr; /* pinned: done flags copied back per chunk of sweeps */
     ~PrWork() {
-        if (h_flags) cudaFreeHost(h_flags);
+        if (h_flags) host_free(h_flags);
     }
 };
 

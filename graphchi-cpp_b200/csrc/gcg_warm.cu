@@ -945,7 +945,7 @@ int gcg_mlp_train(gcg_mlp *m, const float *x, const float *t, uint64_t n, const 
     GCG_CUDA(cudaMemsetAsync(acc.get(), 0, (size_t)std::max<uint32_t>(p->epochs, 1) * 8, s));
     std::vector<uint32_t> order(n);
     uint32_t *h_order = nullptr; /* pinned: the upload of one epoch's order overlaps the previous epoch */
-    GCG_CUDA(cudaMallocHost((void **)&h_order, (size_t)n * 4));
+    GCG_CUDA(host_alloc((void **)&h_order, (size_t)n * 4));
     uint64_t rs = p->seed * 0x2545F4914F6CDD1Dull + 7;
     for (uint32_t ep = 0; ep < p->epochs; ++ep) {
         for (uint64_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
@@ -957,7 +957,7 @@ int gcg_mlp_train(gcg_mlp *m, const float *x, const float *t, uint64_t n, const 
         memcpy(h_order, order.data(), (size_t)n * 4);
         cudaError_t e = cudaMemcpyAsync(idx.get(), h_order, (size_t)n * 4, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) {
-            cudaFreeHost(h_order);
+            host_free(h_order);
             return fail(GCG_ERR_CUDA, std::string("gcg_mlp_train: ") + cudaGetErrorString(e));
         }
         for (uint64_t b0 = 0; b0 < n; b0 += p->batch) {
@@ -996,12 +996,12 @@ int gcg_mlp_train(gcg_mlp *m, const float *x, const float *t, uint64_t n, const 
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) {
-            cudaFreeHost(h_order);
+            host_free(h_order);
             return fail(GCG_ERR_CUDA, std::string("gcg_mlp_train: launch: ") + cudaGetErrorString(e));
         }
     }
     cudaStreamSynchronize(s);
-    cudaFreeHost(h_order);
+    host_free(h_order);
     GCG_TRY(mlp_prepare(m, s));
     std::vector<double> hl(std::max<uint32_t>(p->epochs, 1));
     GCG_CUDA(cudaMemcpyAsync(hl.data(), acc.get(), hl.size() * 8, cudaMemcpyDeviceToHost, s));

@@ -53,7 +53,7 @@ EXPORTED = [
     "gcg_connected_components_ex", "gcg_graph_get_device_view", "gcg_graph_add_edges", "gcg_graph_delete_edges",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
-    "gcg_warm_start_rank",
+    "gcg_warm_start_rank", "gcg_cached_memory", "gcg_release_cached_memory",
 ]
 MLP_IN = 8
 MLP_HIDDEN = 64
@@ -168,6 +168,8 @@ _mlp_train = _sig("gcg_mlp_train", _i, _vp, _vp, _vp, _u64, C.POINTER(MlpTrainPa
 _warm_start = _sig("gcg_warm_start_rank", _i, _vp, _vp, C.c_double, C.c_double, _vp, C.POINTER(C.c_double))
 _last_error = _sig("gcg_last_error", C.c_char_p)
 _version = _sig("gcg_version", C.c_char_p)
+_cached_memory = _sig("gcg_cached_memory", _i, C.POINTER(_u64), C.POINTER(_u64))
+_release_cached = _sig("gcg_release_cached_memory", _i, C.POINTER(_u64))
 
 
 def last_error() -> str:
@@ -176,6 +178,20 @@ def last_error() -> str:
 
 def version() -> str:
     return _version().decode()
+
+
+def cached_memory():
+    """Idle bytes the library's block cache holds: (device, pinned host)."""
+    d, h = _u64(0), _u64(0)
+    check(_cached_memory(C.byref(d), C.byref(h)))
+    return d.value, h.value
+
+
+def release_cached_memory() -> int:
+    """Returns every idle cached block to the driver; gives the bytes released."""
+    b = _u64(0)
+    check(_release_cached(C.byref(b)))
+    return b.value
 
 
 def check(status: int) -> None:

@@ -72,7 +72,23 @@ int gcg_graph_from_edgelist_file(const char *path, uint32_t flags, uint32_t nsha
 int gcg_parse_edgelist_file(const char *path, uint32_t *src, uint32_t *dst, uint64_t capacity,
                             uint64_t *m_out);
 
+/* Frees the graph. Its device blocks go back to the library's block cache
+ * (below), not to the driver. */
 int gcg_graph_free(gcg_graph *g);
+
+/* The library keeps freed device blocks (and small pinned host blocks) per device
+ * and size class and hands them to later allocations of the same class, so a loop
+ * that builds, solves and frees graphs calls neither cudaMalloc nor cudaFree after
+ * its first pass. The reference allocates with malloc/free per run (no
+ * counterpart). Freeing a block into the cache synchronises its device first, as
+ * cudaFree does. The idle cache is capped per device by the environment variable
+ * GCG_DEVICE_CACHE_MB (default: a quarter of the device's memory; 0 turns caching
+ * off; host: GCG_HOST_CACHE_MB, default 256) and is emptied, and the allocation
+ * retried, when the driver runs out of memory.
+ * gcg_cached_memory reports the idle bytes held; gcg_release_cached_memory
+ * returns them all to the driver (released_bytes may be NULL). */
+int gcg_cached_memory(uint64_t *idle_device_bytes, uint64_t *idle_host_bytes);
+int gcg_release_cached_memory(uint64_t *released_bytes);
 
 /* Makes all later work on g run on `stream` (a cudaStream_t; NULL = legacy default). */
 int gcg_graph_set_stream(gcg_graph *g, void *stream);

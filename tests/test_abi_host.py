@@ -102,3 +102,10 @@ def test_write_vout_layout(tmp_path):
     v = np.arange(10, dtype=np.float32) * 0.5
     gcgpu.write_vout(base, v)
     assert np.array_equal(np.fromfile(base + ".4B.vout", dtype=np.float32), v)
+
+
+def test_block_cache_is_empty_without_allocations():
+    # nothing was allocated on a machine without a GPU: the cache holds nothing
+    # and releasing it is a no-op
+    assert gcgpu.cached_memory() == (0, 0)
+    assert gcgpu.release_cached_memory() == 0
