@@ -217,41 +217,172 @@ unsigned grid_for(uint64_t n, int threads) {
 
 namespace {
 
+constexpr uint64_t PIPE_MIN_EDGES = 1ull << 24;
+constexpr int PIPE_CHUNKS = 8; /* a power of two: runs merge in equal pairs */
+
+uint32_t id_bits(uint32_t maxid) {
+    uint32_t b = 1;
+    while (b < 32 && (1ull << b) <= maxid) ++b;
+    return b;
+}
+
+/* Host edge arrays, sorted while they cross PCIe. The edges are copied in
+ * PIPE_CHUNKS pieces on a copy stream; each piece is scanned (self-loops, max
+ * id, range) as soon as it lands; its keys (dst << 32 | src) are radix-sorted on
+ * the sort stream while later pieces are still in flight (only the digits its
+ * largest id needs), and sorted runs are merged pairwise as soon as two of equal
+ * length exist. After the last piece lands, only its sort and the merges that
+ * take it in remain. The sorted keys end in *sorted (keys or tmp); the scan
+ * results of all pieces are combined into *info. */
+int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bool sym, uint32_t nv_given,
+                    uint32_t *sbuf, uint32_t *dbuf_, uint64_t *keys, uint64_t *tmp, uint64_t **sorted,
+                    ScanInfo *info) {
+    const int K = PIPE_CHUNKS;
+    const uint64_t cm = ((m + K - 1) / K + 4095) & ~(uint64_t)4095;
+    const uint64_t kmul = sym ? 2 : 1;
+    cudaStream_t cs = nullptr, ss = nullptr, ks = nullptr;
+    cudaEvent_t ev_copy[PIPE_CHUNKS] = {}, ev_scan[PIPE_CHUNKS] = {};
+    ScanInfo *h_info = nullptr;
+    tbuf<ScanInfo> d_info;
+    int st = GCG_OK;
+    auto done = [&](int status) {
+        if (ks) cudaStreamSynchronize(ks);
+        if (ss) cudaStreamSynchronize(ss);
+        if (cs) cudaStreamSynchronize(cs);
+        for (int i = 0; i < K; ++i) {
+            if (ev_copy[i]) cudaEventDestroy(ev_copy[i]);
+            if (ev_scan[i]) cudaEventDestroy(ev_scan[i]);
+        }
+        if (cs) cudaStreamDestroy(cs);
+        if (ss) cudaStreamDestroy(ss);
+        if (ks) cudaStreamDestroy(ks);
+        if (h_info) host_free(h_info);
+        return status;
+    };
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking) != cudaSuccess)
+        return done(fail(GCG_ERR_CUDA, "edge pipeline: stream creation failed"));
+    for (int i = 0; i < K; ++i)
+        if (cudaEventCreateWithFlags(&ev_copy[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_scan[i], cudaEventDisableTiming) != cudaSuccess)
+            return done(fail(GCG_ERR_CUDA, "edge pipeline: event creation failed"));
+    if (host_alloc((void **)&h_info, sizeof(ScanInfo) * K) != cudaSuccess)
+        return done(fail(GCG_ERR_NOMEM, "edge pipeline: pinned scan results"));
+    if ((st = d_info.alloc(K, 0))) return done(st);
+    if (cudaMemsetAsync(d_info.get(), 0, sizeof(ScanInfo) * K, 0) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess) /* the buffers exist before the other streams use them */
+        return done(fail(GCG_ERR_CUDA, "edge pipeline: setup"));
+
+    /* every piece's copy and scan are queued at once; the copies run back to back */
+    for (int i = 0; i < K; ++i) {
+        const uint64_t c0 = (uint64_t)i * cm, cn = std::min<uint64_t>(cm, m - std::min(m, c0));
+        if (cn) {
+            if (cudaMemcpyAsync(sbuf + c0, src_u + c0, cn * 4, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
+                cudaMemcpyAsync(dbuf_ + c0, dst_u + c0, cn * 4, cudaMemcpyHostToDevice, cs) != cudaSuccess)
+                return done(fail(GCG_ERR_CUDA, "edge pipeline: host to device copy"));
+        }
+        cudaEventRecord(ev_copy[i], cs);
+        cudaStreamWaitEvent(ss, ev_copy[i], 0);
+        if (cn) k_scan_edges<<<grid_for(cn), 256, 0, ss>>>(sbuf + c0, dbuf_ + c0, cn, nv_given, d_info.get() + i);
+        cudaMemcpyAsync(h_info + i, d_info.get() + i, sizeof(ScanInfo), cudaMemcpyDeviceToHost, ss);
+        cudaEventRecord(ev_scan[i], ss);
+    }
+    if (cudaGetLastError() != cudaSuccess) return done(fail(GCG_ERR_CUDA, "edge pipeline: queueing failed"));
+
+    struct Run {
+        int level;
+        uint64_t start, len;
+    };
+    Run stack[PIPE_CHUNKS + 1];
+    int top = 0;
+    info->kept = 0;
+    info->maxid = 0;
+    info->bad = 0;
+    for (int i = 0; i < K; ++i) {
+        if (cudaEventSynchronize(ev_scan[i]) != cudaSuccess)
+            return done(fail(GCG_ERR_CUDA, "edge pipeline: copy or scan failed"));
+        const ScanInfo ci = h_info[i];
+        info->kept += ci.kept;
+        info->maxid = std::max(info->maxid, ci.maxid);
+        info->bad |= ci.bad;
+        const uint64_t c0 = (uint64_t)i * cm, cn = std::min<uint64_t>(cm, m - std::min(m, c0));
+        const uint64_t k0 = kmul * c0, kn = kmul * cn;
+        cudaStreamWaitEvent(ks, ev_scan[i], 0);
+        if (kn) {
+            k_make_keys<<<grid_for(cn), 256, 0, ks>>>(sbuf + c0, dbuf_ + c0, cn, 32, sym ? 1 : 0, keys + k0);
+            const int cb = (int)id_bits(ci.maxid);
+            uint64_t *r1 = nullptr, *r2 = nullptr;
+            if ((st = radix_sort_u64(keys + k0, tmp + k0, kn, 0, cb, &r1, ks))) return done(st);
+            uint64_t *o1 = (r1 == keys + k0) ? tmp + k0 : keys + k0;
+            if ((st = radix_sort_u64(r1, o1, kn, 32, 32 + cb, &r2, ks))) return done(st);
+            if (r2 != keys + k0 &&
+                cudaMemcpyAsync(keys + k0, r2, kn * 8, cudaMemcpyDeviceToDevice, ks) != cudaSuccess)
+                return done(fail(GCG_ERR_CUDA, "edge pipeline: run copy"));
+        }
+        /* runs of level L live in keys (L even) or tmp (L odd) */
+        stack[top++] = Run{0, k0, kn};
+        while (top >= 2 && stack[top - 1].level == stack[top - 2].level) {
+            const Run b = stack[--top], a = stack[--top];
+            uint64_t *from = (a.level & 1) ? tmp : keys, *to = (a.level & 1) ? keys : tmp;
+            if ((st = merge_u64(from + a.start, a.len, from + b.start, b.len, to + a.start, ks))) return done(st);
+            stack[top++] = Run{a.level + 1, a.start, a.len + b.len};
+        }
+    }
+    if (top != 1) return done(fail(GCG_ERR_CUDA, "edge pipeline: runs left unmerged"));
+    *sorted = (stack[0].level & 1) ? tmp : keys;
+    if (cudaStreamSynchronize(ks) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+        return done(fail(GCG_ERR_CUDA, std::string("edge pipeline: ") + cudaGetErrorString(cudaGetLastError())));
+    return done(GCG_OK);
+}
+
 int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32_t nv_given, uint32_t flags,
                 uint32_t nshards, gcg_graph **out) {
     cudaStream_t s = 0;
-    /* stage inputs */
-    tbuf<uint32_t> sbuf, dbuf_;
-    const uint32_t *src = src_u, *dst = dst_u;
-    if (m > 0 && !is_device_ptr(src_u)) {
-        GCG_TRY(sbuf.alloc(m, s));
-        GCG_TRY(copy_in(sbuf.get(), src_u, m * 4, s));
-        src = sbuf.get();
-    }
-    if (m > 0 && !is_device_ptr(dst_u)) {
-        GCG_TRY(dbuf_.alloc(m, s));
-        GCG_TRY(copy_in(dbuf_.get(), dst_u, m * 4, s));
-        dst = dbuf_.get();
-    }
-    /* max id, kept count, range check */
-    tbuf<ScanInfo> d_info;
-    GCG_TRY(d_info.alloc(1, s));
-    GCG_CUDA(cudaMemsetAsync(d_info.get(), 0, sizeof(ScanInfo), s));
-    if (m > 0) {
-        k_scan_edges<<<grid_for(m), 256, 0, s>>>(src, dst, m, nv_given, d_info.get());
-        GCG_LAUNCH_CHECK();
-    }
-    ScanInfo info;
-    GCG_CUDA(cudaMemcpyAsync(&info, d_info.get(), sizeof(info), cudaMemcpyDeviceToHost, s));
-    GCG_CUDA(cudaStreamSynchronize(s));
-    if (info.bad) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: vertex id >= num_vertices");
-    uint32_t nv = nv_given ? nv_given : info.maxid + 1; /* sharder.hpp:925: 1 + max_vertex_id */
     const bool sym = (flags & GCG_BUILD_SYMMETRISE) != 0;
     const uint64_t nk = sym ? 2 * m : m;
+    tbuf<uint32_t> sbuf, dbuf_;
+    tbuf<uint64_t> keys, tmp;
+    uint64_t *sorted = nullptr;
+    ScanInfo info;
+    uint32_t kbits = 0; /* width of the src half of a key: 32 when sorted in pieces, else vbits */
+    const bool pipelined = m >= PIPE_MIN_EDGES && !is_device_ptr(src_u) && !is_device_ptr(dst_u);
+    const uint32_t *src = src_u, *dst = dst_u;
+    if (pipelined) {
+        if (sbuf.alloc(m, s) || dbuf_.alloc(m, s) || keys.alloc(nk, s) || tmp.alloc(nk, s)) return GCG_ERR_NOMEM;
+        GCG_TRY(sort_host_edges(src_u, dst_u, m, sym, nv_given, sbuf.get(), dbuf_.get(), keys.get(), tmp.get(),
+                                &sorted, &info));
+        kbits = 32;
+    } else {
+        /* stage inputs */
+        if (m > 0 && !is_device_ptr(src_u)) {
+            GCG_TRY(sbuf.alloc(m, s));
+            GCG_TRY(copy_in(sbuf.get(), src_u, m * 4, s));
+            src = sbuf.get();
+        }
+        if (m > 0 && !is_device_ptr(dst_u)) {
+            GCG_TRY(dbuf_.alloc(m, s));
+            GCG_TRY(copy_in(dbuf_.get(), dst_u, m * 4, s));
+            dst = dbuf_.get();
+        }
+        /* max id, kept count, range check */
+        tbuf<ScanInfo> d_info;
+        GCG_TRY(d_info.alloc(1, s));
+        GCG_CUDA(cudaMemsetAsync(d_info.get(), 0, sizeof(ScanInfo), s));
+        if (m > 0) {
+            k_scan_edges<<<grid_for(m), 256, 0, s>>>(src, dst, m, nv_given, d_info.get());
+            GCG_LAUNCH_CHECK();
+        }
+        GCG_CUDA(cudaMemcpyAsync(&info, d_info.get(), sizeof(info), cudaMemcpyDeviceToHost, s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+    }
+    if (info.bad) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: vertex id >= num_vertices");
+    uint32_t nv = nv_given ? nv_given : info.maxid + 1; /* sharder.hpp:925: 1 + max_vertex_id */
     const uint64_t kept = sym ? 2 * (uint64_t)info.kept : (uint64_t)info.kept;
     if (kept > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "more than 2^32-1 edges after filtering");
     uint32_t vbits = 1;
     while (vbits < 32 && (1ull << vbits) < nv) ++vbits;
+    if (!pipelined) kbits = vbits;
 
     gcg_graph *g = new gcg_graph();
     g->nv = nv;
@@ -265,15 +396,16 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         return st;
     };
 
-    tbuf<uint64_t> keys, tmp;
-    uint64_t *sorted = nullptr;
     uint64_t ne = kept;
     if (nk > 0) {
-        if (keys.alloc(nk, s) || tmp.alloc(nk, s)) return cleanup(GCG_ERR_NOMEM);
-        k_make_keys<<<grid_for(m), 256, 0, s>>>(src, dst, m, vbits, sym ? 1 : 0, keys.get());
-        if (cudaGetLastError() != cudaSuccess) return cleanup(fail(GCG_ERR_CUDA, "k_make_keys launch"));
-        int st = radix_sort_u64(keys.get(), tmp.get(), nk, 0, 2 * (int)vbits, &sorted, s);
-        if (st) return cleanup(st);
+        int st = GCG_OK;
+        if (!pipelined) {
+            if (keys.alloc(nk, s) || tmp.alloc(nk, s)) return cleanup(GCG_ERR_NOMEM);
+            k_make_keys<<<grid_for(m), 256, 0, s>>>(src, dst, m, vbits, sym ? 1 : 0, keys.get());
+            if (cudaGetLastError() != cudaSuccess) return cleanup(fail(GCG_ERR_CUDA, "k_make_keys launch"));
+            st = radix_sort_u64(keys.get(), tmp.get(), nk, 0, 2 * (int)vbits, &sorted, s);
+            if (st) return cleanup(st);
+        }
         if ((flags & GCG_BUILD_DEDUP) && kept > 0) {
             tbuf<uint32_t> fl;
             tbuf<uint32_t> d_total;
@@ -294,7 +426,7 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
     if (ne == 0) {
         cudaMemsetAsync(g->in_rowptr.get(), 0, ((size_t)nv + 1) * 4, s);
     } else {
-        k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(sorted, ne, vbits, nv, g->in_rowptr.get(), g->in_col.get());
+        k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(sorted, ne, kbits, nv, g->in_rowptr.get(), g->in_col.get());
     }
     k_degree<<<grid_for(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, g->indeg.get());
     if (!(flags & GCG_BUILD_NO_OUT_CSR)) {
@@ -304,12 +436,12 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         } else {
             uint64_t *a = (sorted == keys.get()) ? tmp.get() : keys.get();
             uint64_t *b = sorted;
-            k_swap_key<<<grid_for(ne), 256, 0, s>>>(sorted, ne, vbits, a);
+            k_swap_key<<<grid_for(ne), 256, 0, s>>>(sorted, ne, kbits, a);
             uint64_t *res = nullptr;
             /* stable sort by the source half only: (dst, src) order -> (src, dst) */
-            int st = radix_sort_u64(a, b, ne, (int)vbits, 2 * (int)vbits, &res, s);
+            int st = radix_sort_u64(a, b, ne, (int)kbits, (int)(kbits + vbits), &res, s);
             if (st) return cleanup(st);
-            k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(res, ne, vbits, nv, g->out_rowptr.get(), g->out_col.get());
+            k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(res, ne, kbits, nv, g->out_rowptr.get(), g->out_col.get());
         }
         k_degree<<<grid_for(nv), 256, 0, s>>>(g->out_rowptr.get(), nv, g->outdeg.get());
         g->has_out = true;

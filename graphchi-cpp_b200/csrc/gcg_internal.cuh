@@ -168,6 +168,10 @@ int radix_sort_u64(uint64_t *keys, uint64_t *tmp, uint64_t n, int begin_bit, int
  * (device pointer, may be null). in and out may alias. */
 int scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total_dev, cudaStream_t s);
 
+/* Merge of sorted runs a[0..na) and b[0..nb) into out[0..na+nb), stable (a's
+ * first on equal keys); out overlaps neither run. */
+int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t *out, cudaStream_t s);
+
 /* Unique of sorted keys: out[0..total) = distinct keys (flags: n scratch). */
 int unique_u64(const uint64_t *in, uint64_t n, uint32_t *flags, uint32_t *total_dev, uint64_t *out, cudaStream_t s);
 

@@ -13,6 +13,8 @@
  * Tiles are 4096 keys (256 threads x 16); each warp reads its 512 keys as 16
  * coalesced rounds of 32.
  */
+#include <algorithm>
+
 #include "gcg_internal.cuh"
 
 namespace gcg {
@@ -216,7 +218,90 @@ __global__ void __launch_bounds__(SC_THREADS) sc_scan_tile(const uint32_t *in, u
     }
 }
 
+/* ---- merge of two sorted runs (merge path) ------------------------------ */
+
+constexpr int MG_THREADS = 256;
+constexpr int MG_ITEMS = 8;
+constexpr int MG_TILE = MG_THREADS * MG_ITEMS;
+
+/* how many of the first diag outputs come from a (a first on equal keys) */
+template <typename I>
+__device__ __forceinline__ I merge_path(const uint64_t *a, I na, const uint64_t *b, I nb, I diag) {
+    I lo = diag > nb ? diag - nb : 0, hi = diag < na ? diag : na;
+    while (lo < hi) {
+        const I mid = (lo + hi) >> 1;
+        if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+/* split[t] = a's share of the first t*MG_TILE outputs, t = 0..ntiles */
+__global__ void k_merge_split(const uint64_t *__restrict__ a, uint64_t na, const uint64_t *__restrict__ b,
+                              uint64_t nb, uint64_t ntiles, uint64_t *__restrict__ split) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t d = t * MG_TILE < na + nb ? t * MG_TILE : na + nb;
+        split[t] = merge_path<uint64_t>(a, na, b, nb, d);
+    }
+}
+
+/* One output tile per block: its pieces of a and b are staged in shared memory,
+ * each thread merges MG_ITEMS outputs from its own merge-path split, and the
+ * tile is written back with coalesced stores. */
+__global__ void __launch_bounds__(MG_THREADS) k_merge_u64(const uint64_t *__restrict__ a, uint64_t na,
+                                                          const uint64_t *__restrict__ b, uint64_t nb,
+                                                          const uint64_t *__restrict__ split,
+                                                          uint64_t *__restrict__ out) {
+    __shared__ uint64_t s_in[MG_TILE];
+    const uint64_t n = na + nb;
+    const uint64_t d0 = (uint64_t)blockIdx.x * MG_TILE;
+    const uint64_t d1 = d0 + MG_TILE < n ? d0 + MG_TILE : n;
+    const uint64_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
+    const uint64_t b0 = d0 - a0, b1 = d1 - a1;
+    const uint32_t la = (uint32_t)(a1 - a0), lb = (uint32_t)(b1 - b0), tot = la + lb;
+    for (uint32_t i = threadIdx.x; i < la; i += MG_THREADS) s_in[i] = a[a0 + i];
+    for (uint32_t i = threadIdx.x; i < lb; i += MG_THREADS) s_in[la + i] = b[b0 + i];
+    __syncthreads();
+    const uint64_t *sa = s_in, *sb = s_in + la;
+    const uint32_t dg = threadIdx.x * MG_ITEMS < tot ? threadIdx.x * MG_ITEMS : tot;
+    uint32_t i = merge_path<uint32_t>(sa, la, sb, lb, dg), j = dg - i;
+    uint64_t v[MG_ITEMS];
+#pragma unroll
+    for (int k = 0; k < MG_ITEMS; ++k) {
+        v[k] = 0;
+        if (dg + k < tot) {
+            const bool take_a = i < la && (j >= lb || sa[i] <= sb[j]);
+            v[k] = take_a ? sa[i] : sb[j];
+            if (take_a) ++i; else ++j;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < MG_ITEMS; ++k)
+        if (dg + k < tot) s_in[dg + k] = v[k];
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < tot; x += MG_THREADS) out[d0 + x] = s_in[x];
+}
+
 }  // namespace
+
+int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t *out, cudaStream_t s) {
+    const uint64_t n = na + nb;
+    if (n == 0) return GCG_OK;
+    if (na == 0 || nb == 0) {
+        GCG_CUDA(cudaMemcpyAsync(out, na ? a : b, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        return GCG_OK;
+    }
+    const uint64_t ntiles = (n + MG_TILE - 1) / MG_TILE;
+    if (ntiles >= 0x7FFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "merge: too many keys");
+    tbuf<uint64_t> split;
+    GCG_TRY(split.alloc(ntiles + 1, s));
+    k_merge_split<<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
+        a, na, b, nb, ntiles, split.get());
+    k_merge_u64<<<(unsigned)ntiles, MG_THREADS, 0, s>>>(a, na, b, nb, split.get(), out);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
 
 int scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total_dev, cudaStream_t s) {
     if (n == 0) {

@@ -155,3 +155,53 @@ def test_large_sort_matches_numpy():
         orp, ocol = g.csr(gcgpu.CSR_OUT)
         k2 = np.unique((s[keep].astype(np.uint64) << np.uint64(32)) | d[keep].astype(np.uint64))
         assert np.array_equal(ocol, (k2 & np.uint64(0xFFFFFFFF)).astype(np.uint32))
+
+
+def _same_graph(a, b):
+    assert (a.num_vertices, a.num_edges) == (b.num_vertices, b.num_edges)
+    for w in (gcgpu.CSR_IN, gcgpu.CSR_OUT):
+        ra, ca = a.csr(w)
+        rb, cb = b.csr(w)
+        assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
+    assert np.array_equal(a.degrees(), b.degrees())
+    assert np.array_equal(a.intervals(), b.intervals())
+
+
+@pytest.mark.parametrize("sym,dedup,pinned", [(False, True, True), (True, True, True), (False, False, False)])
+def test_host_edges_sorted_in_pieces_equal_one_sort(sym, dedup, pinned):
+    """From 2^24 host edges on, the sharder sorts pieces of the edge list while
+    later pieces are still being copied in and merges the sorted runs; the graph
+    equals the one sorted in one piece from the same edges on the device. The
+    last piece is ragged; R-MAT brings self-loops and duplicates."""
+    import torch
+    m = (1 << 24) + 12345
+    s, d = O.rmat_numpy(20, m, seed=31)
+    ts = torch.from_numpy(s.view(np.int32)).cuda()
+    td = torch.from_numpy(d.view(np.int32)).cuda()
+    if pinned:
+        hs = torch.from_numpy(s.view(np.int32)).pin_memory()
+        hd = torch.from_numpy(d.view(np.int32)).pin_memory()
+    else:
+        hs, hd = s, d
+    with gcgpu.Graph.from_edges(hs, hd, dedup=dedup, symmetrise=sym, nshards=8) as a, \
+            gcgpu.Graph.from_edges(ts, td, dedup=dedup, symmetrise=sym, nshards=8) as b:
+        _same_graph(a, b)
+        if not sym and dedup:
+            keep = s != d
+            k = np.unique((d[keep].astype(np.uint64) << np.uint64(32)) | s[keep].astype(np.uint64))
+            assert a.num_edges == k.shape[0]
+            _, col = a.csr(gcgpu.CSR_IN)
+            assert np.array_equal(col, (k & np.uint64(0xFFFFFFFF)).astype(np.uint32))
+
+
+def test_host_edges_in_pieces_reject_out_of_range_ids():
+    m = 1 << 24
+    s, d = O.rmat_numpy(20, m, seed=32)
+    d[m - 7] = (1 << 20) + 5  # in the last piece
+    with pytest.raises(gcgpu.GcgError) as e:
+        gcgpu.Graph.from_edges(s, d, num_vertices=1 << 20)
+    assert e.value.status == -1
+    # the same edges with a vertex count that admits the id build normally
+    with gcgpu.Graph.from_edges(s, d, num_vertices=(1 << 20) + 6, dedup=True, out_csr=False) as g:
+        assert g.num_vertices == (1 << 20) + 6
+        assert g.degrees()[(1 << 20) + 5, 0] == 1  # the planted edge's destination
