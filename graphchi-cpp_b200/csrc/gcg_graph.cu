@@ -55,13 +55,18 @@ __global__ void k_scan_edges(const uint32_t *__restrict__ src, const uint32_t *_
 /* key = (row << vbits) | col; self-loops become the all-ones sentinel, which
  * sorts after every real key (a real key never has row == col == all ones). */
 __global__ void k_make_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t m,
-                            uint32_t vbits, int sym, uint64_t *__restrict__ keys) {
+                            uint32_t vbits, int sym, uint64_t *__restrict__ keys, uint32_t *__restrict__ outcnt) {
     const uint64_t sent = (vbits >= 32) ? ~0ull : ((1ull << (2 * vbits)) - 1ull);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t s = src[i], d = dst[i];
         bool self = s == d;
         keys[i] = self ? sent : ((d << vbits) | s);
         if (sym) keys[m + i] = self ? sent : ((s << vbits) | d);
+        /* raw out-degrees: one count per key's source (repeats are taken off later) */
+        if (outcnt && !self) {
+            atomicAdd(outcnt + s, 1u);
+            if (sym) atomicAdd(outcnt + d, 1u);
+        }
     }
 }
 
@@ -231,12 +236,20 @@ uint32_t id_bits(uint32_t maxid) {
  * id, range) as soon as it lands; its keys (dst << 32 | src) are radix-sorted on
  * the sort stream while later pieces are still in flight (only the digits its
  * largest id needs), and sorted runs are merged pairwise as soon as two of equal
- * length exist. After the last piece lands, only its sort and the merges that
- * take it in remain. The sorted keys end in *sorted (keys or tmp); the scan
- * results of all pieces are combined into *info. */
+ * length exist, all but the last merge, which the caller fuses with the
+ * duplicate filter and the CSR decode. After the last piece lands, only its sort
+ * and the merges that take it in remain. The two final runs come back in
+ * run[0], run[1] (pointer, length); the scan results of all pieces are combined
+ * into *info. With outcnt, the raw out-degree of every id is counted into
+ * outcnt (grown as larger ids arrive; outgrown buffers are kept in old). */
+struct SortedRuns {
+    const uint64_t *p[2];
+    uint64_t n[2];
+};
+
 int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bool sym, uint32_t nv_given,
-                    uint32_t *sbuf, uint32_t *dbuf_, uint64_t *keys, uint64_t *tmp, uint64_t **sorted,
-                    ScanInfo *info) {
+                    uint32_t *sbuf, uint32_t *dbuf_, uint64_t *keys, uint64_t *tmp, SortedRuns *runs,
+                    ScanInfo *info, dbuf<uint32_t> *outcnt, std::vector<dbuf<uint32_t> *> &old) {
     const int K = PIPE_CHUNKS;
     const uint64_t cm = ((m + K - 1) / K + 4095) & ~(uint64_t)4095;
     const uint64_t kmul = sym ? 2 : 1;
@@ -309,8 +322,32 @@ int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bo
         const uint64_t c0 = (uint64_t)i * cm, cn = std::min<uint64_t>(cm, m - std::min(m, c0));
         const uint64_t k0 = kmul * c0, kn = kmul * cn;
         cudaStreamWaitEvent(ks, ev_scan[i], 0);
+        if (outcnt && !info->bad && (uint64_t)info->maxid + 1 > outcnt->n) {
+            uint64_t cap = (uint64_t)1 << 16;
+            while (cap < (uint64_t)info->maxid + 1) cap <<= 1;
+            dbuf<uint32_t> *grown = new dbuf<uint32_t>();
+            if (grown->alloc(cap)) {
+                delete grown;
+                return done(GCG_ERR_NOMEM);
+            }
+            if (cudaMemsetAsync(grown->get(), 0, cap * 4, ks) != cudaSuccess ||
+                (outcnt->n && cudaMemcpyAsync(grown->get(), outcnt->get(), outcnt->n * 4, cudaMemcpyDeviceToDevice,
+                                              ks) != cudaSuccess)) {
+                delete grown;
+                return done(fail(GCG_ERR_CUDA, "edge pipeline: out-degree counts"));
+            }
+            /* the outgrown buffer may still be read by queued work: freed with the build */
+            dbuf<uint32_t> *prev = new dbuf<uint32_t>();
+            std::swap(prev->p, outcnt->p);
+            std::swap(prev->n, outcnt->n);
+            std::swap(outcnt->p, grown->p);
+            std::swap(outcnt->n, grown->n);
+            delete grown;
+            old.push_back(prev);
+        }
         if (kn) {
-            k_make_keys<<<grid_for(cn), 256, 0, ks>>>(sbuf + c0, dbuf_ + c0, cn, 32, sym ? 1 : 0, keys + k0);
+            k_make_keys<<<grid_for(cn), 256, 0, ks>>>(sbuf + c0, dbuf_ + c0, cn, 32, sym ? 1 : 0, keys + k0,
+                                                      (outcnt && !info->bad) ? outcnt->get() : nullptr);
             const int cb = (int)id_bits(ci.maxid);
             uint64_t *r1 = nullptr, *r2 = nullptr;
             if ((st = radix_sort_u64(keys + k0, tmp + k0, kn, 0, cb, &r1, ks))) return done(st);
@@ -320,17 +357,21 @@ int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bo
                 cudaMemcpyAsync(keys + k0, r2, kn * 8, cudaMemcpyDeviceToDevice, ks) != cudaSuccess)
                 return done(fail(GCG_ERR_CUDA, "edge pipeline: run copy"));
         }
-        /* runs of level L live in keys (L even) or tmp (L odd) */
+        /* runs of level L live in keys (L even) or tmp (L odd); the final merge is the caller's */
         stack[top++] = Run{0, k0, kn};
-        while (top >= 2 && stack[top - 1].level == stack[top - 2].level) {
+        while (top >= 2 && stack[top - 1].level == stack[top - 2].level && !(i == K - 1 && top == 2)) {
             const Run b = stack[--top], a = stack[--top];
             uint64_t *from = (a.level & 1) ? tmp : keys, *to = (a.level & 1) ? keys : tmp;
             if ((st = merge_u64(from + a.start, a.len, from + b.start, b.len, to + a.start, ks))) return done(st);
             stack[top++] = Run{a.level + 1, a.start, a.len + b.len};
         }
     }
-    if (top != 1) return done(fail(GCG_ERR_CUDA, "edge pipeline: runs left unmerged"));
-    *sorted = (stack[0].level & 1) ? tmp : keys;
+    if (top != 2 || stack[0].level != stack[1].level)
+        return done(fail(GCG_ERR_CUDA, "edge pipeline: runs left unmerged"));
+    for (int r = 0; r < 2; ++r) {
+        runs->p[r] = ((stack[r].level & 1) ? tmp : keys) + stack[r].start;
+        runs->n[r] = stack[r].len;
+    }
     if (cudaStreamSynchronize(ks) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return done(fail(GCG_ERR_CUDA, std::string("edge pipeline: ") + cudaGetErrorString(cudaGetLastError())));
     return done(GCG_OK);
@@ -344,14 +385,24 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
     tbuf<uint32_t> sbuf, dbuf_;
     tbuf<uint64_t> keys, tmp;
     uint64_t *sorted = nullptr;
+    SortedRuns runs = {{nullptr, nullptr}, {0, 0}};
     ScanInfo info;
     uint32_t kbits = 0; /* width of the src half of a key: 32 when sorted in pieces, else vbits */
     const bool pipelined = m >= PIPE_MIN_EDGES && !is_device_ptr(src_u) && !is_device_ptr(dst_u);
+    const bool want_out = !(flags & GCG_BUILD_NO_OUT_CSR);
+    dbuf<uint32_t> outcnt; /* raw out-degrees counted while the pieces are sorted */
+    std::vector<dbuf<uint32_t> *> outgrown;
+    struct FreeOld {
+        std::vector<dbuf<uint32_t> *> &v;
+        ~FreeOld() {
+            for (auto *b : v) delete b;
+        }
+    } free_old{outgrown};
     const uint32_t *src = src_u, *dst = dst_u;
     if (pipelined) {
         if (sbuf.alloc(m, s) || dbuf_.alloc(m, s) || keys.alloc(nk, s) || tmp.alloc(nk, s)) return GCG_ERR_NOMEM;
         GCG_TRY(sort_host_edges(src_u, dst_u, m, sym, nv_given, sbuf.get(), dbuf_.get(), keys.get(), tmp.get(),
-                                &sorted, &info));
+                                &runs, &info, want_out ? nullptr : &outcnt, outgrown));
         kbits = 32;
     } else {
         /* stage inputs */
@@ -396,40 +447,33 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         return st;
     };
 
-    uint64_t ne = kept;
-    if (nk > 0) {
+    uint64_t ne = 0;
+    if (g->in_rowptr.alloc((size_t)nv + 1) || g->in_col.alloc(kept) || g->indeg.alloc(nv) || g->outdeg.alloc(nv))
+        return cleanup(GCG_ERR_NOMEM);
+    {
         int st = GCG_OK;
-        if (!pipelined) {
+        if (!pipelined && nk > 0) {
             if (keys.alloc(nk, s) || tmp.alloc(nk, s)) return cleanup(GCG_ERR_NOMEM);
-            k_make_keys<<<grid_for(m), 256, 0, s>>>(src, dst, m, vbits, sym ? 1 : 0, keys.get());
+            k_make_keys<<<grid_for(m), 256, 0, s>>>(src, dst, m, vbits, sym ? 1 : 0, keys.get(), nullptr);
             if (cudaGetLastError() != cudaSuccess) return cleanup(fail(GCG_ERR_CUDA, "k_make_keys launch"));
             st = radix_sort_u64(keys.get(), tmp.get(), nk, 0, 2 * (int)vbits, &sorted, s);
             if (st) return cleanup(st);
+            runs.p[0] = sorted;
+            runs.n[0] = nk;
         }
-        if ((flags & GCG_BUILD_DEDUP) && kept > 0) {
-            tbuf<uint32_t> fl;
-            tbuf<uint32_t> d_total;
-            if (fl.alloc(kept, s) || d_total.alloc(1, s)) return cleanup(GCG_ERR_NOMEM);
-            uint64_t *other = (sorted == keys.get()) ? tmp.get() : keys.get();
-            if ((st = unique_u64(sorted, kept, fl.get(), d_total.get(), other, s))) return cleanup(st);
-            uint32_t total = 0;
-            if (cudaMemcpyAsync(&total, d_total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess)
-                return cleanup(fail(GCG_ERR_CUDA, "dedup: readback failed"));
-            sorted = other;
-            ne = total;
-        }
+        /* the kept keys go to the buffer that holds no run, when the out-CSR needs them */
+        uint64_t *kept_keys = nullptr;
+        if (want_out && kept > 0) kept_keys = (runs.p[0] >= keys.get() && runs.p[0] < keys.get() + nk) ? tmp.get()
+                                                                                                      : keys.get();
+        st = merge_unique_csr(runs.p[0], runs.n[0], runs.p[1], runs.n[1], kept, (flags & GCG_BUILD_DEDUP) != 0,
+                              kbits, nv, g->in_rowptr.get(), g->in_col.get(), kept_keys,
+                              outcnt.get() && !want_out ? outcnt.get() : nullptr, &ne, s);
+        if (st) return cleanup(st);
+        sorted = kept_keys;
     }
     g->ne = ne;
-    if (g->in_rowptr.alloc((size_t)nv + 1) || g->in_col.alloc(ne) || g->indeg.alloc(nv) || g->outdeg.alloc(nv))
-        return cleanup(GCG_ERR_NOMEM);
-    if (ne == 0) {
-        cudaMemsetAsync(g->in_rowptr.get(), 0, ((size_t)nv + 1) * 4, s);
-    } else {
-        k_csr_from_keys<<<grid_for(ne), 256, 0, s>>>(sorted, ne, kbits, nv, g->in_rowptr.get(), g->in_col.get());
-    }
     k_degree<<<grid_for(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, g->indeg.get());
-    if (!(flags & GCG_BUILD_NO_OUT_CSR)) {
+    if (want_out) {
         if (g->out_rowptr.alloc((size_t)nv + 1) || g->out_col.alloc(ne)) return cleanup(GCG_ERR_NOMEM);
         if (ne == 0) {
             cudaMemsetAsync(g->out_rowptr.get(), 0, ((size_t)nv + 1) * 4, s);
@@ -445,6 +489,12 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         }
         k_degree<<<grid_for(nv), 256, 0, s>>>(g->out_rowptr.get(), nv, g->outdeg.get());
         g->has_out = true;
+    } else if (outcnt.get()) {
+        /* counted during the piecewise sort, repeats taken off by the finish; ids
+         * above the largest one seen (a caller-given vertex count) have none */
+        const size_t have = std::min<size_t>(nv, outcnt.n);
+        if (have < nv) cudaMemsetAsync(g->outdeg.get() + have, 0, (nv - have) * 4, s);
+        cudaMemcpyAsync(g->outdeg.get(), outcnt.get(), have * 4, cudaMemcpyDeviceToDevice, s);
     } else {
         cudaMemsetAsync(g->outdeg.get(), 0, (size_t)nv * 4, s);
         if (ne > 0) {

@@ -172,6 +172,16 @@ int scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *total_dev,
  * first on equal keys); out overlaps neither run. */
 int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t *out, cudaStream_t s);
 
+/* The sharder's last step in one pass: merges sorted runs a and b (b may be
+ * null with nb = 0), keeps the first kept merged keys (the rest are self-loop
+ * sentinels), drops repeats when dedup, and writes the CSR of the kept keys
+ * (row = key >> kbits, column = low kbits): rowptr[0..nv], col[0..*ne). Also
+ * writes the kept keys to keys_out and decrements outdeg_dup[column] for every
+ * dropped repeat, when those are given. Synchronises s. */
+int merge_unique_csr(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t kept, bool dedup,
+                     uint32_t kbits, uint32_t nv, uint32_t *rowptr, uint32_t *col, uint64_t *keys_out,
+                     uint32_t *outdeg_dup, uint64_t *ne, cudaStream_t s);
+
 /* Unique of sorted keys: out[0..total) = distinct keys (flags: n scratch). */
 int unique_u64(const uint64_t *in, uint64_t n, uint32_t *flags, uint32_t *total_dev, uint64_t *out, cudaStream_t s);
 

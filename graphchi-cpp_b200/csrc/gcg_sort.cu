@@ -283,6 +283,177 @@ __global__ void __launch_bounds__(MG_THREADS) k_merge_u64(const uint64_t *__rest
     for (uint32_t x = threadIdx.x; x < tot; x += MG_THREADS) out[d0 + x] = s_in[x];
 }
 
+/* ---- merge + unique + CSR in one pass ------------------------------------
+ * The last merge of the sharder's sorted runs, the duplicate filter, the
+ * compaction offsets and the CSR decode fused: each block merges one tile of
+ * MG_TILE outputs (as k_merge_u64), flags the keys to keep, and finds where its
+ * kept keys start in the output by a decoupled look-back over the tiles before
+ * it (tiles are taken in ticket order, so a block only waits on blocks that are
+ * already running; every wait is bounded and sets an error flag on expiry).
+ * It then writes the column of every kept key, the row pointers of the rows
+ * its keys open, optionally the kept keys themselves, and takes duplicates off
+ * the raw out-degree counts. */
+static_assert(MG_THREADS == RS_THREADS, "block_excl_scan is sized for RS_THREADS");
+constexpr uint32_t TS_AGG = 1u, TS_INC = 2u;
+constexpr long long LB_SPIN = 1ll << 22;
+
+__device__ __forceinline__ void ts_store(unsigned long long *p, uint32_t status, uint32_t val) {
+    const unsigned long long w = ((unsigned long long)status << 32) | val;
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ts_load(const unsigned long long *p) {
+    unsigned long long w;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+
+struct FinishArgs {
+    const uint64_t *a, *b;
+    uint64_t na, nb, kept;
+    const uint64_t *split;
+    uint32_t kbits, nv;
+    int dedup;
+    uint32_t *rowptr, *col;
+    uint64_t *keys_out;   /* kept keys, or null */
+    uint32_t *outdeg_dup; /* raw out-degree counts to take duplicates off, or null */
+    uint32_t *ticket;
+    unsigned long long *tstate;
+    uint32_t *total;
+    int *err;
+};
+
+/* exclusive prefix of tile t's kept keys: warp 0 walks back over the tile states,
+ * 32 at a time, until it meets an inclusive prefix */
+__device__ __forceinline__ uint32_t look_back(const FinishArgs &f, uint32_t t, uint32_t lane) {
+    uint32_t excl = 0;
+    int64_t j = (int64_t)t - 1;
+    while (j >= 0) {
+        const int64_t idx = j - (int64_t)lane;
+        unsigned long long w = 0;
+        if (idx >= 0) {
+            long long spin = 0;
+            do {
+                w = ts_load(f.tstate + idx);
+            } while ((w >> 32) == 0 && ++spin < LB_SPIN);
+            if ((w >> 32) == 0) atomicExch(f.err, 1);
+        }
+        const uint32_t status = (uint32_t)(w >> 32);
+        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, idx >= 0 && status == TS_INC);
+        const uint32_t stop = inc ? (uint32_t)(__ffs(inc) - 1) : 31u; /* nearest inclusive tile */
+        uint32_t v = (idx >= 0 && lane <= stop) ? (uint32_t)w : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        excl += v;
+        if (inc) break;
+        j -= 32;
+    }
+    return excl;
+}
+
+__global__ void __launch_bounds__(MG_THREADS) k_merge_finish(FinishArgs f) {
+    __shared__ uint64_t s_in[MG_TILE];
+    __shared__ uint32_t s_warp[RS_WARPS];
+    __shared__ uint32_t s_tile, s_excl, s_sum;
+    if (threadIdx.x == 0) s_tile = atomicAdd(f.ticket, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const uint64_t n = f.na + f.nb;
+    const uint64_t d0 = (uint64_t)t * MG_TILE;
+    const uint64_t d1 = d0 + MG_TILE < n ? d0 + MG_TILE : n;
+    const uint64_t a0 = f.split[t], a1 = f.split[t + 1];
+    const uint64_t b0 = d0 - a0, b1 = d1 - a1;
+    const uint32_t la = (uint32_t)(a1 - a0), lb = (uint32_t)(b1 - b0), tot = la + lb;
+    for (uint32_t i = threadIdx.x; i < la; i += MG_THREADS) s_in[i] = f.a[a0 + i];
+    for (uint32_t i = threadIdx.x; i < lb; i += MG_THREADS) s_in[la + i] = f.b[b0 + i];
+    __syncthreads();
+    const uint64_t *sa = s_in, *sb = s_in + la;
+    const uint32_t dg = threadIdx.x * MG_ITEMS < tot ? threadIdx.x * MG_ITEMS : tot;
+    uint32_t i = merge_path<uint32_t>(sa, la, sb, lb, dg), j = dg - i;
+    uint64_t v[MG_ITEMS];
+#pragma unroll
+    for (int k = 0; k < MG_ITEMS; ++k) {
+        v[k] = 0;
+        if (dg + k < tot) {
+            const bool take_a = i < la && (j >= lb || sa[i] <= sb[j]);
+            v[k] = take_a ? sa[i] : sb[j];
+            if (take_a) ++i; else ++j;
+        }
+    }
+    /* the key before this thread's first: the previous thread's last, or the
+     * previous tile's last (the larger of the last a and b keys before it) */
+    uint64_t prev = 0;
+    if (threadIdx.x == 0) {
+        if (d0 > 0) {
+            const uint64_t x = a0 ? f.a[a0 - 1] : 0ull, y = b0 ? f.b[b0 - 1] : 0ull;
+            prev = x > y ? x : y;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < MG_ITEMS; ++k)
+        if (dg + k < tot) s_in[dg + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x > 0 && dg > 0) prev = s_in[dg - 1];
+    uint32_t fl = 0, cnt = 0;
+    {
+        uint64_t pk = prev;
+#pragma unroll
+        for (int k = 0; k < MG_ITEMS; ++k) {
+            const uint64_t gi = d0 + dg + k;
+            if (dg + k < tot && gi < f.kept) {
+                const bool keep = !f.dedup || gi == 0 || v[k] != pk;
+                fl |= (keep ? 1u : 0u) << k;
+                cnt += keep ? 1u : 0u;
+            }
+            pk = v[k];
+        }
+    }
+    const uint32_t local = block_excl_scan(cnt, s_warp);
+    if (threadIdx.x == MG_THREADS - 1) {
+        const uint32_t tile_sum = local + cnt;
+        if (t == 0) ts_store(f.tstate, TS_INC, tile_sum);
+        else ts_store(f.tstate + t, TS_AGG, tile_sum);
+        s_sum = tile_sum;
+    }
+    __syncthreads();
+    const uint32_t tile_sum = s_sum;
+    if (threadIdx.x < 32) {
+        uint32_t excl = 0;
+        if (t > 0) {
+            excl = look_back(f, t, threadIdx.x);
+            if (threadIdx.x == 0) ts_store(f.tstate + t, TS_INC, excl + tile_sum);
+        }
+        if (threadIdx.x == 0) s_excl = excl;
+    }
+    __syncthreads();
+    const uint64_t mask = (f.kbits >= 64) ? ~0ull : ((1ull << f.kbits) - 1ull);
+    uint32_t p = s_excl + local;
+    uint64_t pk = prev;
+#pragma unroll
+    for (int k = 0; k < MG_ITEMS; ++k) {
+        const uint64_t gi = d0 + dg + k;
+        if (dg + k < tot && gi < f.kept) {
+            const uint64_t key = v[k];
+            const uint32_t row = (uint32_t)(key >> f.kbits);
+            if ((fl >> k) & 1u) {
+                f.col[p] = (uint32_t)(key & mask);
+                if (f.keys_out) f.keys_out[p] = key;
+                const int64_t prow = gi == 0 ? -1 : (int64_t)(pk >> f.kbits);
+                for (int64_t r = prow + 1; r <= (int64_t)row; ++r) f.rowptr[r] = p;
+                ++p;
+            } else if (f.outdeg_dup) {
+                atomicSub(f.outdeg_dup + (uint32_t)(key & mask), 1u);
+            }
+            if (gi == f.kept - 1) { /* rows after the last key end at the total */
+                for (uint64_t r = (uint64_t)row + 1; r <= f.nv; ++r) f.rowptr[r] = p;
+                *f.total = p;
+            }
+        }
+        pk = v[k];
+    }
+}
+
 }  // namespace
 
 int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t *out, cudaStream_t s) {
@@ -300,6 +471,55 @@ int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, ui
         a, na, b, nb, ntiles, split.get());
     k_merge_u64<<<(unsigned)ntiles, MG_THREADS, 0, s>>>(a, na, b, nb, split.get(), out);
     GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
+int merge_unique_csr(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, uint64_t kept, bool dedup,
+                     uint32_t kbits, uint32_t nv, uint32_t *rowptr, uint32_t *col, uint64_t *keys_out,
+                     uint32_t *outdeg_dup, uint64_t *ne, cudaStream_t s) {
+    *ne = 0;
+    if (kept == 0) {
+        GCG_CUDA(cudaMemsetAsync(rowptr, 0, ((size_t)nv + 1) * 4, s));
+        return GCG_OK;
+    }
+    const uint64_t n = na + nb;
+    if (kept > n || kept > 0xFFFFFFFFull) return fail(GCG_ERR_INVALID, "merge_unique_csr: bad key count");
+    const uint64_t ntiles = (kept + MG_TILE - 1) / MG_TILE;
+    tbuf<uint64_t> split;
+    tbuf<unsigned long long> tstate;
+    tbuf<uint32_t> ctl; /* ticket, total, err */
+    GCG_TRY(split.alloc(ntiles + 1, s));
+    GCG_TRY(tstate.alloc(ntiles, s));
+    GCG_TRY(ctl.alloc(3, s));
+    GCG_CUDA(cudaMemsetAsync(tstate.get(), 0, ntiles * sizeof(unsigned long long), s));
+    GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 3 * sizeof(uint32_t), s));
+    k_merge_split<<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
+        a, na, b ? b : a, nb, ntiles, split.get());
+    FinishArgs f;
+    f.a = a;
+    f.b = b ? b : a;
+    f.na = na;
+    f.nb = nb;
+    f.kept = kept;
+    f.split = split.get();
+    f.kbits = kbits;
+    f.nv = nv;
+    f.dedup = dedup ? 1 : 0;
+    f.rowptr = rowptr;
+    f.col = col;
+    f.keys_out = keys_out;
+    f.outdeg_dup = outdeg_dup;
+    f.ticket = ctl.get();
+    f.tstate = tstate.get();
+    f.total = ctl.get() + 1;
+    f.err = (int *)(ctl.get() + 2);
+    k_merge_finish<<<(unsigned)ntiles, MG_THREADS, 0, s>>>(f);
+    GCG_LAUNCH_CHECK();
+    uint32_t h[2] = {0, 0};
+    GCG_CUDA(cudaMemcpyAsync(h, ctl.get() + 1, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    if (h[1]) return fail(GCG_ERR_TIMEOUT, "merge_unique_csr: a tile's prefix never arrived");
+    *ne = h[0];
     return GCG_OK;
 }
 

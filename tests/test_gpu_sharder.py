@@ -159,7 +159,8 @@ def test_large_sort_matches_numpy():
 
 def _same_graph(a, b):
     assert (a.num_vertices, a.num_edges) == (b.num_vertices, b.num_edges)
-    for w in (gcgpu.CSR_IN, gcgpu.CSR_OUT):
+    assert a.info().has_out_csr == b.info().has_out_csr
+    for w in ((gcgpu.CSR_IN, gcgpu.CSR_OUT) if a.info().has_out_csr else (gcgpu.CSR_IN,)):
         ra, ca = a.csr(w)
         rb, cb = b.csr(w)
         assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
@@ -167,12 +168,17 @@ def _same_graph(a, b):
     assert np.array_equal(a.intervals(), b.intervals())
 
 
-@pytest.mark.parametrize("sym,dedup,pinned", [(False, True, True), (True, True, True), (False, False, False)])
-def test_host_edges_sorted_in_pieces_equal_one_sort(sym, dedup, pinned):
+@pytest.mark.parametrize("sym,dedup,pinned,out_csr,extra", [
+    (False, True, True, True, 0), (True, True, True, False, 0), (False, False, False, True, 0),
+    (False, True, True, False, 100), (True, False, True, False, 0)])
+def test_host_edges_sorted_in_pieces_equal_one_sort(sym, dedup, pinned, out_csr, extra):
     """From 2^24 host edges on, the sharder sorts pieces of the edge list while
-    later pieces are still being copied in and merges the sorted runs; the graph
-    equals the one sorted in one piece from the same edges on the device. The
-    last piece is ragged; R-MAT brings self-loops and duplicates."""
+    later pieces are still being copied in, merges the sorted runs and fuses the
+    last merge with the duplicate filter and the CSR decode (out-degrees are
+    counted per piece when no out-CSR is built); the graph equals the one sorted
+    in one piece from the same edges on the device. The last piece is ragged;
+    R-MAT brings self-loops and duplicates; extra > 0 gives trailing isolated
+    vertices through a caller-given vertex count."""
     import torch
     m = (1 << 24) + 12345
     s, d = O.rmat_numpy(20, m, seed=31)
@@ -183,8 +189,9 @@ def test_host_edges_sorted_in_pieces_equal_one_sort(sym, dedup, pinned):
         hd = torch.from_numpy(d.view(np.int32)).pin_memory()
     else:
         hs, hd = s, d
-    with gcgpu.Graph.from_edges(hs, hd, dedup=dedup, symmetrise=sym, nshards=8) as a, \
-            gcgpu.Graph.from_edges(ts, td, dedup=dedup, symmetrise=sym, nshards=8) as b:
+    nv = (1 << 20) + extra if extra else 0
+    kw = dict(num_vertices=nv, dedup=dedup, symmetrise=sym, nshards=8, out_csr=out_csr)
+    with gcgpu.Graph.from_edges(hs, hd, **kw) as a, gcgpu.Graph.from_edges(ts, td, **kw) as b:
         _same_graph(a, b)
         if not sym and dedup:
             keep = s != d
