@@ -840,7 +840,7 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
 static int batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_out, uint32_t *grab_out, double *ms_out) {
     const ChunkPlan &pl = *b->u->cplan;
     std::vector<uint32_t> hubs;
-    for (uint32_t h : {0u, 8192u, 16384u, 32768u, HUB_MAX})
+    for (uint32_t h : {0u, 8192u, 16384u, 32768u, HUB_DEFAULT, HUB_MAX})
         if (h <= pl.hub && std::find(hubs.begin(), hubs.end(), h) == hubs.end()) hubs.push_back(h);
     if (std::find(hubs.begin(), hubs.end(), pl.hub) == hubs.end()) hubs.push_back(pl.hub);
     const uint32_t grabs[] = {0u, 1u, 4u, 16u};

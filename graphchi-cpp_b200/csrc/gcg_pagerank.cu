@@ -704,7 +704,7 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
     GCG_TRY(ensure_chunk_plan(g));
     ChunkPlan &pl = *g->cplan;
     std::vector<uint32_t> hubs;
-    for (uint32_t h : {0u, 16384u, 32768u, HUB_MAX})
+    for (uint32_t h : {0u, 16384u, 32768u, HUB_DEFAULT, HUB_MAX})
         if (h <= pl.hub && std::find(hubs.begin(), hubs.end(), h) == hubs.end()) hubs.push_back(h);
     if (std::find(hubs.begin(), hubs.end(), pl.hub) == hubs.end()) hubs.push_back(pl.hub);
     const uint32_t runs[] = {1u, 2u, 4u, 16u};
@@ -716,7 +716,7 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
     tbuf<float> out;
     GCG_TRY(out.alloc(std::max<uint32_t>(g->nv, 1), g->stream));
     double best = 1e300;
-    uint32_t bh = pl.hub, br = 1;
+    uint32_t bh = std::min(pl.hub, HUB_DEFAULT), br = RUN_DEFAULT;
     for (uint32_t h : hubs)
         for (uint32_t r : runs) {
             pl.tune_hub = h;

@@ -228,10 +228,12 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * depend on it): hub_entries = shared-memory contribution cache entries (sources
  * whose out-degree rank is below it are read from shared memory; capped at the
  * plan's 49152), chunk_run = consecutive 256-edge chunks a warp takes at a time
- * (1 = warps stride chunk by chunk). gcg_pagerank_autotune times `sweeps` fixed
- * sweeps of each candidate (hub entries {0, 16384, 32768, 49152, the plan's} x
- * runs {1, 2, 4, 16}), keeps the fastest for later calls on this graph and
- * reports it (outputs may be NULL). */
+ * (1 = warps stride chunk by chunk). Default: 41728 entries (the largest hub
+ * that leaves the SM its 164 KB shared-memory carve-out, so L1 keeps ~92 KB) and
+ * chunk_run 2, the fastest measured at R-MAT scale 24. gcg_pagerank_autotune
+ * times `sweeps` fixed sweeps of each candidate (hub entries {0, 16384, 32768,
+ * 41728, 49152, the plan's} x runs {1, 2, 4, 16}), keeps the fastest for later
+ * calls on this graph and reports it (outputs may be NULL). */
 int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_run);
 int gcg_pagerank_get_config(gcg_graph *g, uint32_t *hub_entries, uint32_t *chunk_run);
 int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint32_t *chunk_run, double *ms_per_sweep);
@@ -281,7 +283,7 @@ int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ran
  * candidate configuration and keeps the fastest for later solves (results do not
  * depend on it). Candidates: shared-memory hub entries (sources whose out-degree
  * rank is below it are read from shared memory: the degree threshold of the
- * cache) in {0, 8192, 16384, 32768, 49152, the plan's}, and the edge phase's work
+ * cache) in {0, 8192, 16384, 32768, 41728, 49152, the plan's}, and the edge phase's work
  * distribution: warps striding over the chunks (queue_run 0) or taking runs of
  * 1, 4 or 16 chunks from a device work queue. Outputs may be NULL. */
 int gcg_batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_entries, uint32_t *queue_run, double *ms_per_sweep);
