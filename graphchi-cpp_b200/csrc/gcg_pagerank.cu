@@ -101,7 +101,17 @@ __global__ void k_split_list(const uint32_t *__restrict__ nz_start, uint32_t nnz
 
 
 
+/* Programmatic dependent launch: the three sweep kernels are queued with
+ * programmatic stream serialisation, so a kernel's blocks may be scheduled while
+ * its predecessor drains. Each kernel first waits (griddepcontrol.wait) until its
+ * predecessor has completed and its writes are visible, and lets its own
+ * successor be scheduled as soon as all its blocks are running. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
+    pdl_wait();
+    pdl_launch_next();
     if (*(volatile const int *)a.done) return;
     extern __shared__ float s_hub[];
     const uint32_t lane = threadIdx.x & 31u;
@@ -140,6 +150,8 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
  * partials of each long (hub) row cooperatively: lane-strided partial sums, then
  * a fixed xor-shuffle tree, so the order is fixed. */
 __global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
+    pdl_wait();
+    pdl_launch_next();
     if (*(volatile const int *)a.done) return;
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
@@ -197,6 +209,8 @@ __device__ __forceinline__ double2 block_sum2(double x, double y, double2 *s_red
 }
 
 __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int const_pass) {
+    pdl_wait();
+    pdl_launch_next();
     if (*(volatile const int *)a.done) return;
     __shared__ double2 s_red[8];
     __shared__ int s_last;
@@ -422,9 +436,26 @@ int ensure_chunk_plan(gcg_graph *g) {
     return GCG_OK;
 }
 
+/* queues kern<<<grid, block, smem, s>>>(args...) with programmatic stream
+ * serialisation (the kernel must begin with pdl_wait) */
+template <typename... K, typename... Args>
+static void launch_pdl(void (*kern)(K...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 /* one CTA of EDGE_THREADS per SM (the hub cache takes most of shared memory) */
 static void launch_edges(int ge, uint32_t hub_bytes, cudaStream_t s, const SweepArgs &a) {
-    k_pr_edges<<<ge, EDGE_THREADS, hub_bytes, s>>>(a);
+    launch_pdl(k_pr_edges, ge, EDGE_THREADS, hub_bytes, s, a);
 }
 
 static int edge_grid(uint32_t hub_bytes) {
@@ -571,8 +602,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
             } else {
                 launch_edges(ge, hub_bytes, s, a);
             }
-            k_pr_fix<<<fg, 256, 0, s>>>(a);
-            k_pr_vertex<<<gv, 256, 0, s>>>(a, sw, sw < 2 ? 1 : 0);
+            launch_pdl(k_pr_fix, fg, 256, 0, s, a);
+            launch_pdl(k_pr_vertex, gv, 256, 0, s, a, sw, sw < 2 ? 1 : 0);
         }
         launched += n;
         if (cudaGetLastError() != cudaSuccess) {
