@@ -205,10 +205,19 @@ def run_extras(args):
         gb.free()
     del s, d
     bms = min(t_build[1:])
+    # the LSD sort of (dst, src) keys: ceil(b/8) 8-bit digit passes per half, b = bits of a vertex id;
+    # a pass reads every key twice (histogram, scatter) and writes it once: 24 bytes per key
+    vb = max(1, int(args.scale))
+    passes = 2 * ((vb + 7) // 8)
+    pass_bytes = 24.0 * m * passes
     out["sharder"] = {"raw_edges": m, "ms": bms, "first_call_ms": t_build[0], "sort_bytes_16E": 16.0 * m,
                       "frac_of_16E_at_hbm_peak": 16.0 * m / peak / 1e6 / bms,
-                      "note": "dedup + in-CSR + degrees + 64 intervals; the LSD sort makes 2b/8 passes of "
-                              "24 bytes per key (b = bits of a vertex id), so 16E is a one-pass lower bound"}
+                      "radix_passes": passes, "radix_pass_bytes": pass_bytes,
+                      "frac_of_radix_pass_bytes_at_hbm_peak": pass_bytes / peak / 1e6 / bms,
+                      "note": "dedup + in-CSR + degrees + 64 intervals, whole build timed; 16E is the one-pass "
+                              "lower bound of a sort, radix_pass_bytes what the LSD passes move (24 B per key "
+                              "per pass); the scatter pass is bound by shared-memory bank conflicts, see "
+                              "profiles/sharder_radix_rmat22.md"}
 
     # ---- connected components (and triangles at scale 20) ----
     cc = {}
