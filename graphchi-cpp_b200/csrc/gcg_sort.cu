@@ -7,7 +7,7 @@
  *   per 8-bit digit pass: upsweep (per-tile digit histogram, per-warp shared-memory
  *   counters) -> exclusive scan of the digit-major count table -> downsweep (each
  *   warp ranks its own contiguous 512 keys with warp-private digit counters and
- *   __match_any_sync, one digit-major scan over (digit, warp) gives every key its
+ *   per-bit ballots, one digit-major scan over (digit, warp) gives every key its
  *   place in the tile, keys are regrouped by digit in shared memory and written so
  *   that each digit run of a tile is a contiguous, coalesced store).
  * Tiles are 4096 keys (256 threads x 16); each warp reads its 512 keys as 16
@@ -110,10 +110,13 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint64_t *__res
         key[k] = (i < n) ? __ldg(keys_in + i) : 0ull;
     }
     for (int w = 0; w < RS_WARPS; ++w) s_wcnt[w][tid] = 0;
-    s_gofs[tid] = offsets[(uint64_t)tid * ntiles + blockIdx.x];
+    const uint32_t gofs = offsets[(uint64_t)tid * ntiles + blockIdx.x];
     const uint32_t h = counts[(uint64_t)tid * ntiles + blockIdx.x];
     const uint32_t lstart = block_excl_scan(h, s_scan); /* synchronises: s_wcnt is clear */
     s_lstart[tid] = lstart;
+    /* tile position i of digit d goes to gofs[d] + (i - lstart[d]); one table
+     * instead of two (uint32 wrap-around is exact: every index is below 2^32) */
+    s_gofs[tid] = gofs - lstart;
 
     /* warp-private ranking over the warp's 16 rounds, in key order */
     uint16_t lrank[RS_ITEMS];
@@ -122,7 +125,14 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint64_t *__res
         const uint64_t i = wbase + (uint64_t)k * 32 + lane;
         const bool valid = i < n;
         const uint32_t d = valid ? (uint32_t)((key[k] >> shift) & dmask) : 256u;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        /* lanes holding the same digit, from one vote per digit bit (cheaper here
+         * than __match_any_sync, which competes with the shared-memory traffic) */
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t vb = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? vb : ~vb;
+        }
         const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
         lrank[k] = (uint16_t)(before + __popc(peers & lanemask_lt()));
         __syncwarp();
@@ -153,7 +163,7 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint64_t *__res
     for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
         const uint64_t kk = s_keys[i];
         const uint32_t d = (uint32_t)((kk >> shift) & dmask);
-        keys_out[(uint64_t)s_gofs[d] + (i - s_lstart[d])] = kk;
+        keys_out[(uint32_t)(s_gofs[d] + i)] = kk;
     }
 }
 
