@@ -458,7 +458,8 @@ int copy_columns(const float *src, uint32_t kp, uint32_t nv, const std::vector<u
  * that sweep; whenever the columns still iterating fit a layout at most 3/4 as
  * wide, they are compacted into it, so later sweeps gather narrower rows. */
 int ppr_group(gcg_graph *g, const PprPlan &pl, const uint32_t *src_host, uint32_t k, const gcg_pr_params *p,
-              float *out, uint32_t out_pitch, gcg_pr_stats *st, std::vector<double> *res_log) {
+              float *out, uint32_t out_pitch, gcg_pr_stats *st, std::vector<double> *res_log,
+              std::vector<int> *col_sweeps) {
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
     const int max_sweeps = p->max_sweeps;
@@ -673,6 +674,7 @@ int ppr_group(gcg_graph *g, const PprPlan &pl, const uint32_t *src_host, uint32_
         worst = std::max(worst, fin_res[j]);
         if (!(p->tol > 0.0 && fin_res[j] <= p->tol)) conv = false;
     }
+    if (col_sweeps) col_sweeps->insert(col_sweeps->end(), fin_sweeps.begin(), fin_sweeps.end());
     st->sweeps = std::max(st->sweeps, mx);
     st->converged = st->converged && conv;
     st->residual = std::max(st->residual, worst);
@@ -704,11 +706,29 @@ extern "C" int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t n
     GCG_TRY(ensure_ppr_plan(g));
     gcg_pr_stats st = {0, 1, 0.0, 0.0, 0.0, 0, 0};
     std::vector<double> lg;
+    std::vector<int> col_sweeps; /* sweeps each source took */
     for (uint32_t g0 = 0; g0 < nsources; g0 += KMAX) {
         const uint32_t k = std::min(KMAX, nsources - g0);
-        GCG_TRY(ppr_group(g, *g->pplan, src.data() + g0, k, params, out + g0, nsources, &st, &lg));
+        GCG_TRY(ppr_group(g, *g->pplan, src.data() + g0, k, params, out + g0, nsources, &st, &lg, &col_sweeps));
     }
     if (params->residuals && !lg.empty()) GCG_TRY(copy_out(params->residuals, lg.data(), lg.size() * 8, g->stream));
+    if (params->work_log && params->max_sweeps > 0) {
+        /* cumulative work of the sources still iterating: sweep i updates every
+         * vertex and gathers every in-edge once per source with more than i sweeps */
+        const int S = params->max_sweeps;
+        std::vector<uint64_t> active((size_t)S + 1, 0);
+        for (int c : col_sweeps) ++active[(size_t)std::min(c, S)];
+        std::vector<uint64_t> wl(2 * (size_t)S);
+        uint64_t left = col_sweeps.size(), upd = 0, gat = 0;
+        for (int i = 0; i < S; ++i) {
+            left -= active[(size_t)i]; /* sources that took exactly i sweeps are done */
+            upd += left * (uint64_t)g->nv;
+            gat += left * g->ne;
+            wl[2 * (size_t)i] = upd;
+            wl[2 * (size_t)i + 1] = gat;
+        }
+        GCG_TRY(copy_out(params->work_log, wl.data(), wl.size() * 8, g->stream));
+    }
     if (stats) *stats = st;
     return GCG_OK;
 }

@@ -355,8 +355,10 @@ class Graph:
         return h.value, r.value, ms.value
 
     def ppr_batched(self, sources, max_sweeps=100, teleport=0.15, damping=0.85, tol=0.0, out=None,
-                    residuals=None, time_sweeps=False):
-        """Batched personalised PageRank; returns (V x k ranks, PrStats)."""
+                    residuals=None, time_sweeps=False, work_log=None):
+        """Batched personalised PageRank; returns (V x k ranks, PrStats). work_log
+        (2 x max_sweeps uint64) receives the cumulative (vertex updates, in-edge
+        gathers) of the sources still iterating."""
         src = np.ascontiguousarray(sources, dtype=np.uint32) if isinstance(sources, (list, np.ndarray)) else sources
         k = int(src.shape[0])
         p = PrParams()
@@ -365,6 +367,8 @@ class Graph:
         p.flags = PR_TIME_SWEEPS if time_sweeps else 0
         if residuals is not None:
             p.residuals = ptr(residuals)
+        if work_log is not None:
+            p.work_log = ptr(work_log)
         if out is None:
             out = np.zeros((self.num_vertices, k), dtype=np.float32)
         st = PrStats()

@@ -250,7 +250,10 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
  * mode must be GCG_PR_JACOBI, init_rank NULL and source GCG_NO_SOURCE.
  * sources: nsources ids, host or device. out: num_vertices x nsources floats,
  * out[v * nsources + s], host or device. params->residuals (if set) receives the
- * per-sweep maximum residual of the sources still iterating. stats->sweeps is
+ * per-sweep maximum residual of the sources still iterating; params->work_log
+ * (if set, 2 x max_sweeps entries) the cumulative work: work_log[2i] = vertex
+ * updates and work_log[2i+1] = in-edges gathered, summed over the sources still
+ * iterating in sweeps 0..i (V and E per source and sweep). stats->sweeps is
  * the largest per-source count. Sources run in groups of 256. */
 int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t nsources, const gcg_pr_params *params,
                     float *out, gcg_pr_stats *stats);

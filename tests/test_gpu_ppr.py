@@ -92,3 +92,26 @@ def test_scalar_personalised_pagerank_vs_oracle():
     with gcgpu.Graph.from_edges(s, d, dedup=True) as g:
         r, st = g.pagerank(max_sweeps=30, teleport=TELE, source=5)
     assert np.abs(r - ref[:, 0]).sum() / np.abs(ref[:, 0]).sum() <= L1_TOL
+
+
+def test_ppr_batched_work_log_counts_the_sources_still_iterating():
+    # without a tolerance every source runs every sweep: the log grows by k x (V, E)
+    s, d = O.rmat_numpy(10, 16 << 10, seed=5)
+    with gcgpu.Graph.from_edges(s, d, dedup=True) as g:
+        V, E, k, S = g.num_vertices, g.num_edges, 40, 25
+        src = np.random.default_rng(5).integers(0, V, k).astype(np.uint32)
+        wl = np.zeros(2 * S, np.uint64)
+        _, st = g.ppr_batched(src, max_sweeps=S, teleport=TELE, work_log=wl)
+        i = np.arange(1, S + 1, dtype=np.uint64)
+        assert np.array_equal(wl[0::2], i * k * V) and np.array_equal(wl[1::2], i * k * E)
+        # with one: sources leave as they converge, so the increments shrink, the
+        # first is all k sources and the log stays flat after the last sweep
+        S = 300
+        src = np.random.default_rng(6).integers(0, V, 64).astype(np.uint32)
+        wl = np.zeros(2 * S, np.uint64)
+        _, st = g.ppr_batched(src, max_sweeps=S, teleport=TELE, tol=1e-8, work_log=wl)
+        upd, gat = wl[0::2].astype(np.int64), wl[1::2].astype(np.int64)
+        assert np.array_equal(gat * V, upd * E)
+        inc = np.diff(np.concatenate([[0], gat]))
+        assert inc[0] == 64 * E and np.all(np.diff(inc) <= 0)
+        assert inc[st.sweeps - 1] >= E and np.all(inc[st.sweeps:] == 0)
