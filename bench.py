@@ -147,6 +147,32 @@ def reference_pagerank_sample(scale, ef, seed, niters, threads, steps=1, warmup=
     return vals, E, sample, extra
 
 
+def reference_time_to_tol(scale, ef, seed, tol, threads):
+    """Times the reference's own functional (bulk-synchronous) engine running a
+    PageRank kernel with a residual stop (oracle/_ref/pr_functional_oracle) to
+    normalised L1 `tol` on an R-MAT sample: measured time to tolerance."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import gcgpu
+    s, d = gcgpu.generate_rmat(scale, ef << scale, seed=seed)
+    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
+    E = int(cs.shape[0])
+    with O.RefWorkdir(prefix="gcg_bench_ttt_") as w:
+        el = w.file("g.el")
+        O.write_edgelist(el, cs, cd)
+        O.run_ref("pr_functional_oracle", el, {"niters": 1, "nshards": "auto"}, threads)  # shards, untimed
+        out, wall = O.run_ref("pr_functional_oracle", el, {"niters": 1000, "tol": tol, "teleport": "const",
+                                                            "nshards": "auto"}, threads)
+    its = [int(line.split()[1]) for line in out.splitlines() if line.startswith("iterations")]
+    n = its[-1] if its else 0
+    rt = O.ref_runtime(out) or wall
+    return {"program": "oracle/_ref/pr_functional_oracle (the reference's functional engine, bulk-synchronous, "
+                       "apply 0.15 + 0.85 sum, after_iteration residual stop)",
+            "graph": f"rmat{scale}_ef{ef}_seed{seed}", "edges": E, "tol": tol, "iterations": n,
+            "converged": n < 1000, "runtime_s": rt, "wall_s": wall, "GTEPS": E * n / rt / 1e9 if rt > 0 else None,
+            "threads": threads}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -430,6 +456,8 @@ def run_ours(args, rank, world):
             cpu["estimated_s_to_tol_at_headline_size"] = E * sweeps[0] / (vals[0] * 1e9)
             cpu["estimate_note"] = ("per-iteration rate of the sample x the sweeps the headline solve needs; "
                                     "the reference's PageRank has no residual stop (pagerank.cpp)")
+            cpu["functional_time_to_tol"] = reference_time_to_tol(16, args.ef, args.seed, args.tol,
+                                                                  os.cpu_count() or 1)
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"[:300]}
