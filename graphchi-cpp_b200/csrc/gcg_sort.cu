@@ -231,12 +231,26 @@ __global__ void __launch_bounds__(SC_THREADS) sc_scan_tile(const uint32_t *in, u
 /* ---- merge of two sorted runs (merge path) ------------------------------ */
 
 constexpr int MG_THREADS = 256;
-constexpr int MG_ITEMS = 8;
+constexpr int MG_ITEMS = 8; /* pairwise merges of the piecewise sort */
 constexpr int MG_TILE = MG_THREADS * MG_ITEMS;
+constexpr int MF_ITEMS = 16; /* the fused last merge: larger tiles hide its per-tile latency */
+constexpr int MF_TILE = MG_THREADS * MF_ITEMS;
+
+/* Tiles are staged in shared memory with one pad slot after every ITEMS keys, so
+ * the ITEMS consecutive keys a thread writes after merging fall on distinct banks. */
+template <int ITEMS>
+__device__ __forceinline__ uint32_t padx(uint32_t e) { return e + e / ITEMS; }
+
+template <int ITEMS>
+struct SView { /* keys [off, off + n) of a padded tile */
+    const uint64_t *s;
+    uint32_t off;
+    __device__ __forceinline__ uint64_t operator[](uint32_t i) const { return s[padx<ITEMS>(off + i)]; }
+};
 
 /* how many of the first diag outputs come from a (a first on equal keys) */
-template <typename I>
-__device__ __forceinline__ I merge_path(const uint64_t *a, I na, const uint64_t *b, I nb, I diag) {
+template <typename A, typename B, typename I>
+__device__ __forceinline__ I merge_path(const A &a, I na, const B &b, I nb, I diag) {
     I lo = diag > nb ? diag - nb : 0, hi = diag < na ? diag : na;
     while (lo < hi) {
         const I mid = (lo + hi) >> 1;
@@ -245,39 +259,33 @@ __device__ __forceinline__ I merge_path(const uint64_t *a, I na, const uint64_t 
     return lo;
 }
 
-/* split[t] = a's share of the first t*MG_TILE outputs, t = 0..ntiles */
+/* split[t] = a's share of the first t*TILE outputs, t = 0..ntiles */
+template <int TILE>
 __global__ void k_merge_split(const uint64_t *__restrict__ a, uint64_t na, const uint64_t *__restrict__ b,
                               uint64_t nb, uint64_t ntiles, uint64_t *__restrict__ split) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles;
          t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t d = t * MG_TILE < na + nb ? t * MG_TILE : na + nb;
-        split[t] = merge_path<uint64_t>(a, na, b, nb, d);
+        const uint64_t d = t * TILE < na + nb ? t * TILE : na + nb;
+        split[t] = merge_path(a, na, b, nb, d);
     }
 }
 
-/* One output tile per block: its pieces of a and b are staged in shared memory,
- * each thread merges MG_ITEMS outputs from its own merge-path split, and the
- * tile is written back with coalesced stores. */
-__global__ void __launch_bounds__(MG_THREADS) k_merge_u64(const uint64_t *__restrict__ a, uint64_t na,
-                                                          const uint64_t *__restrict__ b, uint64_t nb,
-                                                          const uint64_t *__restrict__ split,
-                                                          uint64_t *__restrict__ out) {
-    __shared__ uint64_t s_in[MG_TILE];
-    const uint64_t n = na + nb;
-    const uint64_t d0 = (uint64_t)blockIdx.x * MG_TILE;
-    const uint64_t d1 = d0 + MG_TILE < n ? d0 + MG_TILE : n;
-    const uint64_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
-    const uint64_t b0 = d0 - a0, b1 = d1 - a1;
-    const uint32_t la = (uint32_t)(a1 - a0), lb = (uint32_t)(b1 - b0), tot = la + lb;
-    for (uint32_t i = threadIdx.x; i < la; i += MG_THREADS) s_in[i] = a[a0 + i];
-    for (uint32_t i = threadIdx.x; i < lb; i += MG_THREADS) s_in[la + i] = b[b0 + i];
+/* Stages a tile's pieces a[a0, a0+la) and b[b0, b0+lb) in s, merges them (each
+ * thread ITEMS outputs from its own merge-path split) and leaves the merged tile
+ * in s (padded); v[k] = merged output dg + k of this thread. */
+template <int ITEMS>
+__device__ __forceinline__ void tile_merge(const uint64_t *__restrict__ a, uint64_t a0, uint32_t la,
+                                           const uint64_t *__restrict__ b, uint64_t b0, uint32_t lb, uint64_t *s,
+                                           uint64_t (&v)[ITEMS], uint32_t &dg) {
+    const uint32_t tot = la + lb;
+    for (uint32_t i = threadIdx.x; i < la; i += MG_THREADS) s[padx<ITEMS>(i)] = a[a0 + i];
+    for (uint32_t i = threadIdx.x; i < lb; i += MG_THREADS) s[padx<ITEMS>(la + i)] = b[b0 + i];
     __syncthreads();
-    const uint64_t *sa = s_in, *sb = s_in + la;
-    const uint32_t dg = threadIdx.x * MG_ITEMS < tot ? threadIdx.x * MG_ITEMS : tot;
-    uint32_t i = merge_path<uint32_t>(sa, la, sb, lb, dg), j = dg - i;
-    uint64_t v[MG_ITEMS];
+    const SView<ITEMS> sa{s, 0}, sb{s, la};
+    dg = threadIdx.x * ITEMS < tot ? threadIdx.x * ITEMS : tot;
+    uint32_t i = merge_path(sa, la, sb, lb, dg), j = dg - i;
 #pragma unroll
-    for (int k = 0; k < MG_ITEMS; ++k) {
+    for (int k = 0; k < ITEMS; ++k) {
         v[k] = 0;
         if (dg + k < tot) {
             const bool take_a = i < la && (j >= lb || sa[i] <= sb[j]);
@@ -287,16 +295,33 @@ __global__ void __launch_bounds__(MG_THREADS) k_merge_u64(const uint64_t *__rest
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < MG_ITEMS; ++k)
-        if (dg + k < tot) s_in[dg + k] = v[k];
+    for (int k = 0; k < ITEMS; ++k)
+        if (dg + k < tot) s[padx<ITEMS>(dg + k)] = v[k];
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < tot; x += MG_THREADS) out[d0 + x] = s_in[x];
+}
+
+/* One output tile per block, written back with coalesced stores. */
+__global__ void __launch_bounds__(MG_THREADS) k_merge_u64(const uint64_t *__restrict__ a, uint64_t na,
+                                                          const uint64_t *__restrict__ b, uint64_t nb,
+                                                          const uint64_t *__restrict__ split,
+                                                          uint64_t *__restrict__ out) {
+    __shared__ uint64_t s_in[MG_TILE + MG_TILE / MG_ITEMS];
+    const uint64_t n = na + nb;
+    const uint64_t d0 = (uint64_t)blockIdx.x * MG_TILE;
+    const uint64_t d1 = d0 + MG_TILE < n ? d0 + MG_TILE : n;
+    const uint64_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
+    const uint64_t b0 = d0 - a0, b1 = d1 - a1;
+    const uint32_t la = (uint32_t)(a1 - a0), lb = (uint32_t)(b1 - b0), tot = la + lb;
+    uint64_t v[MG_ITEMS];
+    uint32_t dg;
+    tile_merge<MG_ITEMS>(a, a0, la, b, b0, lb, s_in, v, dg);
+    for (uint32_t x = threadIdx.x; x < tot; x += MG_THREADS) out[d0 + x] = s_in[padx<MG_ITEMS>(x)];
 }
 
 /* ---- merge + unique + CSR in one pass ------------------------------------
  * The last merge of the sharder's sorted runs, the duplicate filter, the
  * compaction offsets and the CSR decode fused: each block merges one tile of
- * MG_TILE outputs (as k_merge_u64), flags the keys to keep, and finds where its
+ * MF_TILE outputs (as k_merge_u64), flags the keys to keep, and finds where its
  * kept keys start in the output by a decoupled look-back over the tiles before
  * it (tiles are taken in ticket order, so a block only waits on blocks that are
  * already running; every wait is bounded and sets an error flag on expiry).
@@ -361,35 +386,22 @@ __device__ __forceinline__ uint32_t look_back(const FinishArgs &f, uint32_t t, u
     return excl;
 }
 
-__global__ void __launch_bounds__(MG_THREADS) k_merge_finish(FinishArgs f) {
-    __shared__ uint64_t s_in[MG_TILE];
+__global__ void __launch_bounds__(MG_THREADS, 4) k_merge_finish(FinishArgs f) {
+    __shared__ uint64_t s_in[MF_TILE + MF_TILE / MF_ITEMS];
     __shared__ uint32_t s_warp[RS_WARPS];
     __shared__ uint32_t s_tile, s_excl, s_sum;
     if (threadIdx.x == 0) s_tile = atomicAdd(f.ticket, 1u);
     __syncthreads();
     const uint32_t t = s_tile;
     const uint64_t n = f.na + f.nb;
-    const uint64_t d0 = (uint64_t)t * MG_TILE;
-    const uint64_t d1 = d0 + MG_TILE < n ? d0 + MG_TILE : n;
+    const uint64_t d0 = (uint64_t)t * MF_TILE;
+    const uint64_t d1 = d0 + MF_TILE < n ? d0 + MF_TILE : n;
     const uint64_t a0 = f.split[t], a1 = f.split[t + 1];
     const uint64_t b0 = d0 - a0, b1 = d1 - a1;
     const uint32_t la = (uint32_t)(a1 - a0), lb = (uint32_t)(b1 - b0), tot = la + lb;
-    for (uint32_t i = threadIdx.x; i < la; i += MG_THREADS) s_in[i] = f.a[a0 + i];
-    for (uint32_t i = threadIdx.x; i < lb; i += MG_THREADS) s_in[la + i] = f.b[b0 + i];
-    __syncthreads();
-    const uint64_t *sa = s_in, *sb = s_in + la;
-    const uint32_t dg = threadIdx.x * MG_ITEMS < tot ? threadIdx.x * MG_ITEMS : tot;
-    uint32_t i = merge_path<uint32_t>(sa, la, sb, lb, dg), j = dg - i;
-    uint64_t v[MG_ITEMS];
-#pragma unroll
-    for (int k = 0; k < MG_ITEMS; ++k) {
-        v[k] = 0;
-        if (dg + k < tot) {
-            const bool take_a = i < la && (j >= lb || sa[i] <= sb[j]);
-            v[k] = take_a ? sa[i] : sb[j];
-            if (take_a) ++i; else ++j;
-        }
-    }
+    uint64_t v[MF_ITEMS];
+    uint32_t dg;
+    tile_merge<MF_ITEMS>(f.a, a0, la, f.b, b0, lb, s_in, v, dg);
     /* the key before this thread's first: the previous thread's last, or the
      * previous tile's last (the larger of the last a and b keys before it) */
     uint64_t prev = 0;
@@ -398,18 +410,14 @@ __global__ void __launch_bounds__(MG_THREADS) k_merge_finish(FinishArgs f) {
             const uint64_t x = a0 ? f.a[a0 - 1] : 0ull, y = b0 ? f.b[b0 - 1] : 0ull;
             prev = x > y ? x : y;
         }
+    } else if (dg > 0) {
+        prev = s_in[padx<MF_ITEMS>(dg - 1)];
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < MG_ITEMS; ++k)
-        if (dg + k < tot) s_in[dg + k] = v[k];
-    __syncthreads();
-    if (threadIdx.x > 0 && dg > 0) prev = s_in[dg - 1];
     uint32_t fl = 0, cnt = 0;
     {
         uint64_t pk = prev;
 #pragma unroll
-        for (int k = 0; k < MG_ITEMS; ++k) {
+        for (int k = 0; k < MF_ITEMS; ++k) {
             const uint64_t gi = d0 + dg + k;
             if (dg + k < tot && gi < f.kept) {
                 const bool keep = !f.dedup || gi == 0 || v[k] != pk;
@@ -438,29 +446,38 @@ __global__ void __launch_bounds__(MG_THREADS) k_merge_finish(FinishArgs f) {
     }
     __syncthreads();
     const uint64_t mask = (f.kbits >= 64) ? ~0ull : ((1ull << f.kbits) - 1ull);
-    uint32_t p = s_excl + local;
+    const uint32_t base = s_excl;
+    /* the kept keys, compacted in shared memory (the merged tile is no longer
+     * read), then written out with coalesced stores; row pointers and repeat
+     * counts from the thread that holds the key */
+    uint32_t q = local;
     uint64_t pk = prev;
 #pragma unroll
-    for (int k = 0; k < MG_ITEMS; ++k) {
+    for (int k = 0; k < MF_ITEMS; ++k) {
         const uint64_t gi = d0 + dg + k;
         if (dg + k < tot && gi < f.kept) {
             const uint64_t key = v[k];
             const uint32_t row = (uint32_t)(key >> f.kbits);
             if ((fl >> k) & 1u) {
-                f.col[p] = (uint32_t)(key & mask);
-                if (f.keys_out) f.keys_out[p] = key;
+                s_in[padx<MF_ITEMS>(q)] = key;
                 const int64_t prow = gi == 0 ? -1 : (int64_t)(pk >> f.kbits);
-                for (int64_t r = prow + 1; r <= (int64_t)row; ++r) f.rowptr[r] = p;
-                ++p;
+                for (int64_t r = prow + 1; r <= (int64_t)row; ++r) f.rowptr[r] = base + q;
+                ++q;
             } else if (f.outdeg_dup) {
                 atomicSub(f.outdeg_dup + (uint32_t)(key & mask), 1u);
             }
             if (gi == f.kept - 1) { /* rows after the last key end at the total */
-                for (uint64_t r = (uint64_t)row + 1; r <= f.nv; ++r) f.rowptr[r] = p;
-                *f.total = p;
+                for (uint64_t r = (uint64_t)row + 1; r <= f.nv; ++r) f.rowptr[r] = base + q;
+                *f.total = base + q;
             }
         }
         pk = v[k];
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < tile_sum; x += MG_THREADS) {
+        const uint64_t key = s_in[padx<MF_ITEMS>(x)];
+        f.col[base + x] = (uint32_t)(key & mask);
+        if (f.keys_out) f.keys_out[base + x] = key;
     }
 }
 
@@ -477,7 +494,7 @@ int merge_u64(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t nb, ui
     if (ntiles >= 0x7FFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "merge: too many keys");
     tbuf<uint64_t> split;
     GCG_TRY(split.alloc(ntiles + 1, s));
-    k_merge_split<<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
+    k_merge_split<MG_TILE><<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
         a, na, b, nb, ntiles, split.get());
     k_merge_u64<<<(unsigned)ntiles, MG_THREADS, 0, s>>>(a, na, b, nb, split.get(), out);
     GCG_LAUNCH_CHECK();
@@ -494,7 +511,7 @@ int merge_unique_csr(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t
     }
     const uint64_t n = na + nb;
     if (kept > n || kept > 0xFFFFFFFFull) return fail(GCG_ERR_INVALID, "merge_unique_csr: bad key count");
-    const uint64_t ntiles = (kept + MG_TILE - 1) / MG_TILE;
+    const uint64_t ntiles = (kept + MF_TILE - 1) / MF_TILE;
     tbuf<uint64_t> split;
     tbuf<unsigned long long> tstate;
     tbuf<uint32_t> ctl; /* ticket, total, err */
@@ -503,7 +520,7 @@ int merge_unique_csr(const uint64_t *a, uint64_t na, const uint64_t *b, uint64_t
     GCG_TRY(ctl.alloc(3, s));
     GCG_CUDA(cudaMemsetAsync(tstate.get(), 0, ntiles * sizeof(unsigned long long), s));
     GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 3 * sizeof(uint32_t), s));
-    k_merge_split<<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
+    k_merge_split<MF_TILE><<<(unsigned)std::min<uint64_t>((ntiles + 256) / 256, (uint64_t)num_sms() * 8), 256, 0, s>>>(
         a, na, b ? b : a, nb, ntiles, split.get());
     FinishArgs f;
     f.a = a;
