@@ -216,15 +216,34 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
     __shared__ int s_last;
     double dsum = 0.0, nsum = 0.0;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    for (uint32_t i = tid; i < a.nnz; i += nth) {
-        const float rn = a.source == GCG_NO_SOURCE ? pr_value(a, a.nzsum[i])
-                                                   : pr_value_at(a, a.nzsum[i], a.nz_rows[i]);
-        const float ro = a.r_nz_old[i];
-        const uint32_t od = a.od_nz[i];
-        a.r_nz_new[i] = rn;
-        a.c_new[a.nz_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
-        dsum += fabs((double)rn - (double)ro);
-        nsum += fabs((double)rn);
+    /* four rows (i, i + nth, i + 2 nth, i + 3 nth) per trip: their loads are all
+     * issued before the first store; the residual sums keep the row order */
+    constexpr int VB = 4;
+    for (uint32_t i0 = tid; i0 < a.nnz; i0 += VB * nth) {
+        float sum[VB], ro[VB];
+        uint32_t od[VB], cid[VB], row[VB];
+#pragma unroll
+        for (int u = 0; u < VB; ++u) {
+            const uint64_t i = (uint64_t)i0 + (uint64_t)u * nth;
+            if (i < a.nnz) {
+                sum[u] = a.nzsum[i];
+                ro[u] = a.r_nz_old[i];
+                od[u] = a.od_nz[i];
+                cid[u] = a.nz_cidx[i];
+                row[u] = a.source == GCG_NO_SOURCE ? 0u : a.nz_rows[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < VB; ++u) {
+            const uint64_t i = (uint64_t)i0 + (uint64_t)u * nth;
+            if (i < a.nnz) {
+                const float rn = a.source == GCG_NO_SOURCE ? pr_value(a, sum[u]) : pr_value_at(a, sum[u], row[u]);
+                a.r_nz_new[i] = rn;
+                a.c_new[cid[u]] = od[u] ? __fdiv_rn(rn, (float)od[u]) : 0.0f;
+                dsum += fabs((double)rn - (double)ro[u]);
+                nsum += fabs((double)rn);
+            }
+        }
     }
     if (const_pass) {
         /* vertices without in-edges: value teleport from the first sweep on;
