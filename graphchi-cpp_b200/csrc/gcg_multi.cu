@@ -213,7 +213,8 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
 
         /* ---- B: rows crossing chunk boundaries, summed exactly as the
          *         single-graph fix-up does (k_pr_fix): short rows by one lane in
-         *         chunk order, long rows by the warp (lane-strided, xor tree) ---- */
+         *         chunk order, long rows by the warp in the fixed group order of
+         *         long_row_sum_warp ---- */
         const uint32_t totB = active_prefix(m, 1, s_pref);
         for (uint32_t wb = gwarp * 32u; wb < totB; wb += nwarps * 32u) {
             const uint32_t x = wb + lane;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
                 const uint32_t g = find_graph(s_pref, m.ng, x);
                 sp = a.split[m.gr[g].ss + (x - s_pref[g])];
             }
-            const bool lng = valid && (sp.z - sp.y) > 8u;
+            const bool lng = valid && (sp.z - sp.y) > LONG_SPAN;
             if (valid && !lng) {
                 float s = __ldcg(a.tail_part + sp.y);
                 for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += __ldcg(a.head_part + c);
@@ -236,10 +237,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
                 const uint32_t row = __shfl_sync(FULL, sp.x, srcl);
                 const uint32_t cs = __shfl_sync(FULL, sp.y, srcl);
                 const uint32_t ce = __shfl_sync(FULL, sp.z, srcl);
-                float s = 0.0f;
-                for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) s += __ldcg(a.head_part + c);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+                const float s = long_row_sum_warp<true>(a.head_part, cs, ce, lane);
                 if (lane == 0) a.nzsum[row] = __ldcg(a.tail_part + cs) + s;
             }
         }

@@ -149,36 +149,40 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
  * each lane finishes its own row when it spans few chunks, and the warp sums the
  * partials of each long (hub) row cooperatively: lane-strided partial sums, then
  * a fixed xor-shuffle tree, so the order is fixed. */
+/* Blocks [0, nlong) take one long row each (a warp per group of the fixed
+ * long-row order); the other blocks take the short rows, one per lane, in
+ * chunk order. */
 __global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
     pdl_wait();
     pdl_launch_next();
     if (*(volatile const int *)a.done) return;
-    const uint32_t FULL = 0xFFFFFFFFu;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; wb < a.nsplit; wb += nwarps * 32u) {
-        const uint32_t k = wb + lane;
-        uint4 sp = make_uint4(0, 0, 0, 0);
-        if (k < a.nsplit) sp = a.split[k];
-        const bool valid = k < a.nsplit;
-        const bool lng = valid && (sp.z - sp.y) > 8u;
-        if (valid && !lng) {
-            float s = a.tail_part[sp.y];
-            for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += a.head_part[c];
-            a.nzsum[sp.x] = s;
-        }
-        uint32_t m = __ballot_sync(FULL, lng);
-        while (m) {
-            const int src = __ffs(m) - 1;
-            m &= m - 1;
-            const uint32_t row = __shfl_sync(FULL, sp.x, src);
-            const uint32_t cs = __shfl_sync(FULL, sp.y, src);
-            const uint32_t ce = __shfl_sync(FULL, sp.z, src);
-            float s = 0.0f;
-            for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) s += a.head_part[c];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    static_assert(LONG_GROUPS == 256 / 32, "one warp per group");
+    if (blockIdx.x < a.nlong) {
+        __shared__ float s_grp[LONG_GROUPS];
+        const uint4 sp = a.split[a.long_split[blockIdx.x]];
+        const float g = long_row_group<false>(a.head_part, sp.y, sp.z, (int)warp, lane);
+        if (lane == 0) s_grp[warp] = g;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.0f;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
-            if (lane == 0) a.nzsum[row] = a.tail_part[cs] + s;
+            for (int w = 0; w < LONG_GROUPS; ++w) t += s_grp[w];
+            a.nzsum[sp.x] = a.tail_part[sp.y] + t;
+        }
+        return;
+    }
+    const uint32_t nwarps = ((gridDim.x - a.nlong) * blockDim.x) >> 5;
+    for (uint32_t wb = (((blockIdx.x - a.nlong) * blockDim.x + threadIdx.x) >> 5) * 32u; wb < a.nsplit;
+         wb += nwarps * 32u) {
+        const uint32_t k = wb + lane;
+        if (k < a.nsplit) {
+            const uint4 sp = a.split[k];
+            if (sp.z - sp.y <= LONG_SPAN) {
+                float s = a.tail_part[sp.y];
+                for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += a.head_part[c];
+                a.nzsum[sp.x] = s;
+            }
         }
     }
 }
@@ -350,6 +354,14 @@ __global__ void k_gather_u32(uint32_t n, const uint32_t *__restrict__ idx, const
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
 }
 
+__global__ void k_long_list(const uint4 *__restrict__ split, uint32_t nsplit, uint32_t *count,
+                            uint32_t *__restrict__ list) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nsplit; i += gridDim.x * blockDim.x) {
+        const uint4 sp = split[i];
+        if (sp.z - sp.y > LONG_SPAN) list[atomicAdd(count, 1u)] = i;
+    }
+}
+
 inline unsigned grid1d(uint64_t n, uint64_t cap_per_sm = 16) {
     uint64_t b = (n + 255) / 256;
     uint64_t cap = (uint64_t)num_sms() * cap_per_sm;
@@ -419,6 +431,17 @@ int ensure_chunk_plan(gcg_graph *g) {
         p->nsplit = nsplit;
         if (p->split.alloc(std::max<uint32_t>(nsplit, 1))) return bail(GCG_ERR_NOMEM);
         k_split_list<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, ne, pos.get(), p->split.get());
+        /* the long split rows, each summed by a block of the fix-up (any order) */
+        if (nsplit) {
+            GCG_CUDA(cudaMemsetAsync(total.get(), 0, 4, s));
+            if (p->long_split.alloc(nsplit)) return bail(GCG_ERR_NOMEM);
+            k_long_list<<<grid1d(nsplit), 256, 0, s>>>(p->split.get(), nsplit, total.get(), p->long_split.get());
+            uint32_t nlong = 0;
+            if (cudaMemcpyAsync(&nlong, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
+            p->nlong = nlong;
+        }
     }
     /* relabel sources by out-degree so the hottest contribs sit at ids [0, hub) */
     {
@@ -555,6 +578,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     a.nz_rows = pl.nz_rows.get();
     a.zero_rows = pl.zero_rows.get();
     a.split = pl.split.get();
+    a.long_split = pl.long_split.get();
+    a.nlong = pl.nlong;
     a.ne = g->ne;
     a.nchunks = pl.nchunks;
     a.nnz = pl.nnz;
@@ -584,7 +609,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         GCG_CUDA(cudaMemcpy(&sdeg, g->indeg.get() + p->source, 4, cudaMemcpyDeviceToHost));
         a.norm_const = sdeg == 0 ? fabs((double)(float)p->teleport) : 0.0;
     }
-    const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 32);
+    const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 32) + (int)pl.nlong; /* + a block per long row */
 
     cudaEvent_t ev0, ev1;
     GCG_CUDA(cudaEventCreate(&ev0));

@@ -45,6 +45,8 @@ struct SweepArgs {
     const uint8_t *heads;
     const uint32_t *chunk_nz, *nz_rows, *zero_rows;
     const uint4 *split;
+    const uint32_t *long_split; /* indices into split of the rows spanning more than LONG_SPAN chunks */
+    uint32_t nlong;
     uint64_t ne;
     uint32_t nchunks, nnz, nzero, nsplit;
     uint32_t hub; /* contribs of relabelled sources [0, hub) are cached in shared memory */
@@ -242,11 +244,45 @@ struct PrWork {
     }
 };
 
+/* Rows that cross chunk boundaries: a row spanning at most LONG_SPAN chunks is
+ * summed by one thread in chunk order (tail part, then the head parts). A longer
+ * row is summed in one fixed order, the same whether a whole block computes it
+ * (the single-graph fix-up, one warp per group) or one warp does (the batch
+ * kernel): LONG_GROUPS groups of 32 lanes; lane l of group g adds the head parts
+ * of chunks cs+1+32g+l, cs+1+32g+l+256, ... in order; each group is reduced by
+ * an xor tree over its 32 lanes; the group sums are added in group order, and
+ * the tail part last. */
+constexpr uint32_t LONG_SPAN = 8;
+constexpr int LONG_GROUPS = 8;
+
+template <bool COHERENT>
+__device__ __forceinline__ float long_row_group(const float *head_part, uint32_t cs, uint32_t ce, int grp,
+                                                uint32_t lane) {
+    float s = 0.0f;
+    for (uint32_t c = cs + 1 + 32u * (uint32_t)grp + lane; c <= ce; c += 32u * LONG_GROUPS)
+        s += COHERENT ? __ldcg(head_part + c) : head_part[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    return s;
+}
+
+/* the whole long-row sum by one warp (every lane returns it) */
+template <bool COHERENT>
+__device__ __forceinline__ float long_row_sum_warp(const float *head_part, uint32_t cs, uint32_t ce,
+                                                   uint32_t lane) {
+    float t = 0.0f;
+#pragma unroll 1
+    for (int grp = 0; grp < LONG_GROUPS; ++grp) t += long_row_group<COHERENT>(head_part, cs, ce, grp, lane);
+    return t;
+}
+
 struct ChunkPlan {
     PrWork work;
     uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
     dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
     dbuf<uint4> split;
+    uint32_t nlong = 0;
+    dbuf<uint32_t> long_split; /* split rows spanning more than LONG_SPAN chunks */
     /* sources relabelled by out-degree (descending): col_r = newid[col] */
     uint32_t hub = 0;
     dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
