@@ -525,7 +525,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     const uint32_t hub_bytes = std::min(pl.hub, pl.tune_hub) * 4u;
     const uint64_t run = std::max(1u, pl.tune_run);
     const int ge = std::max(1, (int)std::min<uint64_t>((uint64_t)edge_grid(hub_bytes), (pl.nchunks + 32 * run - 1) / (32 * run)));
-    const int gv = (int)grid1d(std::max<uint64_t>(pl.nnz, pl.nzero), 32);
+    const int gv = (int)grid1d(std::max<uint64_t>(pl.nnz, pl.nzero), 16);
     /* the sweep workspace lives with the graph: allocated on the first call,
      * reused by later calls (no allocation on the repeated-solve path) */
     PrWork &w = g->cplan->work;
