@@ -223,7 +223,7 @@ unsigned grid_for(uint64_t n, int threads) {
 namespace {
 
 constexpr uint64_t PIPE_MIN_EDGES = 1ull << 24;
-constexpr int PIPE_CHUNKS = 8; /* a power of two: runs merge in equal pairs */
+constexpr int PIPE_CHUNKS = 16; /* a power of two: runs merge in equal pairs */
 
 uint32_t id_bits(uint32_t maxid) {
     uint32_t b = 1;
