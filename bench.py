@@ -173,6 +173,24 @@ def reference_time_to_tol(scale, ef, seed, tol, threads):
             "threads": threads}
 
 
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks: the slowest replica sets the job's time
+    (identity on one rank)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gteps(edges_per_rank, world, seconds):
+    """GTEPS of the whole job: every rank runs the same workload (replicas), so the
+    edges of all ranks over the slowest rank's time."""
+    return edges_per_rank * world / seconds / 1e9
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -400,14 +418,9 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
     sweeps = [s.sweeps for s in stats]
-    edges_done = sum(E * s for s in sweeps) * world
-    value = edges_done / (ms / 1e3) / 1e9
+    value = whole_job_gteps(sum(E * s for s in sweeps), world, ms / 1e3)
     launches = sum(s.kernel_launches for s in stats)
     kern_ms = sum(s.sweep_kernel_ms for s in stats)
     kern_n = sum(s.timed_sweeps for s in stats)
@@ -437,12 +450,8 @@ def run_ours(args, rank, world):
         if i >= args.e2e_warmup:
             e2e_times.append(dt)
             e2e_edges += E * st.sweeps
-    e2e_s = sum(e2e_times) if e2e_times else float("nan")
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = e2e_edges * world / e2e_s / 1e9 if e2e_times else None
+    e2e_s = max_over_ranks(sum(e2e_times) if e2e_times else float("nan"), world, "cuda")
+    e2e_value = whole_job_gteps(e2e_edges, world, e2e_s) if e2e_times else None
 
     # ---- CPU baseline: the reference's own PageRank on a bounded sample ----
     cpu = None
