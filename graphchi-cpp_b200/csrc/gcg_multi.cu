@@ -14,7 +14,7 @@
  *      (their concatenated chunk ranges; equal-sized chunks need no queue) and run
  *      the same pipelined gather / warp reduction as the single-graph kernel;
  *   B  rows crossing chunks: partials added in chunk order;
- *   C  vertices: CTAs pull 1024-row tiles of the active graphs from a device work
+ *   C  vertices: CTAs pull 4096-row tiles (4 rows per thread) of the active graphs from a device work
  *      queue (atomic counter), apply, and write one FP64 residual partial per tile
  *      (fixed slot);
  *   D  one warp per graph adds its tile partials in a fixed order; a graph whose
@@ -43,7 +43,8 @@
 namespace gcg {
 namespace {
 
-constexpr uint32_t VT = EDGE_THREADS; /* rows per vertex tile (one per thread) */
+constexpr uint32_t VROWS = 4;                 /* rows per thread in a vertex tile */
+constexpr uint32_t VT = EDGE_THREADS * VROWS; /* rows per vertex tile */
 constexpr uint32_t NG_MAX = 1024;     /* graphs per batch */
 
 /* per-graph ranges in the union */
@@ -272,27 +273,44 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
             uint32_t slot;
             if (t < ntn) {
                 slot = r.it_nz + t;
-                const uint32_t i = r.ns + t * VT + threadIdx.x;
-                if (i < r.ne) {
-                    const float rn = pr_value(a, __ldcg(a.nzsum + i));
-                    const float ro = __ldcg(a.r_nz_old + i);
-                    const uint32_t od = a.od_nz[i];
-                    a.r_nz_new[i] = rn;
-                    a.c_new[a.nz_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
-                    d = fabs((double)rn - (double)ro);
-                    n = fabs((double)rn);
+                /* VROWS rows per thread (coalesced per row step), all loads first */
+                const uint32_t i0 = r.ns + t * VT + threadIdx.x;
+                float sum[VROWS], ro[VROWS];
+                uint32_t od[VROWS], cid[VROWS];
+#pragma unroll
+                for (uint32_t u = 0; u < VROWS; ++u) {
+                    const uint32_t i = i0 + u * EDGE_THREADS;
+                    if (i < r.ne) {
+                        sum[u] = __ldcg(a.nzsum + i);
+                        ro[u] = __ldcg(a.r_nz_old + i);
+                        od[u] = a.od_nz[i];
+                        cid[u] = a.nz_cidx[i];
+                    }
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < VROWS; ++u) {
+                    const uint32_t i = i0 + u * EDGE_THREADS;
+                    if (i < r.ne) {
+                        const float rn = pr_value(a, sum[u]);
+                        a.r_nz_new[i] = rn;
+                        a.c_new[cid[u]] = od[u] ? __fdiv_rn(rn, (float)od[u]) : 0.0f;
+                        d += fabs((double)rn - (double)ro[u]);
+                        n += fabs((double)rn);
+                    }
                 }
             } else {
                 slot = r.it_z + (t - ntn);
-                const uint32_t i = r.zs + (t - ntn) * VT + threadIdx.x;
-                if (i < r.ze) {
-                    const uint32_t v = a.zero_rows[i];
-                    const float rn = pr_value(a, 0.0f);
-                    const float ro = sweep == 0 ? __ldcg(a.r_init + v) : rn;
-                    const uint32_t od = a.outdeg[v];
-                    a.c_new[a.zero_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
-                    d = fabs((double)rn - (double)ro);
-                    n = fabs((double)rn);
+                for (uint32_t u = 0; u < VROWS; ++u) {
+                    const uint32_t i = r.zs + (t - ntn) * VT + u * EDGE_THREADS + threadIdx.x;
+                    if (i < r.ze) {
+                        const uint32_t v = a.zero_rows[i];
+                        const float rn = pr_value(a, 0.0f);
+                        const float ro = sweep == 0 ? __ldcg(a.r_init + v) : rn;
+                        const uint32_t od = a.outdeg[v];
+                        a.c_new[a.zero_cidx[i]] = od ? __fdiv_rn(rn, (float)od) : 0.0f;
+                        d += fabs((double)rn - (double)ro);
+                        n += fabs((double)rn);
+                    }
                 }
             }
 #pragma unroll
