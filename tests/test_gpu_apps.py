@@ -78,3 +78,16 @@ def test_pagerank_functional_app_runs_the_kernel_on_the_device(edgelist, mode):
     ref, _, _ = go.pagerank_jacobi(teleport=0.15 / go.nv, damping=0.85, init=1.0, max_sweeps=9)
     ref = np.asarray(ref, np.float64)
     assert np.abs(got - ref).sum() / np.abs(ref).sum() <= 1e-6
+
+
+def test_bulksync_smoketest_app_pins_bulk_synchronous_visibility(edgelist):
+    # the reference's src/tests/bulksync_functional_test.cpp run by the device
+    # functional plug-in: every gather sees the previous iteration, every scatter
+    # the value just computed; three expectations per in-edge and iteration
+    path, go = edgelist
+    out = run("bulksync_smoketest", f"file={path}", "niters=5")
+    assert "Smoketest passed successfully" in out
+    checks = int([line for line in out.splitlines() if line.startswith("checks ")][0].split()[1])
+    assert checks == 3 * 4 * len(go.src)
+    got = O.read_vout(path, np.int32)
+    assert np.all(got[:go.nv] == 4)

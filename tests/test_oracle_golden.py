@@ -139,3 +139,19 @@ def test_planted_mistake_is_caught():
     g = O.OracleGraph(s, d)
     v, _, _ = g.pagerank_jacobi(teleport=0.15, max_sweeps=3, init=1.0)
     assert not np.array_equal(v, z["pr_gs_4_1_0"])
+
+
+@pytest.mark.parametrize("prog,niters", [("basic_smoketest", 4), ("bulksync_functional_test", 5)])
+def test_reference_known_answer_tests_pass(tmp_path, prog, niters):
+    # the reference's own pins, run from the oracle build: async id-order
+    # visibility of the vertex API (basic_smoketest.cpp:65) and bulk-synchronous
+    # visibility of the functional API (bulksync_functional_test.cpp:61-78); both
+    # assert inside the program, so passing means exit status 0 and its message
+    if not O.ref_available():
+        pytest.skip("oracle/_ref is not built")
+    s, d = O.rmat_numpy(10, 8 << 10, seed=52)
+    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
+    path = str(tmp_path / "g.el")
+    O.write_edgelist(path, cs, cd)
+    out, _ = O.run_ref(prog, path, {"niters": niters, "nshards": 2})
+    assert "Smoketest passed successfully" in out
