@@ -428,9 +428,14 @@ int build_graph(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, uint32
         GCG_CUDA(cudaStreamSynchronize(s));
     }
     if (info.bad) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: vertex id >= num_vertices");
-    uint32_t nv = nv_given ? nv_given : info.maxid + 1; /* sharder.hpp:925: 1 + max_vertex_id */
+    const uint64_t nv64 = nv_given ? (uint64_t)nv_given : (uint64_t)info.maxid + 1; /* sharder.hpp:925 */
+    if (nv64 > MAX_VERTICES)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_from_edges: " + std::to_string(nv64) +
+                                             " vertices; at most 2^32 - 2^26 (largest id 4227858431)");
+    const uint32_t nv = (uint32_t)nv64;
     const uint64_t kept = sym ? 2 * (uint64_t)info.kept : (uint64_t)info.kept;
-    if (kept > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "more than 2^32-1 edges after filtering");
+    if (kept > MAX_EDGES)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_from_edges: more than 2^32 - 2^26 edges after filtering");
     uint32_t vbits = 1;
     while (vbits < 32 && (1ull << vbits) < nv) ++vbits;
     if (!pipelined) kbits = vbits;
@@ -654,7 +659,7 @@ int add_edges(gcg_graph *g, const uint32_t *s_u, const uint32_t *d_u, uint64_t m
     }
     const int both = g->symmetric ? 1 : 0;
     const uint64_t total = g->ne + (both ? 2 * m : m);
-    if (total > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: more than 2^32-1 edges");
+    if (total > MAX_EDGES) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: more than 2^32 - 2^26 edges");
     GCG_TRY(src.alloc(std::max<uint64_t>(total, 1), s));
     GCG_TRY(dst.alloc(std::max<uint64_t>(total, 1), s));
     GCG_TRY(mx.alloc(1, s));
@@ -667,7 +672,7 @@ int add_edges(gcg_graph *g, const uint32_t *s_u, const uint32_t *d_u, uint64_t m
     GCG_CUDA(cudaMemcpyAsync(&maxid, mx.get(), 4, cudaMemcpyDeviceToHost, s));
     GCG_CUDA(cudaStreamSynchronize(s));
     const uint64_t nv = std::max<uint64_t>(g->nv, m ? (uint64_t)maxid + 1 : 0);
-    if (nv > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: vertex id 2^32-1 is reserved");
+    if (nv > MAX_VERTICES) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_add_edges: vertex ids at most 2^32 - 2^26 - 1");
     return rebuild_from(g, src.get(), dst.get(), total, (uint32_t)nv);
 }
 
@@ -743,6 +748,8 @@ int gcg_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, u
     *out = nullptr;
     if (m > 0 && (!src || !dst)) return fail(GCG_ERR_INVALID, "gcg_graph_from_edges: null edge arrays");
     if (m > 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_from_edges: more than 2^32-1 edges");
+    if (num_vertices > MAX_VERTICES)
+        return fail(GCG_ERR_UNSUPPORTED, "gcg_graph_from_edges: num_vertices above 2^32 - 2^26");
     return build_graph(src, dst, m, num_vertices, flags, nshards, out);
 }
 

@@ -36,6 +36,13 @@ int fail(int status, const std::string &msg);
 
 #define GCG_LAUNCH_CHECK() GCG_CUDA(cudaGetLastError())
 
+/* Largest vertex count and edge count (after filtering) of a graph, or of the union
+ * of a batch: 2^32 - 2^26. Kernels index vertices, rows, chunks and edges with
+ * 32-bit counters in grid-stride loops; no launch has more than 2^26 threads, so
+ * below this bound no counter can step past 2^32 and wrap around. */
+constexpr uint64_t MAX_VERTICES = (1ull << 32) - (1ull << 26);
+constexpr uint64_t MAX_EDGES = (1ull << 32) - (1ull << 26);
+
 /* ---- block cache (gcg_common.cu): freed device blocks and small pinned host
  *      blocks are kept per device and size class for the next allocation ---- */
 cudaError_t dev_alloc(void **p, size_t bytes);

@@ -529,8 +529,8 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
         R += graphs[g]->nv;
         E += graphs[g]->ne;
         gend[g] = (uint32_t)E;
-        if (V >= 0xFFFFFFFFull || E + CH >= 0xFFFFFFFFull)
-            return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_create: more than 2^32-1 vertices or edges in total");
+        if (V > MAX_VERTICES || E + CH > MAX_EDGES)
+            return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_create: more than 2^32 - 2^26 vertices or edges in total");
     }
     const uint64_t Etot = (E + CH - 1) / CH * CH;
     b->voff[ng] = (uint32_t)V;

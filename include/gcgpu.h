@@ -55,7 +55,9 @@ typedef struct gcg_graph gcg_graph;
  * intervals split exactly like the sharder's k-way merge sink
  * (sharder.hpp:861-892). num_vertices = 0 means max id + 1 (sharder.hpp:925);
  * otherwise every id must be < num_vertices. nshards = 0 means 1.
- * src/dst: m entries each, host or device. Limits: m < 2^32 after filtering. */
+ * src/dst: m entries each, host or device. Limits: m < 2^32; at most 2^32 - 2^26
+ * vertices (ids up to 4227858431) and 2^32 - 2^26 edges after filtering, else
+ * GCG_ERR_UNSUPPORTED. */
 int gcg_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m,
                          uint32_t num_vertices, uint32_t flags, uint32_t nshards,
                          gcg_graph **out);

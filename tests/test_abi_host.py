@@ -109,3 +109,12 @@ def test_block_cache_is_empty_without_allocations():
     # and releasing it is a no-op
     assert gcgpu.cached_memory() == (0, 0)
     assert gcgpu.release_cached_memory() == 0
+
+
+def test_vertex_count_beyond_the_limit_is_rejected_before_any_device_work():
+    # at most 2^32 - 2^26 vertices: 32-bit grid-stride counters cannot wrap
+    s = np.array([0, 1], np.uint32)
+    d = np.array([1, 2], np.uint32)
+    with pytest.raises(gcgpu.GcgError) as e:
+        gcgpu.Graph.from_edges(s, d, num_vertices=(1 << 32) - (1 << 26) + 1)
+    assert e.value.status == -6

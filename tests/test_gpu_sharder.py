@@ -212,3 +212,13 @@ def test_host_edges_in_pieces_reject_out_of_range_ids():
     with gcgpu.Graph.from_edges(s, d, num_vertices=(1 << 20) + 6, dedup=True, out_csr=False) as g:
         assert g.num_vertices == (1 << 20) + 6
         assert g.degrees()[(1 << 20) + 5, 0] == 1  # the planted edge's destination
+
+
+def test_largest_vertex_ids_are_rejected_not_wrapped():
+    # id 2^32 - 1 would make max id + 1 wrap to 0; ids up to 2^32 - 2^26 - 1 are the limit
+    for big in (0xFFFFFFFF, (1 << 32) - (1 << 26)):
+        s = np.array([0, big], np.uint32)
+        d = np.array([1, 2], np.uint32)
+        with pytest.raises(gcgpu.GcgError) as e:
+            gcgpu.Graph.from_edges(s, d)
+        assert e.value.status == -6, big
