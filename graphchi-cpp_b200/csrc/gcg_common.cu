@@ -54,8 +54,10 @@ int copy_out(void *dst_user, const void *src_dev, size_t bytes, cudaStream_t s) 
     return GCG_OK;
 }
 
+static bool g_pool_kept[64] = {false}; /* devices whose default pool keeps freed memory */
+
 void pool_keep_memory() {
-    static bool done[64] = {false};
+    bool *done = g_pool_kept;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
@@ -179,6 +181,25 @@ uint64_t drain(int dev_sel, bool host) {
     return bytes;
 }
 
+}  // namespace
+
+/* Out of device memory: the idle blocks of the current device go back to the
+ * driver and its default pool drops the memory it keeps for freed temporaries. */
+void reclaim_device_memory() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    drain(dev, false);
+    cudaMemPool_t pool;
+    if (cudaDeviceSynchronize() == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+}
+
+namespace {
+
 cudaError_t cached_alloc(void **p, size_t bytes, bool host) {
     *p = nullptr;
     int dev = HOST_DEV;
@@ -207,7 +228,10 @@ cudaError_t cached_alloc(void **p, size_t bytes, bool host) {
     cudaError_t e = host ? cudaMallocHost(p, cls) : cudaMalloc(p, cls);
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
-        drain(host ? NO_DEVS : dev, host);
+        if (host)
+            drain(NO_DEVS, true);
+        else
+            reclaim_device_memory();
         e = host ? cudaMallocHost(p, cls) : cudaMalloc(p, cls);
     }
     if (e != cudaSuccess) {
@@ -430,6 +454,19 @@ int gcg_cached_memory(uint64_t *idle_device_bytes, uint64_t *idle_host_bytes) {
 int gcg_release_cached_memory(uint64_t *released_bytes) {
     const uint64_t b = drain(ALL_DEVS, true);
     if (released_bytes) *released_bytes = b;
+    /* and the stream-ordered temporaries kept by the default pools */
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess) {
+        for (int d = 0; d < 64; ++d) {
+            if (!g_pool_kept[d]) continue;
+            cudaMemPool_t pool;
+            if (cudaSetDevice(d) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+                cudaDeviceGetDefaultMemPool(&pool, d) == cudaSuccess)
+                cudaMemPoolTrimTo(pool, 0);
+        }
+        cudaSetDevice(cur);
+    }
+    cudaGetLastError();
     return GCG_OK;
 }
 

@@ -49,6 +49,9 @@ cudaError_t dev_alloc(void **p, size_t bytes);
 void dev_free(void *p);
 cudaError_t host_alloc(void **p, size_t bytes);
 void host_free(void *p);
+/* after an out-of-memory error: releases the current device's idle cached blocks
+ * and the memory its default stream-ordered pool keeps */
+void reclaim_device_memory();
 
 /* ---- device buffers ----------------------------------------------------- */
 template <typename T>
@@ -101,6 +104,11 @@ struct tbuf {
         s = stream;
         if (count == 0) count = 1;
         cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), stream);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            reclaim_device_memory();
+            e = cudaMallocAsync((void **)&p, count * sizeof(T), stream);
+        }
         if (e != cudaSuccess) {
             p = nullptr;
             return fail(GCG_ERR_NOMEM, std::string("cudaMallocAsync of ") + std::to_string(count * sizeof(T)) +

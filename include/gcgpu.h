@@ -88,7 +88,9 @@ int gcg_graph_free(gcg_graph *g);
  * off; host: GCG_HOST_CACHE_MB, default 256) and is emptied, and the allocation
  * retried, when the driver runs out of memory.
  * gcg_cached_memory reports the idle bytes held; gcg_release_cached_memory
- * returns them all to the driver (released_bytes may be NULL). */
+ * returns them all to the driver (released_bytes, which may be NULL, receives
+ * their count) and also trims the memory that the devices' default stream-ordered
+ * pools keep for the library's temporaries (the sharder's sort buffers). */
 int gcg_cached_memory(uint64_t *idle_device_bytes, uint64_t *idle_host_bytes);
 int gcg_release_cached_memory(uint64_t *released_bytes);
 
