@@ -67,6 +67,7 @@ struct SweepArgs {
     uint32_t source; /* personalisation vertex, or GCG_NO_SOURCE */
     uint32_t run;    /* edge kernel: each warp takes runs of this many consecutive chunks (>= 1) */
     double *delta_log; /* optional: per sweep, sum |r' - r| (FP64) */
+    unsigned long long tex_old; /* texture object over c_old (edge kernel's texture-path gathers) */
 };
 
 /* columns (streamed), head flags and starting row index of one chunk; ne is
@@ -239,8 +240,13 @@ struct PrWork {
     dbuf<uint32_t> ctl;
     dbuf<double> dres;
     int *h_flags = nullptr; /* pinned: done flags copied back per chunk of sweeps */
+    /* texture objects over the two contribution buffers (0: not available, the
+     * edge kernel then gathers with plain loads) */
+    unsigned long long tex[2] = {0, 0};
     ~PrWork() {
         if (h_flags) host_free(h_flags);
+        for (unsigned long long t : tex)
+            if (t) cudaDestroyTextureObject((cudaTextureObject_t)t);
     }
 };
 
