@@ -54,7 +54,7 @@ def load_peaks():
 def load_traffic_per_edge():
     """DRAM bytes per edge of one k_pr_edges launch at scale 24, from the committed
     ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one launch / E)."""
-    path = os.path.join(ROOT, "profiles", "pagerank_edges_rmat24_traffic.md")
+    path = os.path.join(ROOT, "profiles", "pagerank_edges_rmat24_full.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_edge:"):
