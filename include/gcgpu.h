@@ -234,7 +234,7 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * plan's 49152), chunk_run = consecutive 256-edge chunks a warp takes at a time
  * (1 = warps stride chunk by chunk). Default: 41728 entries (the largest hub
  * that leaves the SM its 164 KB shared-memory carve-out, so L1 keeps ~92 KB) and
- * chunk_run 2, the fastest measured at R-MAT scale 24. gcg_pagerank_autotune
+ * chunk_run 1, the fastest measured at R-MAT scale 24. gcg_pagerank_autotune
  * times `sweeps` fixed sweeps of each candidate (hub entries {0, 16384, 32768,
  * 41728, 49152, the plan's} x runs {1, 2, 4, 16}), keeps the fastest for later
  * calls on this graph and reports it (outputs may be NULL). */
