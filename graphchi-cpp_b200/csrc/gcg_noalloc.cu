@@ -18,8 +18,10 @@
  * any stream capture. Every call shares the array and it keeps the last call's
  * contents: the control words are cleared at the start of each call, and two
  * calls that overlap on the GPU (different streams, or host threads) race.
+ * Every call waits for its stream before it returns (it reads the sweep count
+ * and, with a tolerance, the convergence flag on the host). The arrays must be
+ * device memory of the current device (or managed memory).
  */
-#include <chrono>
 #include <mutex>
 
 #include "gcg_internal.cuh"
@@ -36,7 +38,7 @@ constexpr size_t NA_C_OFF = 0;                                  /* float c[2][NA
 constexpr size_t NA_R_OFF = NA_C_OFF + 2ull * NA_MAXV * 4;       /* float r_spare[NA_MAXV] */
 constexpr size_t NA_PART_OFF = NA_R_OFF + (size_t)NA_MAXV * 4;   /* double2 part[NA_BLOCKS] */
 constexpr size_t NA_CTL_OFF = NA_PART_OFF + (size_t)NA_BLOCKS * 16; /* uint32 ticket, done, sweeps, pad */
-constexpr size_t NA_RES_OFF = NA_CTL_OFF + 256;                  /* double last residual */
+constexpr size_t NA_RES_OFF = NA_CTL_OFF + 256;                  /* double last residual, u64 t0, u64 t1 */
 constexpr size_t NA_BYTES = NA_RES_OFF + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
@@ -52,11 +54,21 @@ struct NaArgs {
     uint32_t *ticket;
     int *done, *sweeps;
     double *res;
+    double *res_log; /* caller's residuals[] or NULL: written by the sweeps that run */
+    unsigned long long *t_end;
     double teleport, damping, tol;
 };
 
+/* the GPU's global nanosecond timer */
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __global__ void k_na_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float init, const float *__restrict__ init_rank,
-                          float *__restrict__ r, float *__restrict__ c) {
+                          float *__restrict__ r, float *__restrict__ c, unsigned long long *t_start) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *t_start = globaltimer_ns();
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         const float x = init_rank ? init_rank[v] : init;
         r[v] = x;
@@ -112,7 +124,9 @@ __global__ void __launch_bounds__(NA_THREADS) k_na_sweep(NaArgs a, int sweep) {
     }
     const double res = y > 0.0 ? x / y : 0.0;
     *a.res = res;
+    if (a.res_log) a.res_log[sweep] = res;
     *a.sweeps = sweep + 1;
+    *a.t_end = globaltimer_ns();
     if (a.tol > 0.0 && res <= a.tol) *a.done = 1;
     *a.ticket = 0u;
 }
@@ -138,6 +152,18 @@ int scratch_address(unsigned char **out) {
     return GCG_OK;
 }
 
+/* device memory of device dev (or managed memory, reachable from every device) */
+bool on_device(const void *p, int dev) {
+    if (!p) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError(); /* clear: unregistered host pointer */
+        return false;
+    }
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
+}
+
 }  // namespace
 }  // namespace gcg
 
@@ -156,15 +182,17 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
     if (params->mode != GCG_PR_JACOBI || params->source != GCG_NO_SOURCE)
         return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank_csr_noalloc: only plain GCG_PR_JACOBI is available");
     if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_pagerank_csr_noalloc: max_sweeps < 0");
-    if (!is_device_ptr(in_rowptr) || !is_device_ptr(in_col) || !is_device_ptr(outdeg) || !is_device_ptr(out_rank) ||
-        (params->init_rank && !is_device_ptr(params->init_rank)) ||
-        (params->residuals && !is_device_ptr(params->residuals)))
+    int dev = 0;
+    GCG_CUDA(cudaGetDevice(&dev));
+    if (!on_device(in_rowptr, dev) || !on_device(in_col, dev) || !on_device(outdeg, dev) || !on_device(out_rank, dev) ||
+        (params->init_rank && !on_device(params->init_rank, dev)) ||
+        (params->residuals && !on_device(params->residuals, dev)))
         return fail(GCG_ERR_INVALID,
-                    "gcg_pagerank_csr_noalloc: every array must be device memory (this entry point allocates nothing)");
+                    "gcg_pagerank_csr_noalloc: every array must be device memory of the current device "
+                    "(this entry point allocates nothing)");
     unsigned char *base = nullptr;
     GCG_TRY(scratch_address(&base));
     cudaStream_t s = (cudaStream_t)stream;
-    const auto t0 = std::chrono::steady_clock::now();
 
     float *c = (float *)(base + NA_C_OFF);
     float *r_spare = (float *)(base + NA_R_OFF);
@@ -179,13 +207,16 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
     a.done = (int *)(ctl + 1);
     a.sweeps = (int *)(ctl + 2);
     a.res = (double *)(base + NA_RES_OFF);
+    a.res_log = params->residuals;
+    unsigned long long *t_dev = (unsigned long long *)(base + NA_RES_OFF + 8); /* start, end */
+    a.t_end = t_dev + 1;
     a.teleport = params->teleport;
     a.damping = params->damping;
     a.tol = params->tol;
     /* the array keeps the previous call's contents: clear the control words */
     GCG_CUDA(cudaMemsetAsync(base + NA_CTL_OFF, 0, 256 + 256, s));
     unsigned ib = (unsigned)std::min<uint64_t>(((uint64_t)num_vertices + 255) / 256, (uint64_t)num_sms() * 8);
-    k_na_init<<<ib, 256, 0, s>>>(num_vertices, outdeg, params->init, params->init_rank, out_rank, c);
+    k_na_init<<<ib, 256, 0, s>>>(num_vertices, outdeg, params->init, params->init_rank, out_rank, c, t_dev);
     GCG_LAUNCH_CHECK();
     /* ranks ping-pong between the caller's output and the spare buffer */
     float *rb[2] = {out_rank, r_spare};
@@ -201,8 +232,6 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
             a.r_old = rb[sw & 1];
             a.r_new = rb[(sw + 1) & 1];
             k_na_sweep<<<grid, NA_THREADS, 0, s>>>(a, sw);
-            if (params->residuals)
-                cudaMemcpyAsync(params->residuals + sw, a.res, sizeof(double), cudaMemcpyDeviceToDevice, s);
         }
         GCG_LAUNCH_CHECK();
         launched += n;
@@ -214,7 +243,9 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
     }
     GCG_CUDA(cudaMemcpyAsync(flags, ctl + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     double res = 0.0;
+    unsigned long long t_ns[2] = {0, 0};
     GCG_CUDA(cudaMemcpyAsync(&res, a.res, sizeof(double), cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaMemcpyAsync(t_ns, t_dev, sizeof(t_ns), cudaMemcpyDeviceToHost, s));
     GCG_CUDA(cudaStreamSynchronize(s));
     const int sweeps = flags[1];
     if (sweeps & 1) { /* the result sits in the spare buffer */
@@ -225,7 +256,8 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
         stats->sweeps = sweeps;
         stats->converged = flags[0];
         stats->residual = res;
-        stats->device_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        /* GPU global timer: start of the initial-vector kernel to the end of the last sweep that ran */
+        stats->device_ms = (sweeps > 0 && t_ns[1] > t_ns[0]) ? (double)(t_ns[1] - t_ns[0]) * 1e-6 : 0.0;
         stats->sweep_kernel_ms = 0.0;
         stats->timed_sweeps = 0;
         stats->kernel_launches = 1 + launched;

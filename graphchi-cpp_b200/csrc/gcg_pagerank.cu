@@ -331,10 +331,13 @@ __global__ void k_newid(const uint64_t *__restrict__ sorted, uint32_t nv, uint32
         newid[(uint32_t)(sorted[i] & mask)] = i;
 }
 
-__global__ void k_relabel(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
-                          uint32_t *__restrict__ col_r) {
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x)
-        col_r[e] = newid[col[e]];
+/* col_r = newid[col] in the chunk layout of load_chunk (chunk_slot), whole
+ * chunks: slots past the last edge hold 0 */
+__global__ void k_relabel(const uint32_t *__restrict__ col, uint64_t ne, uint64_t nslots,
+                          const uint32_t *__restrict__ newid, uint32_t *__restrict__ col_r) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nslots;
+         e += (uint64_t)gridDim.x * blockDim.x)
+        col_r[chunk_slot(e)] = e < ne ? newid[col[e]] : 0u;
 }
 
 __global__ void k_max_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t *out) {
@@ -463,7 +466,7 @@ int ensure_chunk_plan(gcg_graph *g) {
         tbuf<uint32_t> dmax;
         tbuf<uint64_t> keys, tmp;
         if (dmax.alloc(1, s) || keys.alloc(std::max<uint32_t>(nv, 1), s) || tmp.alloc(std::max<uint32_t>(nv, 1), s) ||
-            p->newid.alloc(std::max<uint32_t>(nv, 1)) || p->col_r.alloc(std::max<uint64_t>(ne, 1)) ||
+            p->newid.alloc(std::max<uint32_t>(nv, 1)) || p->col_r.alloc(std::max<uint64_t>((uint64_t)p->nchunks * CH, CH)) ||
             p->nz_cidx.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_cidx.alloc(std::max<uint32_t>(p->nzero, 1)))
             return bail(GCG_ERR_NOMEM);
         cudaMemsetAsync(dmax.get(), 0, 4, s);
@@ -479,7 +482,9 @@ int ensure_chunk_plan(gcg_graph *g) {
         if ((st = radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + dbits), &sorted, s)))
             return bail(st);
         k_newid<<<grid1d(nv), 256, 0, s>>>(sorted, nv, g->vbits, p->newid.get());
-        if (ne) k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, p->newid.get(), p->col_r.get());
+        if (ne)
+            k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, (uint64_t)p->nchunks * CH, p->newid.get(),
+                                                     p->col_r.get());
         if (nnz) k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), p->newid.get(), p->nz_cidx.get());
         if (p->nzero)
             k_gather_u32<<<grid1d(p->nzero), 256, 0, s>>>(p->nzero, p->zero_rows.get(), p->newid.get(),
@@ -866,7 +871,8 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
     if (params->source != GCG_NO_SOURCE && params->mode != GCG_PR_JACOBI)
         return fail(GCG_ERR_UNSUPPORTED, "gcg_pagerank: personalisation needs GCG_PR_JACOBI");
     if (params->mode == GCG_PR_JACOBI) return pagerank_jacobi(g, params, out_rank, stats);
-    if (params->mode == GCG_PR_GS_EXACT) return pagerank_gs_exact(g, params, out_rank, stats);
+    if (params->mode == GCG_PR_GS_EXACT || params->mode == GCG_PR_GS_EDGE)
+        return pagerank_gs_exact(g, params, out_rank, stats);
     if (params->mode == GCG_PR_DELTA) return pagerank_delta(g, params, out_rank, stats);
     return fail(GCG_ERR_INVALID, "gcg_pagerank: unknown mode");
 }

@@ -13,6 +13,12 @@
  * values above it. Levels come from a monotone relaxation over the in-CSR and a
  * radix sort of (level, id); the per-level launches of one sweep are captured
  * once in a CUDA graph and replayed per sweep.
+ *
+ * The same schedule runs the edge-value program of the app (PagerankProgram,
+ * example_apps/pagerank.cpp:73-113, taken when num_vertices * 4 >= membudget):
+ * there the value on every out-edge of u is u's pagerank / outdeg in float,
+ * initially (float)(1.0/outdeg), the vertex value is the pagerank itself, and
+ * each iteration logs the sum of |pagerank - old| (pagerank.cpp:108).
  */
 #include <algorithm>
 #include <vector>
@@ -74,11 +80,25 @@ __global__ void k_gs_init(uint32_t nv, const uint32_t *__restrict__ outdeg, floa
     }
 }
 
-/* pagerank.cpp:127-136 for the vertices of one level */
+/* pagerank.cpp:80-85 (edge-value program, iteration 0): out-edges hold
+ * (float)(1.0 / outdeg), the vertex 0.15 */
+__global__ void k_gs_edge_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float reset, float *c, float *val) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const uint32_t oc = outdeg[v];
+        c[v] = oc > 0 ? __double2float_rn(__ddiv_rn(1.0, (double)oc)) : 0.0f;
+        val[v] = reset;
+    }
+}
+
+/* One level of a sweep. In-memory program (EDGE = false), pagerank.cpp:127-136:
+ * pr = (float)((0.15 + 0.85 * (double)sum) / outc). Edge-value program (EDGE =
+ * true), pagerank.cpp:89-111: pagerank = (float)(0.15 + 0.85 * (double)sum), the
+ * out-edge value pagerank / outc in float, |pagerank - old| into delta[v]. */
+template <bool EDGE>
 __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, uint32_t end,
                            const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
                            const uint32_t *__restrict__ outdeg, const float *__restrict__ pr_old, float *pr_new,
-                           double reset, double damping) {
+                           float *val, float *delta, double reset, double damping) {
     for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const uint32_t v = order[i];
         float sum = 0.0f;
@@ -91,8 +111,49 @@ __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, u
          * the reference's separate double multiply and add */
         const int outc = (int)outdeg[v];
         const double t = __dadd_rn(reset, __dmul_rn(damping, (double)sum));
-        pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
+        if (EDGE) {
+            const float pagerank = __double2float_rn(t);
+            pr_new[v] = outc > 0 ? __fdiv_rn(pagerank, (float)outc) : 0.0f;
+            delta[v] = fabsf(__fsub_rn(pagerank, val[v]));
+            val[v] = pagerank;
+        } else {
+            pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
+        }
     }
+}
+
+/* The sweep's delta sum: each block adds a fixed slice in FP64, the last block
+ * to finish adds the block sums in block order into log[*slot] and advances
+ * *slot (the next sweep's entry). */
+constexpr int DSUM_BLOCKS = 256;
+__global__ void __launch_bounds__(256) k_gs_delta_sum(const float *__restrict__ delta, uint32_t nv, double *part,
+                                                      uint32_t *ticket, uint32_t *slot, double *log) {
+    __shared__ double s[8];
+    __shared__ int s_last;
+    const uint32_t per = (nv + gridDim.x - 1) / gridDim.x;
+    const uint32_t b0 = blockIdx.x * per, b1 = min(nv, b0 + per);
+    double x = 0.0;
+    for (uint32_t v = b0 + threadIdx.x; v < b1; v += blockDim.x) x += (double)delta[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += s[w];
+        part[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    double t = 0.0;
+    for (uint32_t b = 0; b < gridDim.x; ++b) t += __ldcg(part + b);
+    const uint32_t k = *slot;
+    log[k] = t;
+    *slot = k + 1;
+    *ticket = 0u;
 }
 
 /* pagerank.cpp:140-143: the stored value is pr * outc on the last iteration */
@@ -164,16 +225,31 @@ static int build_gs_plan(gcg_graph *g, GsPlan &pl) {
     return GCG_OK;
 }
 
+/* GCG_PR_GS_EXACT (in-memory program) and GCG_PR_GS_EDGE (edge-value program) */
 int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats) {
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
+    const bool edge = p->mode == GCG_PR_GS_EDGE;
     GsPlan pl;
     GCG_TRY(build_gs_plan(g, pl));
-    tbuf<float> pr;
+    const int nsw = p->max_sweeps;
+    tbuf<float> pr, val, delta;
+    tbuf<double> dlog, part;
+    tbuf<uint32_t> ctl; /* ticket, slot */
     GCG_TRY(pr.alloc((size_t)2 * nv, s));
     float *pr_old = pr.get(), *pr_new = pr.get() + nv;
     const float reset = (float)p->teleport;
-    k_gs_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old);
+    if (edge) {
+        GCG_TRY(val.alloc(nv, s));
+        GCG_TRY(delta.alloc(nv, s));
+        GCG_TRY(dlog.alloc(std::max(1, nsw), s));
+        GCG_TRY(part.alloc(DSUM_BLOCKS, s));
+        GCG_TRY(ctl.alloc(2, s));
+        GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 2 * sizeof(uint32_t), s));
+        k_gs_edge_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old, val.get());
+    } else {
+        k_gs_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old);
+    }
     GCG_LAUNCH_CHECK();
 
     cudaEvent_t ev0, ev1;
@@ -188,9 +264,17 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
     for (uint32_t l = 0; l < pl.nlev; ++l) {
         uint32_t b = pl.off[l], e = pl.off[l + 1];
         if (b == e) continue;
-        k_gs_level<<<vgrid(e - b), 256, 0, cap>>>(pl.order.get(), b, e, g->in_rowptr.get(), g->in_col.get(),
-                                                 g->outdeg.get(), pr_old, pr_new, p->teleport, p->damping);
+        if (edge)
+            k_gs_level<true><<<vgrid(e - b), 256, 0, cap>>>(pl.order.get(), b, e, g->in_rowptr.get(), g->in_col.get(),
+                                                           g->outdeg.get(), pr_old, pr_new, val.get(), delta.get(),
+                                                           p->teleport, p->damping);
+        else
+            k_gs_level<false><<<vgrid(e - b), 256, 0, cap>>>(pl.order.get(), b, e, g->in_rowptr.get(),
+                                                            g->in_col.get(), g->outdeg.get(), pr_old, pr_new,
+                                                            nullptr, nullptr, p->teleport, p->damping);
     }
+    if (edge)
+        k_gs_delta_sum<<<DSUM_BLOCKS, 256, 0, cap>>>(delta.get(), nv, part.get(), ctl.get(), ctl.get() + 1, dlog.get());
     cudaMemcpyAsync(pr_old, pr_new, (size_t)nv * 4, cudaMemcpyDeviceToDevice, cap);
     cudaError_t ce = cudaStreamEndCapture(cap, &graph);
     if (ce != cudaSuccess) {
@@ -204,10 +288,12 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
         return fail(GCG_ERR_CUDA, std::string("sweep graph instantiate: ") + cudaGetErrorString(ce));
     }
     GCG_CUDA(cudaEventRecord(ev0, s));
-    for (int sw = 0; sw < p->max_sweeps; ++sw) GCG_CUDA(cudaGraphLaunch(exec, s));
+    for (int sw = 0; sw < nsw; ++sw) GCG_CUDA(cudaGraphLaunch(exec, s));
     GCG_CUDA(cudaEventRecord(ev1, s));
-    k_gs_final<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), pr_old, pr_new);
-    GCG_LAUNCH_CHECK();
+    if (!edge) {
+        k_gs_final<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), pr_old, pr_new);
+        GCG_LAUNCH_CHECK();
+    }
     GCG_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
@@ -215,16 +301,25 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
     cudaEventDestroy(ev1);
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
-    if (out_rank) GCG_TRY(copy_out(out_rank, pr_new, (size_t)nv * 4, s));
+    if (out_rank) GCG_TRY(copy_out(out_rank, edge ? val.get() : pr_new, (size_t)nv * 4, s));
+    if (edge && p->delta_log && nsw > 0) GCG_TRY(copy_out(p->delta_log, dlog.get(), (size_t)nsw * sizeof(double), s));
+    if (edge && p->work_log && nsw > 0) { /* every vertex updated, its in- and out-edges touched, per sweep */
+        std::vector<uint64_t> wl(2 * (size_t)nsw);
+        for (int i = 0; i < nsw; ++i) {
+            wl[2 * i] = (uint64_t)nv * (uint64_t)(i + 1);
+            wl[2 * i + 1] = 2 * g->ne * (uint64_t)(i + 1);
+        }
+        GCG_TRY(copy_out(p->work_log, wl.data(), wl.size() * sizeof(uint64_t), s));
+    }
     GCG_CUDA(cudaStreamSynchronize(s));
     if (stats) {
-        stats->sweeps = p->max_sweeps;
+        stats->sweeps = nsw;
         stats->converged = 0;
         stats->residual = 0.0;
         stats->device_ms = ms;
         stats->sweep_kernel_ms = ms;
-        stats->timed_sweeps = p->max_sweeps;
-        stats->kernel_launches = 2 + (int)pl.nlev * p->max_sweeps;
+        stats->timed_sweeps = nsw;
+        stats->kernel_launches = (edge ? 1 : 2) + ((int)pl.nlev + (edge ? 1 : 0)) * nsw;
     }
     return GCG_OK;
 }

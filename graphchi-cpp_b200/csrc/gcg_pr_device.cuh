@@ -70,21 +70,33 @@ struct SweepArgs {
     unsigned long long tex_old; /* texture object over c_old (edge kernel's texture-path gathers) */
 };
 
+/* Column layout of a chunk. Lane l owns the 8 consecutive edges 8l..8l+7 of a
+ * 256-edge chunk, but they are stored split in two halves so that each of the
+ * lane's two 128-bit loads is part of one contiguous 512-byte warp access (16
+ * full sectors) instead of a 1 KiB access using half of each of 32 sectors:
+ * edge 8l+j (j < 4) sits at slot 4l+j, edge 8l+4+j at slot 128+4l+j. The array
+ * holds whole chunks (padding slots are 0). */
+__host__ __device__ __forceinline__ uint64_t chunk_slot(uint64_t e) {
+    const uint64_t l = (e >> 3) & 31u, j = e & 7u;
+    return (e & ~(uint64_t)(CH - 1)) + (j < 4 ? 4u * l + j : 128u + 4u * l + (j - 4u));
+}
+
 /* columns (streamed), head flags and starting row index of one chunk; ne is
  * the end of the edge range being swept (positions at or beyond it are masked) */
 template <typename A>
 __device__ __forceinline__ void load_chunk(const A &a, uint32_t ch, uint32_t lane, uint64_t pol, uint32_t (&col)[EPL],
                                            uint32_t &flags, uint32_t &nvalid, uint32_t &base, uint64_t ne) {
-    const uint64_t e = (uint64_t)ch * CH + (uint64_t)EPL * lane;
+    const uint64_t c0 = (uint64_t)ch * CH;
+    const uint64_t e = c0 + (uint64_t)EPL * lane;
     nvalid = e < ne ? (uint32_t)((ne - e) < EPL ? (ne - e) : EPL) : 0u;
-    if (nvalid == EPL) {
-        uint4 x = ld_stream_v4(a.col + e, pol);
-        uint4 y = ld_stream_v4(a.col + e + 4, pol);
-        col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
-        col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
-    } else {
+    const uint4 x = ld_stream_v4(a.col + c0 + 4u * lane, pol);
+    const uint4 y = ld_stream_v4(a.col + c0 + 128u + 4u * lane, pol);
+    col[0] = x.x; col[1] = x.y; col[2] = x.z; col[3] = x.w;
+    col[4] = y.x; col[5] = y.y; col[6] = y.z; col[7] = y.w;
+    if (nvalid < EPL) {
 #pragma unroll
-        for (int j = 0; j < EPL; ++j) col[j] = (uint32_t)j < nvalid ? a.col[e + j] : 0u;
+        for (int j = 0; j < EPL; ++j)
+            if ((uint32_t)j >= nvalid) col[j] = 0u;
     }
     flags = nvalid ? ((uint32_t)a.heads[e >> 3] & ((1u << nvalid) - 1u)) : 0u;
     base = a.chunk_nz[ch];

@@ -37,6 +37,7 @@ CSR_OUT = 1
 PR_JACOBI = 0
 PR_GS_EXACT = 1
 PR_DELTA = 2
+PR_GS_EDGE = 3
 PR_TIME_SWEEPS = 0x1
 
 # Every symbol include/gcgpu.h declares (checked by the CPU test suite).
@@ -448,15 +449,18 @@ def write_vout(base, values):
 
 
 def pagerank_csr_noalloc(in_rowptr, in_col, outdeg, out, num_vertices=None, max_sweeps=3, teleport=0.15,
-                         damping=0.85, tol=0.0, init=1.0, stream=0):
+                         damping=0.85, tol=0.0, init=1.0, stream=0, residuals=None):
     """gcg_pagerank_csr_noalloc: Jacobi PageRank over a CSR already in device
     memory (CUDA tensors), with no device allocation by the library.
-    Returns PrStats; the ranks are written into ``out``."""
+    Returns PrStats; the ranks are written into ``out`` and, when given, each
+    sweep's residual into the float64 device tensor ``residuals``."""
     n = int(out.shape[0]) if num_vertices is None else int(num_vertices)
     p = PrParams()
     _pr_default(C.byref(p))
     p.mode, p.max_sweeps, p.teleport, p.damping, p.tol, p.init = (PR_JACOBI, max_sweeps, teleport, damping, tol,
                                                                   init)
+    if residuals is not None:
+        p.residuals = ptr(residuals)
     st = PrStats()
     check(_pr_noalloc(ptr(in_rowptr), ptr(in_col), ptr(outdeg), n, C.byref(p), ptr(out), stream, C.byref(st)))
     return st

@@ -204,7 +204,8 @@ inline int convert_if_notexists_novalues(std::string base, std::string nshards) 
 
 /* ---- program, context ------------------------------------------------------ */
 enum class device_program {
-    pagerank_vertex_api,  /* example_apps/pagerank.cpp (Gauss-Seidel, bit-exact) */
+    pagerank_vertex_api,  /* example_apps/pagerank.cpp in-memory program (Gauss-Seidel, bit-exact) */
+    pagerank_edge_values, /* example_apps/pagerank.cpp edge-value program (Gauss-Seidel, bit-exact) */
     pagerank_functional,  /* example_apps/pagerank_functional.cpp, mode sync (Jacobi) */
     connected_components, /* example_apps/connectedcomponents.cpp */
     triangle_counting     /* example_apps/trianglecounting.cpp */
@@ -341,11 +342,13 @@ public:
         int last = niters - 1;
         switch (program.device_kind()) {
             case device_program::pagerank_vertex_api:
+            case device_program::pagerank_edge_values:
             case device_program::pagerank_functional: {
                 gcg_pr_params p;
                 gcg_pr_params_default(&p);
-                const bool vapi = program.device_kind() == device_program::pagerank_vertex_api;
-                p.mode = vapi ? GCG_PR_GS_EXACT : GCG_PR_JACOBI;
+                const bool edge = program.device_kind() == device_program::pagerank_edge_values;
+                const bool vapi = edge || program.device_kind() == device_program::pagerank_vertex_api;
+                p.mode = edge ? GCG_PR_GS_EDGE : vapi ? GCG_PR_GS_EXACT : GCG_PR_JACOBI;
                 p.max_sweeps = std::max(0, niters - 1);
                 p.teleport = vapi ? 0.15 : 0.15 / (double)nv;
                 p.tol = program.tolerance();
@@ -367,7 +370,18 @@ public:
                 for (uint32_t v = 0; v < nv; ++v) values[v] = (VertexDataType)r[v];
                 last = st.sweeps;
                 ctx_.last_residual = st.residual;
-                if (logged && st.sweeps > 0) {
+                if (p.mode == GCG_PR_GS_EDGE) {
+                    /* the engine logs iteration 0 (the initialisation: every vertex and
+                     * its in- and out-edges, no change) before the sweeps */
+                    dl.insert(dl.begin(), 0.0);
+                    wl.insert(wl.begin(), {(uint64_t)nv, 2 * (uint64_t)num_edges()});
+                    for (int i = 1; i <= st.sweeps; ++i) {
+                        wl[2 * i] += (uint64_t)nv;
+                        wl[2 * i + 1] += 2 * (uint64_t)num_edges();
+                    }
+                    write_delta_log(dl, wl, st.sweeps + 1);
+                    ctx_.last_deltasum = dl[st.sweeps];
+                } else if (logged && st.sweeps > 0) {
                     write_delta_log(dl, wl, st.sweeps);
                     ctx_.last_deltasum = dl[st.sweeps - 1];
                 }
@@ -442,29 +456,62 @@ inline std::vector<vertex_value<VT>> get_top_vertices(std::string base, int ntop
     return all;
 }
 
-/* vertex_aggregator.hpp:125 (sum over [fromv, tov)) */
+/* vertex_aggregator.hpp:68-127: the sum over [fromv, tov) read in windows of
+ * 2^20 vertices. As in the reference, a window holding a single vertex is
+ * skipped (its `if (st < en)` test, :84), so when (tov - fromv) % 2^20 == 1 the
+ * last vertex is not added. */
 template <typename VT, typename ST>
 inline ST sum_vertices(std::string base, vid_t fromv, vid_t tov) {
     auto v = read_vertex_values<VT>(base);
+    const vid_t window = 1024 * 1024;
     ST acc = 0;
-    for (vid_t i = fromv; i < tov && i < v.size(); ++i) acc += (ST)v[i];
+    for (uint64_t st = fromv; st <= (uint64_t)tov; st += window) {
+        uint64_t en = st + window - 1;
+        if (en >= (uint64_t)tov) en = (uint64_t)tov - 1;
+        if (!(st < en)) continue;
+        for (uint64_t i = st; i <= en && i < v.size(); ++i) acc += (ST)v[i];
+    }
     return acc;
 }
 
-/* labelanalysis.hpp:67: component sizes, written to <base>.components as "label,size" */
+/* labelanalysis.hpp:67-189: component sizes written to <base>.components as
+ * "label,size" lines. As in the reference: a vertex whose value is its own id
+ * (a component's representative) is not counted, every other vertex adds one
+ * to its label, a label's size is printed as count + 1, and labels are listed in
+ * decreasing count order as std::sort leaves them when started from ascending
+ * label order (so a component of one vertex does not appear). */
 template <typename VT>
 inline void analyze_labels(std::string base, int printtop = 20) {
     auto v = read_vertex_values<VT>(base);
-    std::map<VT, size_t> count;
-    for (size_t i = 0; i < v.size(); ++i) count[v[i]]++;
-    std::vector<std::pair<size_t, VT>> bysize;
-    for (auto &kv : count) bysize.push_back({kv.second, kv.first});
-    std::sort(bysize.begin(), bysize.end(), [](auto &a, auto &b) { return a.first > b.first; });
-    std::ofstream f(base + ".components");
-    for (auto &kv : count) f << kv.first << "," << kv.second << "\n";
-    std::cout << "Number of components: " << count.size() << std::endl;
-    for (int i = 0; i < printtop && i < (int)bysize.size(); ++i)
-        std::cout << (i + 1) << ". label: " << bysize[i].second << ", size: " << bysize[i].first << std::endl;
+    uint64_t nv = v.size();
+    {
+        std::ifstream nf(base + ".numvertices");
+        uint64_t x = 0;
+        if (nf >> x && x < nv) nv = x;
+    }
+    struct labelcount {
+        VT label;
+        uint64_t count;
+    };
+    std::vector<VT> lab;
+    lab.reserve(nv);
+    for (uint64_t i = 0; i < nv; ++i)
+        if (v[i] != (VT)i && v[i] != VT(0xffffffff)) lab.push_back(v[i]);
+    std::sort(lab.begin(), lab.end());
+    std::vector<labelcount> cur;
+    for (size_t i = 0; i < lab.size(); ++i) {
+        if (i > 0 && lab[i] == lab[i - 1]) cur.back().count++;
+        else cur.push_back({lab[i], 1});
+    }
+    std::sort(cur.begin(), cur.end(), [](const labelcount &a, const labelcount &b) { return a.count > b.count; });
+    const std::string outname = base + ".components";
+    std::ofstream f(outname);
+    if (!f) throw gcg_error(GCG_ERR_IO, "cannot write " + outname);
+    for (auto &c : cur) f << c.label << "," << c.count + 1 << "\n";
+    std::cout << "Total number of different labels (components/communities): " << cur.size() << std::endl;
+    std::cout << "List of labels was written to file: " << outname << std::endl;
+    for (int i = 0; i < printtop && i < (int)cur.size(); ++i)
+        std::cout << (i + 1) << ". label: " << cur[i].label << ", size: " << cur[i].count + 1 << std::endl;
 }
 
 }  // namespace graphchi

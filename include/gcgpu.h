@@ -165,7 +165,12 @@ int gcg_write_vout(const char *base, const void *values, uint32_t num_vertices, 
 /* ---- PageRank ---------------------------------------------------------- */
 
 #define GCG_PR_JACOBI 0   /* bulk-synchronous (functional engine, sync mode) */
-#define GCG_PR_GS_EXACT 1 /* vertex-API Gauss-Seidel in id order, bit-exact */
+#define GCG_PR_GS_EXACT 1 /* vertex-API in-memory program (pagerank.cpp:121-146): Gauss-Seidel
+                             in id order, bit-exact; the values are pr * outdeg as the app stores them */
+#define GCG_PR_GS_EDGE 3  /* vertex-API edge-value program (pagerank.cpp:73-113, the app's choice when
+                             num_vertices * 4 >= membudget): Gauss-Seidel in id order with
+                             pagerank / outdeg (float) on the out-edges, bit-exact; the values are
+                             the pageranks; delta_log gets each sweep's sum of |pagerank - old| */
 #define GCG_PR_DELTA 2    /* selective scheduling: Jacobi sweeps over a device frontier
                              (bitset_scheduler.hpp:38-104): sweep 0 updates every vertex; a vertex
                              whose rank moved by more than delta_threshold x its rank schedules its
@@ -173,7 +178,7 @@ int gcg_write_vout(const char *base, const void *values, uint32_t num_vertices, 
                              tol or at max_sweeps. Needs the out-edge CSR. */
 
 typedef struct {
-    int mode;               /* GCG_PR_JACOBI or GCG_PR_GS_EXACT */
+    int mode;               /* GCG_PR_JACOBI, GCG_PR_GS_EXACT, GCG_PR_DELTA or GCG_PR_GS_EDGE */
     int max_sweeps;         /* update sweeps after the initial one (niters - 1) */
     double teleport;        /* added term: 0.15 (pagerank.cpp:94) or 0.15/N (pagerank_functional.cpp:74) */
     double damping;         /* 0.85 */
@@ -188,8 +193,9 @@ typedef struct {
     /* optional per-sweep progress log, the reference's write_delta_log line
      * "iteration,nupdates,work,delta" (graphchi_engine.hpp:593-599): delta_log[i] = sum over
      * vertices of |r' - r| in sweep i (FP64; graphchi_context::log_change, graphchi_context.hpp:82-106);
-     * work_log[2i], [2i+1] = vertex updates and in-edges gathered up to and including sweep i.
-     * max_sweeps entries (2 x for work_log), host or device. JACOBI and DELTA modes. */
+     * work_log[2i], [2i+1] = vertex updates and in-edges gathered up to and including sweep i
+     * (GS_EDGE: in- plus out-edges, as the engine counts them for a program with edge values).
+     * max_sweeps entries (2 x for work_log), host or device. JACOBI, DELTA and GS_EDGE modes. */
     double *delta_log;
     uint64_t *work_log;
     /* GCG_PR_DELTA: a vertex whose rank moved by more than delta_threshold x its new rank
@@ -306,12 +312,17 @@ int gcg_batch_free(gcg_batch *b);
  * GPU, or a loop that must not incur cudaMalloc/cudaFree synchronisation). It
  * allocates nothing: in_rowptr (num_vertices+1), in_col, outdeg (num_vertices),
  * out_rank (num_vertices) and the optional params->init_rank / residuals must all
- * be device memory, or the call fails. Its scratch is a fixed static device
+ * be device memory of the current device (or managed memory), or the call fails
+ * with GCG_ERR_INVALID. Its scratch is a fixed static device
  * array sized for GCG_NOALLOC_MAX_VERTICES vertices (about 12.6 MB, held by every
  * GPU that loads the library); larger graphs are rejected with
  * GCG_ERR_UNSUPPORTED. The first call on a device looks up that array's address;
  * make it before any stream capture. All calls share the array: calls that
- * overlap on the GPU race. stream: a cudaStream_t (NULL = legacy default). */
+ * overlap on the GPU race. Each call waits for `stream` before it returns.
+ * residuals[i] is written for the sweeps that ran (i < stats->sweeps) only;
+ * stats->device_ms is read from the GPU's global timer (start of the first
+ * kernel to the end of the last sweep). stream: a cudaStream_t (NULL = legacy
+ * default). */
 #define GCG_NOALLOC_MAX_VERTICES (1u << 20)
 int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_t *in_col, const uint32_t *outdeg,
                              uint32_t num_vertices, const gcg_pr_params *params, float *out_rank,

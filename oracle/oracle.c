@@ -1,11 +1,13 @@
 /*
  * ORACLE — test infrastructure only (see oracle.h). Plain C restatement of the
  * GraphChi PSW hot path; each function cites the reference file:line it follows.
- * Single-threaded and written for clarity, not speed.
+ * Single-threaded and written for clarity, not speed, except the _mt variants at
+ * the end (OpenMP over rows or edges, same results) used for full-size checks.
  */
 #include "oracle.h"
 
 #include <math.h>
+#include <omp.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -381,4 +383,272 @@ int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
     free(frozen);
     free(r); free(c); free(acc); free(dsum); free(nsum);
     return sweeps;
+}
+
+/* ---- multithreaded variants for full-size checks ----------------------- */
+
+/* The seeded R-MAT generator of the library (csrc/gcg_rng.h), restated: edge i,
+ * level l draws u = hi32 (l even) or lo32 (l odd) of
+ * SplitMix64(key + (i*ceil(scale/2) + l/2 + 1) * golden), key =
+ * SplitMix64(seed ^ 0x6A09E667F3BCC909); u < floor(a 2^32) -> quadrant (0,0),
+ * < floor((a+b) 2^32) -> (0,1), < floor((a+b+c) 2^32) -> (1,0), else (1,1); the
+ * (src, dst) bits are appended most significant first. Edges are independent,
+ * so the threads split them freely. */
+static uint64_t orc_mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+void orc_rmat_edges(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed,
+                    uint32_t *src, uint32_t *dst) {
+    const double two32 = 4294967296.0;
+    const uint64_t ta = (uint64_t)(a * two32), tab = (uint64_t)((a + b) * two32),
+                   tabc = (uint64_t)((a + b + c) * two32);
+    const uint64_t key = orc_mix64(seed ^ 0x6A09E667F3BCC909ULL);
+    const uint64_t ndraw = (scale + 1) / 2;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < (int64_t)m; ++ii) {
+        const uint64_t i = (uint64_t)ii;
+        uint32_t s = 0, d = 0;
+        uint64_t w = 0;
+        for (uint32_t l = 0; l < scale; ++l) {
+            if ((l & 1u) == 0) w = orc_mix64(key + (i * ndraw + (l >> 1) + 1) * 0x9E3779B97F4A7C15ULL);
+            const uint64_t u = (l & 1u) ? (w & 0xFFFFFFFFULL) : (w >> 32);
+            const uint32_t q = (u >= ta) + (u >= tab) + (u >= tabc);
+            s = (s << 1) | (q >> 1);
+            d = (d << 1) | (q & 1u);
+        }
+        src[i] = s;
+        dst[i] = d;
+    }
+}
+
+#define ORC_BLK 65536u /* rows per residual block: the FP64 sums do not depend on the thread count */
+
+/* orc_pagerank_jacobi with the rows of a sweep split across OpenMP threads.
+ * Every row's float sum is the same ascending-source sum, so the ranks are
+ * bit-identical to the single-threaded function; the residual's two FP64 sums
+ * are formed per block of ORC_BLK rows and the blocks added in order. */
+int orc_pagerank_jacobi_mt(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                           const uint32_t *outdeg, double teleport, double damping, float init,
+                           int max_sweeps, double tol, float *out_rank, double *res_log) {
+    float *r = (float *)malloc((size_t)nv * sizeof(float));
+    float *c = (float *)malloc((size_t)nv * sizeof(float));
+    float *cn = (float *)malloc((size_t)nv * sizeof(float));
+    const uint32_t nb = (nv + ORC_BLK - 1) / ORC_BLK;
+    double *part = (double *)malloc(2 * (size_t)(nb ? nb : 1) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)nv; ++v) {
+        r[v] = init;
+        c[v] = outdeg[v] ? r[v] / (float)outdeg[v] : 0.0f;
+    }
+    int sweeps = 0;
+    for (int s = 0; s < max_sweeps; ++s) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t bk = 0; bk < (int64_t)nb; ++bk) {
+            double dsum = 0, nsum = 0;
+            const uint32_t v0 = (uint32_t)bk * ORC_BLK, v1 = v0 + ORC_BLK < nv ? v0 + ORC_BLK : nv;
+            for (uint32_t v = v0; v < v1; ++v) {
+                float sum = 0.0f;
+                for (uint32_t j = in_rowptr[v]; j < in_rowptr[v + 1]; ++j) sum += c[in_col[j]];
+                const float x = (float)(teleport + damping * (double)sum);
+                dsum += fabs((double)x - (double)r[v]);
+                nsum += fabs((double)x);
+                r[v] = x;
+                cn[v] = outdeg[v] ? x / (float)outdeg[v] : 0.0f;
+            }
+            part[2 * bk] = dsum;
+            part[2 * bk + 1] = nsum;
+        }
+        double dsum = 0, nsum = 0;
+        for (uint32_t bk = 0; bk < nb; ++bk) {
+            dsum += part[2 * bk];
+            nsum += part[2 * bk + 1];
+        }
+        float *t = c; c = cn; cn = t;
+        ++sweeps;
+        const double res = nsum > 0 ? dsum / nsum : 0.0;
+        if (res_log) res_log[s] = res;
+        if (tol > 0 && res <= tol) break;
+    }
+    memcpy(out_rank, r, (size_t)nv * sizeof(float));
+    free(r); free(c); free(cn); free(part);
+    return sweeps;
+}
+
+/* orc_pagerank_jacobi_f64 split across OpenMP threads (rows independent, the
+ * residual summed per block as above). init_vec (may be NULL) replaces the
+ * constant start. res_log (may be NULL) receives each sweep's residual. */
+int orc_pagerank_jacobi_f64_mt(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                               const uint32_t *outdeg, double teleport, double damping, double init,
+                               const double *init_vec, int max_sweeps, double tol, double *out_rank,
+                               double *res_log) {
+    double *r = (double *)malloc((size_t)nv * sizeof(double));
+    double *c = (double *)malloc((size_t)nv * sizeof(double));
+    double *cn = (double *)malloc((size_t)nv * sizeof(double));
+    const uint32_t nb = (nv + ORC_BLK - 1) / ORC_BLK;
+    double *part = (double *)malloc(2 * (size_t)(nb ? nb : 1) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)nv; ++v) {
+        r[v] = init_vec ? init_vec[v] : init;
+        c[v] = outdeg[v] ? r[v] / outdeg[v] : 0.0;
+    }
+    int sweeps = 0;
+    for (int s = 0; s < max_sweeps; ++s) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t bk = 0; bk < (int64_t)nb; ++bk) {
+            double dsum = 0, nsum = 0;
+            const uint32_t v0 = (uint32_t)bk * ORC_BLK, v1 = v0 + ORC_BLK < nv ? v0 + ORC_BLK : nv;
+            for (uint32_t v = v0; v < v1; ++v) {
+                double sum = 0.0;
+                for (uint32_t j = in_rowptr[v]; j < in_rowptr[v + 1]; ++j) sum += c[in_col[j]];
+                const double x = teleport + damping * sum;
+                dsum += fabs(x - r[v]);
+                nsum += fabs(x);
+                r[v] = x;
+                cn[v] = outdeg[v] ? x / outdeg[v] : 0.0;
+            }
+            part[2 * bk] = dsum;
+            part[2 * bk + 1] = nsum;
+        }
+        double dsum = 0, nsum = 0;
+        for (uint32_t bk = 0; bk < nb; ++bk) {
+            dsum += part[2 * bk];
+            nsum += part[2 * bk + 1];
+        }
+        double *t = c; c = cn; cn = t;
+        ++sweeps;
+        const double res = nsum > 0 ? dsum / nsum : 0.0;
+        if (res_log) res_log[s] = res;
+        if (tol > 0 && res <= tol) break;
+    }
+    memcpy(out_rank, r, (size_t)nv * sizeof(double));
+    free(r); free(c); free(cn); free(part);
+    return sweeps;
+}
+
+/* Stable LSD radix sort of the low `bits` bits of 64-bit keys, 16-bit digits,
+ * OpenMP: each thread counts its contiguous block, one thread turns the counts
+ * into digit-major / thread-minor offsets, each thread scatters its block.
+ * Returns the buffer holding the result (a or tmp). */
+static uint64_t *radix_sort_u64_mt(uint64_t *a, uint64_t *tmp, uint64_t n, int bits) {
+    const int maxt = omp_get_max_threads();
+    uint64_t *cnt = (uint64_t *)malloc((size_t)maxt * 65536 * sizeof(uint64_t));
+    uint64_t *src = a, *dst = tmp;
+    const int passes = (bits + 15) / 16;
+#pragma omp parallel
+    {
+        const int T = omp_get_num_threads(), t = omp_get_thread_num();
+        const uint64_t lo = n * (uint64_t)t / (uint64_t)T, hi = n * (uint64_t)(t + 1) / (uint64_t)T;
+        uint64_t *c = cnt + (size_t)t * 65536;
+        for (int pass = 0; pass < passes; ++pass) {
+            const int sh = 16 * pass;
+            memset(c, 0, 65536 * sizeof(uint64_t));
+            for (uint64_t i = lo; i < hi; ++i) c[(src[i] >> sh) & 0xFFFF]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                uint64_t run = 0;
+                for (int d = 0; d < 65536; ++d)
+                    for (int u = 0; u < T; ++u) {
+                        uint64_t *cu = cnt + (size_t)u * 65536 + d;
+                        const uint64_t x = *cu;
+                        *cu = run;
+                        run += x;
+                    }
+            }
+            for (uint64_t i = lo; i < hi; ++i) dst[c[(src[i] >> sh) & 0xFFFF]++] = src[i];
+#pragma omp barrier
+#pragma omp single
+            {
+                uint64_t *x = src;
+                src = dst;
+                dst = x;
+            }
+        }
+    }
+    free(cnt);
+    return src;
+}
+
+/* The in-CSR of the canonical edge set, for full-size checks: self-loops
+ * dropped (sharder.hpp:428-431), duplicates removed, rows by destination with
+ * sources ascending -- the same arrays as orc_canonical_edges(dedup) followed by
+ * orc_build_csr(by_dst=1), built with a multithreaded radix sort of
+ * (dst, src) keys. nv_cap bounds every id (rowptr holds nv_cap+1 entries, col m,
+ * outdeg nv_cap). Writes nv = max id + 1 (1 if no edge is left); returns E. */
+uint64_t orc_in_csr_mt(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t nv_cap,
+                       uint32_t *nv_out, uint32_t *rowptr, uint32_t *col, uint32_t *outdeg) {
+    int vb = 1;
+    while (vb < 32 && (1ull << vb) < (uint64_t)nv_cap) ++vb;
+    uint64_t *k = (uint64_t *)malloc((m ? m : 1) * sizeof(uint64_t));
+    uint64_t *tmp = (uint64_t *)malloc((m ? m : 1) * sizeof(uint64_t));
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < m; ++i) /* sequential: keeps it simple, memory-bound */
+        if (src[i] != dst[i]) k[n++] = ((uint64_t)dst[i] << vb) | src[i];
+    uint64_t *sorted = radix_sort_u64_mt(k, tmp, n, 2 * vb);
+    const uint64_t mask = (1ull << vb) - 1;
+    uint64_t E = 0;
+    uint32_t maxid = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (i > 0 && sorted[i] == sorted[i - 1]) continue;
+        sorted[E++] = sorted[i]; /* in place: E <= i */
+    }
+    memset(outdeg, 0, (size_t)nv_cap * sizeof(uint32_t));
+    for (uint32_t v = 0; v <= nv_cap; ++v) rowptr[v] = 0;
+    for (uint64_t i = 0; i < E; ++i) {
+        const uint32_t d = (uint32_t)(sorted[i] >> vb), s = (uint32_t)(sorted[i] & mask);
+        col[i] = s;
+        rowptr[d + 1]++;
+        outdeg[s]++;
+        if (d > maxid) maxid = d;
+        if (s > maxid) maxid = s;
+    }
+    for (uint32_t v = 0; v < nv_cap; ++v) rowptr[v + 1] += rowptr[v];
+    *nv_out = E ? maxid + 1 : 1;
+    free(k);
+    free(tmp);
+    return E;
+}
+
+/* Vertex-API PageRank, edge-value program (example_apps/pagerank.cpp:73-113;
+ * the app runs it when num_vertices * 4 >= membudget, :166-177) under the
+ * engine's deterministic id-ordered execution: sequential Gauss-Seidel in vertex
+ * id order where the state lives on the edges. Iteration 0 writes
+ * (float)(1.0 / outdeg) to every out-edge and 0.15 to the vertex (:80-85);
+ * iteration i >= 1 sums the in-edge values in ascending source order in float
+ * (:89-92), pagerank = (float)(0.15 + 0.85 * (double)sum) (:94), writes
+ * pagerank / outdeg (float division) to the out-edges (:98-104) and logs
+ * |pagerank - old value| (float) into the iteration's delta sum, added in
+ * double in vertex order (:108, src/api/graphchi_context.hpp:98-103). Every
+ * out-edge of a vertex holds the same value, so one value per source stands for
+ * them. out_values = vertex values after niters iterations; delta_log (may be
+ * NULL) gets niters entries (entry 0, the initialisation, is 0). */
+void orc_pagerank_gs_edge(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                          const uint32_t *outdeg, int niters, float *out_values, double *delta_log) {
+    const double RESET = 0.15; /* pagerank.cpp:43 RANDOMRESETPROB */
+    float *c = (float *)malloc((size_t)(nv ? nv : 1) * sizeof(float));
+    float *val = (float *)malloc((size_t)(nv ? nv : 1) * sizeof(float));
+    for (int it = 0; it < niters; ++it) {
+        double delta = 0.0;
+        for (uint32_t v = 0; v < nv; ++v) {
+            const uint32_t outc = outdeg[v];
+            if (it == 0) {
+                c[v] = outc ? (float)(1.0 / (double)outc) : 0.0f;
+                val[v] = (float)RESET;
+            } else {
+                float sum = 0.0f;
+                for (uint32_t j = in_rowptr[v]; j < in_rowptr[v + 1]; ++j) sum += c[in_col[j]];
+                const float pagerank = (float)(RESET + (1 - RESET) * (double)sum);
+                if (outc > 0) c[v] = pagerank / (float)outc;
+                delta += (double)fabsf(pagerank - val[v]);
+                val[v] = pagerank;
+            }
+        }
+        if (delta_log) delta_log[it] = delta;
+    }
+    memcpy(out_values, val, (size_t)nv * sizeof(float));
+    free(c);
+    free(val);
 }

@@ -53,6 +53,18 @@ uint32_t orc_auto_nshards(uint64_t nedges, uint32_t esize, uint32_t membudget_mb
 void orc_pagerank_gs_inmem(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
                            const uint32_t *outdeg, int niters, float *out_values);
 
+/* Vertex-API PageRank, edge-value program (example_apps/pagerank.cpp:73-113,
+ * chosen by the app when num_vertices * 4 >= membudget, :166-177) under the
+ * engine's id-ordered execution: sequential Gauss-Seidel where every out-edge of
+ * u holds u's pagerank / outdeg (float division), initially (float)(1.0/outdeg);
+ * the vertex value is pagerank = (float)(0.15 + 0.85*(double)sum). out_values:
+ * vertex values after niters iterations (iteration 0 = the initialisation);
+ * delta_log (may be NULL, niters entries): each iteration's sum of
+ * |pagerank - old| (float differences added in double in vertex order), the
+ * value graphchi_engine writes to <base>.deltalog. */
+void orc_pagerank_gs_edge(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                          const uint32_t *outdeg, int niters, float *out_values, double *delta_log);
+
 /* Bulk-synchronous PageRank with the functional kernel contract
  * (src/api/functional/functional_bulksync.hpp:91-113,
  * example_apps/pagerank_functional.cpp:51-81): init value `init`; each sweep
@@ -99,6 +111,33 @@ uint64_t orc_tc(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
 int orc_ppr(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
             const uint32_t *outdeg, const uint32_t *sources, uint32_t k, double damping,
             int max_sweeps, double tol, float *out);
+
+/* ---- multithreaded variants (OpenMP) for checks at full size ---- */
+
+/* The library's seeded R-MAT generator (csrc/gcg_rng.h) restated: m raw edges
+ * (self-loops and duplicates included), bit-identical to the library's. */
+void orc_rmat_edges(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed,
+                    uint32_t *src, uint32_t *dst);
+
+/* orc_pagerank_jacobi with rows split across threads: bit-identical ranks; the
+ * residual's FP64 sums are formed in fixed 65536-row blocks added in order. */
+int orc_pagerank_jacobi_mt(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                           const uint32_t *outdeg, double teleport, double damping, float init,
+                           int max_sweeps, double tol, float *out_rank, double *res_log);
+
+/* orc_pagerank_jacobi_f64 with rows split across threads; init_vec (NULL: the
+ * constant init) is the starting vector; res_log (may be NULL) the residuals. */
+int orc_pagerank_jacobi_f64_mt(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                               const uint32_t *outdeg, double teleport, double damping, double init,
+                               const double *init_vec, int max_sweeps, double tol, double *out_rank,
+                               double *res_log);
+
+/* The in-CSR (and out-degrees) of the canonical edge set -- the arrays of
+ * orc_canonical_edges(dedup) + orc_build_csr(by_dst=1) -- built with a
+ * multithreaded radix sort. Ids must be < nv_cap; rowptr holds nv_cap+1
+ * entries, col m, outdeg nv_cap. Writes nv (max id + 1); returns E. */
+uint64_t orc_in_csr_mt(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t nv_cap,
+                       uint32_t *nv_out, uint32_t *rowptr, uint32_t *col, uint32_t *outdeg);
 
 #ifdef __cplusplus
 }

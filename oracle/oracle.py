@@ -40,12 +40,17 @@ def lib():
             ("orc_intervals", _u32, [_vp, _u32, _u32, _vp]),
             ("orc_auto_nshards", _u32, [_u64, _u32, _u32]),
             ("orc_pagerank_gs_inmem", None, [_u32, _vp, _vp, _vp, _i, _vp]),
+            ("orc_pagerank_gs_edge", None, [_u32, _vp, _vp, _vp, _i, _vp, _vp]),
             ("orc_pagerank_jacobi", _i, [_u32, _vp, _vp, _vp, _d, _d, _f, _i, _d, _vp, _vp]),
             ("orc_pagerank_jacobi_f64", _i, [_u32, _vp, _vp, _vp, _d, _d, _d, _i, _d, _vp]),
             ("orc_cc", _i, [_u32, _vp, _vp, _vp, _vp, _vp]),
             ("orc_tc", _u64, [_u32, _vp, _vp, _vp, _vp, _vp, _vp]),
             ("orc_ppr", _i, [_u32, _vp, _vp, _vp, _vp, _u32, _d, _i, _d, _vp]),
             ("orc_write_edgelist", _i, [C.c_char_p, _vp, _vp, _u64]),
+            ("orc_rmat_edges", None, [_u32, _u64, _d, _d, _d, _u64, _vp, _vp]),
+            ("orc_in_csr_mt", _u64, [_vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp]),
+            ("orc_pagerank_jacobi_mt", _i, [_u32, _vp, _vp, _vp, _d, _d, _f, _i, _d, _vp, _vp]),
+            ("orc_pagerank_jacobi_f64_mt", _i, [_u32, _vp, _vp, _vp, _d, _d, _d, _vp, _i, _d, _vp, _vp]),
         ]:
             f = getattr(_lib, name)
             f.restype = res
@@ -91,18 +96,45 @@ def csr(nv, src, dst, by_dst):
 class OracleGraph:
     """Canonical graph + both CSRs, built by the oracle."""
 
-    def __init__(self, src, dst, symmetrise=False, dedup=True, nv=None):
+    @classmethod
+    def in_csr_only(cls, src, dst):
+        """The in-CSR and out-degrees of the canonical (deduplicated) directed
+        graph, built on all host threads: for full-size PageRank checks. The
+        canonical edge arrays and the out-CSR are not kept."""
+        src, dst = _u32(src), _u32(dst)
+        m = src.shape[0]
+        cap = int(max(src.max(initial=0), dst.max(initial=0))) + 1
+        g = cls.__new__(cls)
+        rp = np.zeros(cap + 1, np.uint32)
+        col = np.zeros(max(1, m), np.uint32)
+        od = np.zeros(cap, np.uint32)
+        nv = C.c_uint32(0)
+        e = lib().orc_in_csr_mt(_p(src), _p(dst), m, cap, C.addressof(nv), _p(rp), _p(col), _p(od))
+        g.nv = int(nv.value)
+        g.in_rowptr = rp[: g.nv + 1].copy()
+        g.in_col = col[:e]
+        g.outdeg = od[: g.nv].copy()
+        g.indeg = np.diff(g.in_rowptr).astype(np.uint32)
+        g.src = g.dst = g.out_rowptr = g.out_col = None
+        g._ne = int(e)
+        return g
+
+    def __init__(self, src, dst, symmetrise=False, dedup=True, nv=None, out_csr=True):
         s, d = canonical_edges(src, dst, symmetrise, dedup)
         self.src, self.dst = s, d
         self.nv = nv if nv is not None else num_vertices(s, d)
         self.in_rowptr, self.in_col = csr(self.nv, s, d, True)
-        self.out_rowptr, self.out_col = csr(self.nv, s, d, False)
         self.indeg = np.diff(self.in_rowptr).astype(np.uint32)
-        self.outdeg = np.diff(self.out_rowptr).astype(np.uint32)
+        if out_csr:
+            self.out_rowptr, self.out_col = csr(self.nv, s, d, False)
+            self.outdeg = np.diff(self.out_rowptr).astype(np.uint32)
+        else:  # full-size PageRank checks need only the in-CSR and out-degrees
+            self.out_rowptr = self.out_col = None
+            self.outdeg = np.bincount(s, minlength=self.nv).astype(np.uint32)
 
     @property
     def ne(self):
-        return int(self.src.shape[0])
+        return self._ne if self.src is None else int(self.src.shape[0])
 
     def intervals(self, nshards):
         out = np.zeros(max(1, nshards), np.uint32)
@@ -117,6 +149,14 @@ class OracleGraph:
         lib().orc_pagerank_gs_inmem(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg), niters, _p(out))
         return out
 
+    def pagerank_gs_edge(self, niters):
+        """Edge-value vertex program (pagerank.cpp:73-113): (values, delta per iteration)."""
+        out = np.zeros(self.nv, np.float32)
+        log = np.zeros(max(1, niters), np.float64)
+        lib().orc_pagerank_gs_edge(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg), niters, _p(out),
+                                   _p(log))
+        return out, log[:niters].copy()
+
     def pagerank_jacobi(self, teleport=0.15, damping=0.85, init=1.0, max_sweeps=3, tol=0.0):
         out = np.zeros(self.nv, np.float32)
         log = np.zeros(max(1, max_sweeps), np.float64)
@@ -129,6 +169,24 @@ class OracleGraph:
         n = lib().orc_pagerank_jacobi_f64(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg),
                                           teleport, damping, init, max_sweeps, tol, _p(out))
         return out, n
+
+    def pagerank_jacobi_mt(self, teleport=0.15, damping=0.85, init=1.0, max_sweeps=3, tol=0.0):
+        """pagerank_jacobi on all host threads (bit-identical ranks)."""
+        out = np.zeros(self.nv, np.float32)
+        log = np.zeros(max(1, max_sweeps), np.float64)
+        n = lib().orc_pagerank_jacobi_mt(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg),
+                                         teleport, damping, init, max_sweeps, tol, _p(out), _p(log))
+        return out, n, log[:n].copy()
+
+    def pagerank_jacobi_f64_mt(self, teleport=0.15, damping=0.85, init=1.0, max_sweeps=3, tol=0.0,
+                               init_vec=None):
+        """pagerank_jacobi_f64 on all host threads; returns (ranks, sweeps, residual log)."""
+        out = np.zeros(self.nv, np.float64)
+        log = np.zeros(max(1, max_sweeps), np.float64)
+        iv = None if init_vec is None else np.ascontiguousarray(init_vec, np.float64)
+        n = lib().orc_pagerank_jacobi_f64_mt(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg),
+                                             teleport, damping, init, _p(iv), max_sweeps, tol, _p(out), _p(log))
+        return out, n, log[:n].copy()
 
     def cc(self):
         out = np.zeros(self.nv, np.uint32)
@@ -196,6 +254,15 @@ def rmat_numpy(scale, m, a=0.57, b=0.19, c=0.19, seed=1):
     return s.astype(np.uint32), d.astype(np.uint32)
 
 
+def rmat_edges(scale, m, a=0.57, b=0.19, c=0.19, seed=1):
+    """The same generator as rmat_numpy, restated in C (oracle.c) on all host
+    threads: for full-size inputs."""
+    s = np.empty(m, np.uint32)
+    d = np.empty(m, np.uint32)
+    lib().orc_rmat_edges(scale, m, a, b, c, seed, _p(s), _p(d))
+    return s, d
+
+
 def er_numpy(n, m, seed=1):
     key = seed_key(seed)
     i = np.arange(m, dtype=np.uint64)
@@ -209,7 +276,7 @@ def er_numpy(n, m, seed=1):
 # ---- the reference's own apps --------------------------------------------
 
 REF_APPS = ["pagerank", "pagerank_functional", "connectedcomponents", "trianglecounting",
-            "basic_smoketest", "bulksync_functional_test", "pr_functional_oracle"]
+            "basic_smoketest", "bulksync_functional_test", "pr_functional_oracle", "aggregate_probe"]
 
 
 def ref_available():
@@ -242,6 +309,18 @@ def run_ref(app, edgelist, opts=None, threads=None, timeout=3600):
     if r.returncode != 0:
         raise RuntimeError(f"{app} failed ({r.returncode}): {r.stderr[-2000:]}{r.stdout[-2000:]}")
     return r.stdout + r.stderr, dt
+
+
+def run_probe(*args, timeout=600):
+    """Runs oracle/_ref/aggregate_probe (the reference's sum_vertices /
+    analyze_labels on a vertex-value file). Returns (stdout, wall seconds)."""
+    cmd = [os.path.join(REF_DIR, "aggregate_probe")] + [str(a) for a in args]
+    env = dict(os.environ, GRAPHCHI_ROOT=REF_DIR)
+    t0 = time.perf_counter()
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"aggregate_probe failed ({r.returncode}): {r.stderr[-2000:]}{r.stdout[-2000:]}")
+    return r.stdout + r.stderr, time.perf_counter() - t0
 
 
 def ref_runtime(output):

@@ -18,6 +18,7 @@ from __future__ import annotations
 import hashlib
 import json
 import os
+import re
 import sys
 
 import numpy as np
@@ -52,12 +53,20 @@ def canonical(spec, s, d):
     return O.canonical_edges(s, d, symmetrise=spec.get("sym", False), dedup=True)
 
 
-def run_case(name, spec, tasks, store_full):
+def run_case(name, spec, tasks, store_full, merge=False):
+    """merge: keep the fields already stored for this case and (re)compute only
+    the given tasks."""
     print(f"== {name}", flush=True)
     raw_s, raw_d = make_input(spec)
     s, d = canonical(spec, raw_s, raw_d)
     nv = O.num_vertices(s, d)
     rec = {"spec": json.dumps(spec), "ne": len(s), "nv": nv}
+    path = os.path.join(OUT, f"{name}.npz")
+    if merge and os.path.exists(path):
+        old = dict(np.load(path, allow_pickle=False))
+        assert str(old["spec"]) == rec["spec"] and int(old["ne"]) == rec["ne"], "case input changed"
+        old.update(rec)
+        rec = old
     def put(k, a):
         # tolerance-compared PageRank vectors are always stored in full
         if store_full or k.startswith(("pr_func", "pr_oracle")):
@@ -94,6 +103,18 @@ def run_case(name, spec, tasks, store_full):
                     opts["membudget_mb"] = budget
                 O.run_ref("pagerank", el, opts, THREADS)
                 put(f"pr_gs_{niters}_{P}_{budget}", O.read_vout(el, np.float32, nv))
+        if "pr_edge" in tasks:
+            # the edge-value program (pagerank.cpp:73-113): the app takes it when
+            # num_vertices * 4 >= membudget; one exec thread keeps the delta sums in
+            # vertex order, and shards of <= 1M edges keep each in-edge list in source
+            # order (memoryshard.hpp:400-401 decodes larger shards in parallel chunks)
+            for niters, P, budget in tasks["pr_edge"]:
+                el = fresh(f"pre{niters}_{P}_{budget}")
+                out, _ = O.run_ref("pagerank", el, {"niters": niters, "nshards": P, "membudget_mb": budget}, 1)
+                assert "in-memory mode" not in out, "the reference took the in-memory program"
+                tag = f"pr_edge_{niters}_{P}_{budget}"
+                put(tag, O.read_vout(el, np.float32, nv))
+                rec[tag + "_deltalog"] = np.frombuffer(open(el + ".deltalog", "rb").read(), np.uint8)
         if "pr_func" in tasks:
             for niters in tasks["pr_func"]:
                 el = fresh(f"prf{niters}")
@@ -116,6 +137,8 @@ def run_case(name, spec, tasks, store_full):
             lab = O.read_vout(el, np.uint32, nv)
             put("cc", lab)
             rec["cc_ncomp"] = int((lab == np.arange(nv, dtype=np.uint32)).sum())
+            # analyze_labels' file, written by the app itself (labelanalysis.hpp:99-176)
+            put("cc_components", np.frombuffer(open(el + ".components", "rb").read(), np.uint8))
         if "tc" in tasks:
             P = tasks["tc"]
             el = fresh("tc")
@@ -124,7 +147,38 @@ def run_case(name, spec, tasks, store_full):
             rec["tc_total"] = int(line.split(":")[1].split("(")[0])
             put("tc_per_rank", O.read_vout(el + "_degord", np.uint32, nv))
             put("tc_vertexmap", np.fromfile(el + ".vertexmap", dtype=np.uint32)[:nv])
-    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **{k: np.asarray(v) for k, v in rec.items()})
+    np.savez_compressed(path, **{k: np.asarray(v) for k, v in rec.items()})
+
+
+AGG_N = (1 << 20) + 16
+AGG_RANGES = [(0, (1 << 20) + 1), (0, (1 << 20) + 2), (0, AGG_N), (7, (1 << 20) + 8), (5, 6), (0, 1),
+              (0, 1000), (3, (1 << 20) + 3)]
+
+
+def aggregate_values():
+    """Seeded uint32 vertex values for the sum_vertices case (small values, so the
+    sums stay exact in any order)."""
+    return np.random.default_rng(11).integers(0, 1000, AGG_N).astype(np.uint32)
+
+
+def run_aggregates():
+    """sum_vertices (vertex_aggregator.hpp:68-127) over ranges whose last 2^20
+    window holds one vertex, computed by the reference's own reader through
+    oracle/_ref/aggregate_probe."""
+    print("== aggregates", flush=True)
+    vals = aggregate_values()
+    sums = []
+    with O.RefWorkdir() as w:
+        base = w.file("agg")
+        vals.tofile(base + ".4B.vout")
+        with open(base + ".numvertices", "w") as f:
+            f.write(f"{AGG_N}\n")
+        for a, b in AGG_RANGES:
+            out, _ = O.run_probe("sum", base, a, b)
+            sums.append(int(re.findall(r"sum (\d+)", out)[-1]))
+    np.savez_compressed(os.path.join(OUT, "aggregates.npz"), n=AGG_N, seed=11,
+                        ranges=np.array(AGG_RANGES, np.uint64), sums=np.array(sums, np.uint64),
+                        values_sha=sha(vals))
 
 
 CASES = [
@@ -145,16 +199,39 @@ CASES = [
      {"shard": [1, 8], "pr_gs": [(4, 1, 0)], "pr_func": [4], "pr_oracle": [(4, 0.0)]}, False),
     ("rmat_s16_ef16_sym_seed1", {"kind": "rmat", "scale": 16, "ef": 16, "seed": 1, "sym": True},
      {"cc": True, "tc": 2}, False),
+    # the edge-value PageRank program (taken when num_vertices * 4 >= membudget):
+    # 1 MB budget, more than 2^18 vertices
+    ("er_n300000_m2400000_seed7", {"kind": "er", "n": 300000, "m": 2400000, "seed": 7},
+     {"pr_edge": [(5, 4, 1), (2, 4, 1)]}, False),
+    ("rmat_s19_ef16_seed3", {"kind": "rmat", "scale": 19, "ef": 16, "seed": 3},
+     {"pr_edge": [(4, 12, 1)]}, False),
+    # config 3's PageRank program at scale 20: the in-memory vertex program, 4
+    # iterations, 20 shards of <= 1M edges
+    ("rmat_s20_ef16_seed1", {"kind": "rmat", "scale": 20, "ef": 16, "seed": 1},
+     {"pr_gs": [(4, 20, 0)]}, False),
     # config 2: CC and TC at scale 20, symmetrised (digests only)
     ("rmat_s20_ef16_sym_seed2", {"kind": "rmat", "scale": 20, "ef": 16, "seed": 2, "sym": True},
      {"cc": True, "tc": 4}, False),
 ]
 
 if __name__ == "__main__":
+    # python make_golden.py [case ...]            (re)makes the named cases (all by default)
+    # python make_golden.py --tasks cc,x case...  recomputes only those tasks, keeping the rest
     if not O.ref_available():
         sys.exit("oracle/_ref is not built: run `make -C oracle lib ref` where the reference tree is present")
-    only = set(sys.argv[1:])
+    argv = sys.argv[1:]
+    only_tasks = None
+    if argv[:1] == ["--tasks"]:
+        only_tasks = set(argv[1].split(","))
+        argv = argv[2:]
+    only = set(argv)
     for name, spec, tasks, full in CASES:
         if only and name not in only:
             continue
-        run_case(name, spec, tasks, full)
+        if only_tasks is not None:
+            tasks = {k: v for k, v in tasks.items() if k in only_tasks}
+            if not tasks:
+                continue
+        run_case(name, spec, tasks, full, merge=only_tasks is not None)
+    if not only or "aggregates" in only:
+        run_aggregates()

@@ -91,3 +91,46 @@ def test_bulksync_smoketest_app_pins_bulk_synchronous_visibility(edgelist):
     assert checks == 3 * 4 * len(go.src)
     got = O.read_vout(path, np.int32)
     assert np.all(got[:go.nv] == 4)
+
+
+@pytest.mark.parametrize("case", ["handmade_components", "rmat_s12_ef8_sym_seed2"])
+def test_connectedcomponents_app_components_file_matches_reference(tmp_path, case):
+    # the whole drop-in path (edge list -> device CC -> .vout -> analyze_labels)
+    # against the .components file the reference's own app wrote for the same input
+    import json
+    g = np.load(os.path.join(ROOT, "tests", "golden", f"{case}.npz"))
+    spec = json.loads(str(g["spec"]))
+    if spec["kind"] == "explicit":
+        s, d = np.array(spec["src"], np.uint32), np.array(spec["dst"], np.uint32)
+    else:
+        s, d = O.rmat_numpy(spec["scale"], spec["ef"] << spec["scale"], seed=spec["seed"])
+    cs, cd = O.canonical_edges(s, d, symmetrise=spec.get("sym", False), dedup=True)
+    path = str(tmp_path / "g.el")
+    O.write_edgelist(path, cs, cd)
+    out = run("connectedcomponents", f"file={path}")
+    assert np.array_equal(O.read_vout(path, np.uint32)[: int(g["nv"])], g["cc"])
+    assert open(path + ".components", "rb").read() == bytes(g["cc_components"])
+    assert "Total number of different labels" in out
+
+
+def test_pagerank_app_edge_program_matches_reference_files(tmp_path):
+    # with num_vertices * 4 >= membudget the app runs the edge-value program
+    # (pagerank.cpp:166-177), as the reference app did on this input: the .vout bit
+    # for bit and the .deltalog as the engine wrote it (counts exact, each delta
+    # to its printed 6 decimals)
+    import hashlib
+    import json
+    g = np.load(os.path.join(ROOT, "tests", "golden", "er_n300000_m2400000_seed7.npz"))
+    spec = json.loads(str(g["spec"]))
+    s, d = O.er_numpy(spec["n"], spec["m"], spec["seed"])
+    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
+    path = str(tmp_path / "g.el")
+    O.write_edgelist(path, cs, cd)
+    out = run("pagerank", f"file={path}", "niters=5", "nshards=4", "membudget_mb=1")
+    assert "in-memory mode" not in out
+    vals = O.read_vout(path, np.float32)[: int(g["nv"])]
+    assert hashlib.sha256(vals.tobytes()).hexdigest() == str(g["pr_edge_5_4_1_sha"])
+    got = [ln.split(",") for ln in open(path + ".deltalog").read().split()]
+    ref = [ln.split(",") for ln in bytes(g["pr_edge_5_4_1_deltalog"]).decode().split()]
+    assert [r[:3] for r in got] == [r[:3] for r in ref]
+    np.testing.assert_allclose([float(r[3]) for r in got], [float(r[3]) for r in ref], rtol=0, atol=2e-6)

@@ -68,6 +68,37 @@ def test_pagerank_vertex_api_bitexact(case):
         check(z, k, g.pagerank_gs_inmem(niters))
 
 
+def deltalog_text(nv, ne, deltas):
+    """<base>.deltalog as graphchi_engine::write_delta_log prints it for the
+    edge-value program (graphchi_engine.hpp:593-599): cumulative vertex updates
+    and edges touched (in + out) per iteration, then the iteration's delta sum."""
+    return "".join("%d,%d,%d,%f\n" % (i, nv * (i + 1), 2 * ne * (i + 1), x) for i, x in enumerate(deltas))
+
+
+def test_pagerank_edge_program_bitexact(case):
+    """example_apps/pagerank.cpp edge-value program (:73-113): vertex values bit for
+    bit, and the .deltalog the engine wrote, byte for byte."""
+    z, spec, g = case
+    keys = sorted({k[:-4] if k.endswith("_sha") else k for k in z.files
+                   if k.startswith("pr_edge_") and not k.endswith("_deltalog")})
+    if not keys:
+        pytest.skip("no edge-program output in this case")
+    for k in keys:
+        niters = int(k.split("_")[2])
+        v, dl = g.pagerank_gs_edge(niters)
+        check(z, k, v)
+        assert deltalog_text(g.nv, g.ne, dl) == bytes(z[k + "_deltalog"]).decode()
+
+
+def test_pagerank_vertex_api_bitexact_scale20():
+    """The in-memory program at scale 20 (20 shards of <= 1M edges, 4 iterations)."""
+    z, spec = load_golden("rmat_s20_ef16_seed1")
+    s, d = golden_input(spec)
+    g = O.OracleGraph.in_csr_only(s, d)
+    assert g.nv == int(z["nv"]) and g.ne == int(z["ne"])
+    check(z, "pr_gs_4_20_0", g.pagerank_gs_inmem(4))
+
+
 def test_pagerank_functional_sync(case):
     """pagerank_functional --mode sync (Jacobi, 0.15/N): normalised L1 <= 1e-6."""
     z, spec, g = case

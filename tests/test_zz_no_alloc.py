@@ -7,10 +7,12 @@ a CSR, out-degrees and an output vector already in their device memory; the
 library's only scratch is a fixed static device array.
 
 Checked here through the C ABI: two calls in a row agree with the regular
-entry point (gcg_pagerank on a graph built by the device sharder) within the
-PageRank tolerance used everywhere else (normalised L1 <= 1e-6), and sizes
-beyond the scratch limit and host arrays are rejected. This file is collected
-last so that a run stopping at the first failure has run every other test.
+entry point (gcg_pagerank on a graph built by the device sharder) and with the
+oracle's FP64 Jacobi iteration within the PageRank tolerance used everywhere
+else (normalised L1 <= 1e-6); each sweep that ran logs its residual and the
+slots after the last one stay untouched; sizes beyond the scratch limit and
+host arrays are rejected. This file is collected last so that a run stopping
+at the first failure has run every other test.
 """
 import numpy as np
 import pytest
@@ -35,22 +37,28 @@ def _device_csr(scale, seed):
     rp, col = g.csr(gcgpu.CSR_IN)
     od = g.degrees()[:, 1].astype(np.uint32)
     dev = lambda a: torch.from_numpy(a.view(np.int32)).cuda()  # noqa: E731
-    return g, dev(rp), dev(col), dev(od)
+    return g, dev(rp), dev(col), dev(od), O.OracleGraph(s, d)
 
 
 def test_noalloc_matches_regular_entry_point_twice():
     import torch
-    g, rp, col, od = _device_csr(16, 5)
+    g, rp, col, od, go = _device_csr(16, 5)
     n = g.num_vertices
-    assert n <= gcgpu.NOALLOC_MAX_VERTICES
+    assert n <= gcgpu.NOALLOC_MAX_VERTICES and n == go.nv
     for kw in (dict(max_sweeps=3), dict(max_sweeps=300, tol=1e-8)):
         ref, rst = g.pagerank(**kw)
+        f64, _ = go.pagerank_jacobi_f64(max_sweeps=kw["max_sweeps"], tol=kw.get("tol", 0.0))
         for _ in range(2):  # the scratch keeps the previous call's contents
             out = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
-            st = gcgpu.pagerank_csr_noalloc(rp, col, od, out, **kw)
+            res = torch.full((kw["max_sweeps"],), -7.0, dtype=torch.float64, device="cuda")
+            st = gcgpu.pagerank_csr_noalloc(rp, col, od, out, residuals=res, **kw)
             torch.cuda.synchronize()
             got = out.cpu().numpy()
             assert nl1(got, ref) <= L1_TOL
+            assert nl1(got, f64) <= L1_TOL
+            log = res.cpu().numpy()
+            assert np.all(log[:st.sweeps] >= 0.0) and np.all(log[st.sweeps:] == -7.0)
+            assert log[st.sweeps - 1] == st.residual and st.device_ms > 0.0
             if kw.get("tol"):
                 assert st.converged == 1 and st.residual <= kw["tol"]
                 assert abs(st.sweeps - rst.sweeps) <= max(3, rst.sweeps // 10)
@@ -61,7 +69,7 @@ def test_noalloc_matches_regular_entry_point_twice():
 
 def test_noalloc_rejects_oversize_and_host_arrays():
     import torch
-    g, rp, col, od = _device_csr(10, 6)
+    g, rp, col, od, _ = _device_csr(10, 6)
     out = torch.zeros(g.num_vertices, dtype=torch.float32, device="cuda")
     with pytest.raises(gcgpu.GcgError) as e:
         gcgpu.pagerank_csr_noalloc(rp, col, od, out, num_vertices=gcgpu.NOALLOC_MAX_VERTICES + 1)
