@@ -13,13 +13,19 @@ the device sharder, 64 vertex intervals.
              gcg_pagerank -> ranks to host, every step
   roofline   the main sweep kernel (k_pr_edges): 8E+16V algorithmic bytes per
              launch / its CUDA-event launch time, against measured HBM copy GB/s
-  cpu_baseline  the reference's own PageRank app (oracle/_ref/pagerank, built
-             from the reference sources) on a bounded sample, all host cores
-  extras     the other rows against their plain methods: connected components
-             (+ triangles) on symmetrised R-MAT, the learned warm start, batched
+  oracle_check  the solve's error against the oracle on the same graph, built
+             independently on the host: FP64 Jacobi to residual 1e-12 and the
+             FP32 iteration to the same tolerance (normalised L1)
+  cpu_baseline  that FP32 oracle iteration (a port of the reference's
+             bulk-synchronous PageRank) timed to the tolerance on all host cores
+  extras     the other rows against their plain methods: the bit-exact
+             vertex-API program to the tolerance, connected components (+
+             triangles) on symmetrised R-MAT, the learned warm start, batched
              personalised PageRank, 64 uneven graphs in one persistent launch
 
---impl reference times the reference alone (rank 0; other ranks exit).
+--impl reference times the reference's own PageRank app (oracle/_ref/pagerank,
+built from the reference sources, its default in-memory vertex program) on the
+same scale-24 graph, one step = one of its iterations (rank 0; other ranks exit).
 Under torchrun (N > 1) every rank solves its own replica (the path does not
 shard: replicas only); value sums the ranks' edges over the max rank time.
 """
@@ -51,17 +57,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic_per_edge():
-    """DRAM bytes per edge of one k_pr_edges launch at scale 24, from the committed
-    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of one launch / E)."""
-    path = os.path.join(ROOT, "profiles", "pagerank_edges_rmat24_full.md")
-    try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_edge:"):
-                return float(line.split(":", 1)[1].split()[0])
-    except Exception:
-        pass
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pr_edges
+# launch per edge at R-MAT scale 24, from one ncu capture of the full-size
+# workload (ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+# --clock-control none -k regex:k_pr_edges -s 2 -c 1 python bench.py --steps 1
+# --warmup 0 --no-extras --no-cpu-baseline --no-oracle-check); traffic scales
+# with the edges swept.
+TRAFFIC_BYTES_PER_EDGE = 4.36
 
 
 class ClockSampler:
@@ -115,62 +117,117 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def reference_pagerank_sample(scale, ef, seed, niters, threads, steps=1, warmup=0):
-    """Times oracle/_ref/pagerank (example_apps/pagerank.cpp) on an R-MAT sample.
-    Returns (GTEPS per step list, edges, sample description)."""
+# Sweeps the vertex-API in-memory program (example_apps/pagerank.cpp:121-146,
+# Gauss-Seidel in vertex id order) needs to reach normalised L1 residual 1e-8 on
+# the R-MAT scale-24 ef-16 seed-1 graph, as this library's bit-exact
+# GCG_PR_GS_EXACT mode measures it (the extras' gs_exact row repeats the
+# measurement live). The reference app has a fixed iteration count and no
+# residual; its time to the tolerance is its iteration time times this count.
+GS_SWEEPS_TO_TOL_RMAT24 = None
+
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np  # noqa: F401
     import oracle as O
-    import gcgpu
+    return O
+
+
+def reference_iterations(scale, ef, seed, warmup, steps, threads):
+    """Runs the reference's own PageRank app (oracle/_ref/pagerank, built from
+    example_apps/pagerank.cpp) on the R-MAT graph of the headline workload, made
+    by the oracle's restatement of the generator (no library code on this path):
+    the edge list is written, the reference shards it (convert_if_notexists,
+    nshards auto), then runs warmup + steps + 2 iterations with its default
+    configuration (membudget 800 MB: the in-memory vertex program). The engine's
+    log line "Start iteration: k" (graphchi_engine.hpp:780; "In-memory mode:
+    Iteration k starts" with a single shard, :468) arrives on stderr as iteration
+    k starts; the time between two of them is one iteration (one sweep over every
+    in-edge).
+    Iteration 0 (initialisation) and the next `warmup` are not timed."""
+    O = _oracle()
     if not O.ref_available():
         raise RuntimeError("oracle/_ref is not built")
-    s, d = gcgpu.generate_rmat(scale, ef << scale, seed=seed)
+    import re
+    t0 = time.perf_counter()
+    s, d = O.rmat_edges(scale, ef << scale, seed=seed)
     cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
-    E = int(cs.shape[0])
-    vals, walls = [], []
+    del s, d
+    E, V = int(cs.shape[0]), O.num_vertices(cs, cd)
+    niters = warmup + steps + 2
     with O.RefWorkdir(prefix="gcg_bench_ref_") as w:
         el = w.file("g.el")
         O.write_edgelist(el, cs, cd)
-        # sharding (timed separately): a 1-iteration run converts the edge list into shards
-        _, shard_wall = O.run_ref("pagerank", el, {"niters": 1, "nshards": "auto"}, threads)
-        for i in range(warmup + steps):
-            out, wall = O.run_ref("pagerank", el, {"niters": niters, "nshards": "auto"}, threads)
-            rt = O.ref_runtime(out) or wall
-            if i >= warmup:
-                vals.append(E * niters / rt / 1e9)
-                walls.append(wall)
-    sample = (f"oracle/_ref/pagerank (example_apps/pagerank.cpp, in-memory vertex program) on R-MAT scale {scale} "
-              f"ef {ef} seed {seed} ({E} edges after dedup), {niters} iterations, engine 'runtime' metric, "
-              f"GTEPS = edges x iterations / runtime, shards prepared untimed, membudget 800 MB")
-    extra = {"first_run_wall_s_with_sharding": shard_wall, "run_wall_s": walls,
-             "engine_runtime_s": [E * niters / v / 1e9 for v in vals]}
-    return vals, E, sample, extra
+        del cs, cd
+        prep_s = time.perf_counter() - t0
+        args = [os.path.join(O.REF_DIR, "pagerank"), "file", el, "filetype", "edgelist", "niters", str(niters),
+                "nshards", "auto", "execthreads", str(threads), "loadthreads", str(threads)]
+        env = dict(os.environ, GRAPHCHI_ROOT=O.REF_DIR, OMP_NUM_THREADS=str(threads))
+        starts, out_lines = {}, []
+        t1 = time.perf_counter()
+        p = subprocess.Popen(args, env=env, cwd=w.path, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        reader = threading.Thread(target=lambda: out_lines.extend(p.stdout), daemon=True)
+        reader.start()
+        err_tail = []
+        for line in p.stderr:
+            t = time.perf_counter()
+            # the shard-streaming engine's line, or the single-shard in-memory mode's
+            m = re.search(r"Start iteration: (\d+)", line) or re.search(r"In-memory mode: Iteration (\d+) starts",
+                                                                          line)
+            if m:
+                starts[int(m.group(1))] = t
+            err_tail = (err_tail + [line])[-20:]
+        rc = p.wait()
+        reader.join(timeout=10)
+        wall = time.perf_counter() - t1
+        if rc != 0:
+            raise RuntimeError(f"reference pagerank failed ({rc}): {''.join(err_tail)[-500:]}")
+        out = "".join(out_lines) + "".join(err_tail)
+        runtime = O.ref_runtime(out)
+    timed = list(range(1 + warmup, 1 + warmup + steps))
+    if any(k + 1 not in starts or k not in starts for k in timed):
+        raise RuntimeError(f"iteration start lines missing: saw {sorted(starts)[:5]}... of {niters}")
+    it_s = [starts[k + 1] - starts[k] for k in timed]
+    shard_s = starts[0] - t1 if 0 in starts else None
+    return {"edges": E, "vertices": V, "iteration_s": it_s, "gteps": [E / t / 1e9 for t in it_s],
+            "prep_s": prep_s, "shard_and_load_s": shard_s, "run_wall_s": wall, "engine_runtime_s": runtime,
+            "niters": niters}
 
 
-def reference_time_to_tol(scale, ef, seed, tol, threads):
-    """Times the reference's own functional (bulk-synchronous) engine running a
-    PageRank kernel with a residual stop (oracle/_ref/pr_functional_oracle) to
-    normalised L1 `tol` on an R-MAT sample: measured time to tolerance."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    import gcgpu
-    s, d = gcgpu.generate_rmat(scale, ef << scale, seed=seed)
-    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
-    E = int(cs.shape[0])
-    with O.RefWorkdir(prefix="gcg_bench_ttt_") as w:
-        el = w.file("g.el")
-        O.write_edgelist(el, cs, cd)
-        O.run_ref("pr_functional_oracle", el, {"niters": 1, "nshards": "auto"}, threads)  # shards, untimed
-        out, wall = O.run_ref("pr_functional_oracle", el, {"niters": 1000, "tol": tol, "teleport": "const",
-                                                            "nshards": "auto"}, threads)
-    its = [int(line.split()[1]) for line in out.splitlines() if line.startswith("iterations")]
-    n = its[-1] if its else 0
-    rt = O.ref_runtime(out) or wall
-    return {"program": "oracle/_ref/pr_functional_oracle (the reference's functional engine, bulk-synchronous, "
-                       "apply 0.15 + 0.85 sum, after_iteration residual stop)",
-            "graph": f"rmat{scale}_ef{ef}_seed{seed}", "edges": E, "tol": tol, "iterations": n,
-            "converged": n < 1000, "runtime_s": rt, "wall_s": wall, "GTEPS": E * n / rt / 1e9 if rt > 0 else None,
-            "threads": threads}
+def oracle_check(scale, ef, seed, tol, gpu_rank, gpu_sweeps, threads):
+    """The headline solve against the oracle on the same graph, built on the host
+    by the oracle alone (generator restatement, canonical in-CSR): the FP64
+    Jacobi iteration to residual 1e-12 (its error to the fixed point is below
+    1e-11) and the FP32 iteration (the reference's bulk-synchronous PageRank
+    restated) to the same tolerance as the GPU; normalised L1 of the GPU's ranks
+    against each. The FP32 run is timed: it is the CPU baseline on this workload."""
+    import numpy as np
+    O = _oracle()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    t0 = time.perf_counter()
+    s, d = O.rmat_edges(scale, ef << scale, seed=seed)
+    go = O.OracleGraph.in_csr_only(s, d)
+    del s, d
+    build_s = time.perf_counter() - t0
+    r = np.asarray(gpu_rank, np.float64)
+
+    def nl1(x):
+        x = np.asarray(x, np.float64)
+        return float(np.abs(r - x).sum() / np.abs(x).sum())
+
+    t0 = time.perf_counter()
+    f64, n64, log64 = go.pagerank_jacobi_f64_mt(max_sweeps=3000, tol=1e-12)
+    f64_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o32, n32, log32 = go.pagerank_jacobi_mt(max_sweeps=3000, tol=tol)
+    f32_s = time.perf_counter() - t0
+    return {"graph": f"rmat{scale}_ef{ef}_seed{seed}", "vertices": go.nv, "edges": go.ne,
+            "fp64_oracle_l1": nl1(f64), "fp64_sweeps": n64, "fp64_last_residual": float(log64[-1]),
+            "fp32_oracle_l1": nl1(o32), "fp32_sweeps": n32, "gpu_sweeps": gpu_sweeps,
+            "fp32_oracle_vs_fp64_l1": float(np.abs(o32.astype(np.float64) - f64).sum() / np.abs(f64).sum()),
+            "tolerance_l1": 1e-6, "pass": nl1(f64) <= 1e-6 and nl1(o32) <= 1e-6,
+            "host_build_s": build_s, "fp64_s": f64_s, "fp32_s": f32_s, "threads": threads,
+            "note": "oracle/oracle.c: graph from the generator restatement (self-loops dropped, duplicates "
+                    "removed), Jacobi 0.15 + 0.85 sum over in-neighbours' rank / outdeg, init 1"}
 
 
 def max_over_ranks(x, world, device):
@@ -196,21 +253,35 @@ def run_reference(args, rank, world):
         return
     threads = os.cpu_count() or 1
     try:
-        vals, E, sample, _ = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters, threads,
-                                                       steps=args.steps, warmup=args.warmup)
+        rec = reference_iterations(args.scale, args.ef, args.seed, args.warmup, args.steps, threads)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"[:300]}))
         return
-    v = sum(vals) / len(vals)
+    E = rec["edges"]
+    tot = sum(rec["iteration_s"])
+    v = E * args.steps / tot / 1e9
+    sample = (f"oracle/_ref/pagerank (example_apps/pagerank.cpp, default membudget 800 MB: the in-memory vertex "
+              f"program, Gauss-Seidel in vertex id order) on R-MAT scale {args.scale} ef {args.ef} seed {args.seed} "
+              f"({E} edges after dedup, the headline graph), {rec['niters']} iterations in one run; one step = one "
+              f"iteration timed between the engine's 'Start iteration' log lines; iteration 0 and {args.warmup} "
+              f"warm-up iterations untimed; sharding untimed")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"pagerank_rmat{args.ref_scale}_ef{args.ef}_cpu_sample", "sample_of":
-                   f"pagerank_rmat{args.scale}_ef{args.ef}_to_{args.tol:g}"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "config": {"workload": f"pagerank_rmat{args.scale}_ef{args.ef}_to_{args.tol:g}", "vertices": rec["vertices"],
+                   "edges": E, "step": "one PageRank iteration (sweep) of the reference engine",
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
+                         "iteration_s": rec["iteration_s"], "shard_and_load_s": rec["shard_and_load_s"],
+                         "input_prep_s": rec["prep_s"], "engine_runtime_s": rec["engine_runtime_s"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if GS_SWEEPS_TO_TOL_RMAT24 and args.scale == 24 and args.ef == 16 and args.seed == 1:
+        line["cpu_baseline"]["time_to_tol_s"] = tot / args.steps * GS_SWEEPS_TO_TOL_RMAT24
+        line["cpu_baseline"]["time_to_tol_note"] = (
+            f"mean iteration time x {GS_SWEEPS_TO_TOL_RMAT24} Gauss-Seidel sweeps to residual {args.tol:g} "
+            "(the sweeps this program needs, measured by the bit-exact GCG_PR_GS_EXACT mode)")
     print(json.dumps(line))
 
 
@@ -260,8 +331,23 @@ def run_extras(args):
                       "frac_of_radix_pass_bytes_at_hbm_peak": pass_bytes / peak / 1e6 / bms,
                       "note": "dedup + in-CSR + degrees + 64 intervals, whole build timed; 16E is the one-pass "
                               "lower bound of a sort, radix_pass_bytes what the LSD passes move (24 B per key "
-                              "per pass); the scatter pass is bound by shared-memory bank conflicts, see "
-                              "profiles/sharder_radix_rmat22.md"}
+                              "per pass); the scatter pass is bound by shared-memory bank conflicts"}
+
+    # ---- the vertex-API in-memory program (bit-exact Gauss-Seidel) to the tolerance ----
+    s, d = dev_edges(args.scale, args.ef << args.scale, args.seed)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, nshards=args.nshards, out_csr=False) as g:
+        del s, d
+        o = torch.empty(g.num_vertices, dtype=torch.float32, device="cuda")
+        runs = [g.pagerank(mode=gcgpu.PR_GS_EXACT, max_sweeps=args.max_sweeps, tol=args.tol, out=o)[1]
+                for _ in range(2)]
+        st = min(runs, key=lambda x: x.device_ms)
+        out["gs_exact"] = {"graph": f"rmat{args.scale}_ef{args.ef}_seed{args.seed}", "sweeps_to_tol": st.sweeps,
+                           "converged": st.converged, "residual": st.residual, "levels": st.levels,
+                           "ms": st.device_ms, "GTEPS": g.num_edges * st.sweeps / st.device_ms / 1e6,
+                           "note": "example_apps/pagerank.cpp in-memory program, id-ordered Gauss-Seidel, "
+                                   "bit-exact; levels of the u<v in-edge dependency schedule, one launch each "
+                                   "per sweep (CUDA graph); time excludes the level schedule's construction"}
+        del o
 
     # ---- connected components (and triangles at scale 20) ----
     cc = {}
@@ -428,8 +514,8 @@ def run_ours(args, rank, world):
     alg_bytes = 8.0 * E + 16.0 * V
     achieved = alg_bytes / per_launch_s / 1e9
     peak, peak_kind = load_peaks()
-    tr = load_traffic_per_edge()
-    traffic = tr * E if (tr and args.scale == 24) else None
+    traffic = TRAFFIC_BYTES_PER_EDGE * E if args.scale == 24 else None
+    gpu_rank = out.cpu().numpy()
 
     # ---- e2e: host buffers through the C ABI ----
     hs = torch.empty(m, dtype=torch.int32, pin_memory=True)
@@ -453,23 +539,27 @@ def run_ours(args, rank, world):
     e2e_s = max_over_ranks(sum(e2e_times) if e2e_times else float("nan"), world, "cuda")
     e2e_value = whole_job_gteps(e2e_edges, world, e2e_s) if e2e_times else None
 
-    # ---- CPU baseline: the reference's own PageRank on a bounded sample ----
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # ---- oracle check and CPU baseline: the oracle on the same graph, host cores ----
+    cpu, check = None, None
+    if rank == 0 and world == 1 and not (args.no_oracle_check and args.no_cpu_baseline):
+        threads = os.cpu_count() or 1
         try:
-            vals, Es, sample, extra = reference_pagerank_sample(args.ref_scale, args.ef, args.seed, args.ref_iters,
-                                                                os.cpu_count() or 1)
-            cpu = {"value": vals[0], "unit": UNIT, "cores": os.cpu_count(), "kind": "reference", "sample": sample}
-            cpu.update(extra)
-            # the headline workload at the sample's rate: edges x sweeps of one solve / edges per second
-            cpu["estimated_s_to_tol_at_headline_size"] = E * sweeps[0] / (vals[0] * 1e9)
-            cpu["estimate_note"] = ("per-iteration rate of the sample x the sweeps the headline solve needs; "
-                                    "the reference's PageRank has no residual stop (pagerank.cpp)")
-            cpu["functional_time_to_tol"] = reference_time_to_tol(16, args.ef, args.seed, args.tol,
-                                                                  os.cpu_count() or 1)
+            check = oracle_check(args.scale, args.ef, args.seed, args.tol, gpu_rank, sweeps[0], threads)
+            if check["vertices"] != V or check["edges"] != E:
+                raise RuntimeError(f"oracle graph differs: {check['vertices']} x {check['edges']} vs {V} x {E}")
+            cpu = {"value": E * check["fp32_sweeps"] / check["fp32_s"] / 1e9, "unit": UNIT, "cores": threads,
+                   "kind": "port", "time_to_tol_s": check["fp32_s"], "sweeps": check["fp32_sweeps"],
+                   "sample": (f"the whole workload: oracle/oracle.c orc_pagerank_jacobi_mt (the reference's "
+                              f"bulk-synchronous PageRank, pagerank_functional.cpp:48-83 with the 0.15 + 0.85 sum "
+                              f"apply, restated in C with OpenMP over rows) from the uniform start to residual "
+                              f"{args.tol:g} on the same R-MAT scale-{args.scale} graph, {threads} threads; "
+                              f"GTEPS = edges x sweeps / time")}
         except Exception as e:  # noqa: BLE001
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"unavailable: {e}"[:300]}
+            check = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+        if args.no_cpu_baseline:
+            cpu = None
+        if args.no_oracle_check:
+            check = None
 
     extras = None
     if rank == 0 and world == 1 and not args.no_extras:
@@ -500,6 +590,7 @@ def run_ours(args, rank, world):
                     "ms_per_step": e2e_s / max(1, args.e2e_steps) * 1e3},
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "oracle_check": check,
             "cpu_baseline": cpu,
             "extras": extras,
         }
@@ -521,9 +612,8 @@ def main():
     ap.add_argument("--nshards", type=int, default=64)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-warmup", type=int, default=1)
-    ap.add_argument("--ref-scale", type=int, default=20)
-    ap.add_argument("--ref-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle-check", action="store_true", help="skip the host oracle's check of the answer")
     ap.add_argument("--no-extras", action="store_true", help="skip the CC / warm-start / batched rows")
     args = ap.parse_args()
 

@@ -844,6 +844,7 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
         /* per-graph init, initial vector (2), the persistent kernel, the rank
          * assembly, the map to the callers' layout, and the map of init_rank */
         stats->kernel_launches = 6 + (p->init_rank ? 1 : 0);
+        stats->levels = 0;
     }
     return GCG_OK;
 }

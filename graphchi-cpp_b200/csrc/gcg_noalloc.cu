@@ -261,6 +261,7 @@ extern "C" int gcg_pagerank_csr_noalloc(const uint32_t *in_rowptr, const uint32_
         stats->sweep_kernel_ms = 0.0;
         stats->timed_sweeps = 0;
         stats->kernel_launches = 1 + launched;
+        stats->levels = 0;
     }
     return GCG_OK;
 }

@@ -865,6 +865,7 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
 
 int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg_pr_stats *stats) {
     if (!g || !params) return fail(GCG_ERR_INVALID, "gcg_pagerank: null argument");
+    if (stats) *stats = gcg_pr_stats{};
     if (params->max_sweeps < 0) return fail(GCG_ERR_INVALID, "gcg_pagerank: max_sweeps < 0");
     if (params->source != GCG_NO_SOURCE && params->source >= g->nv)
         return fail(GCG_ERR_INVALID, "gcg_pagerank: personalisation source >= num_vertices");

@@ -80,25 +80,28 @@ __global__ void k_gs_init(uint32_t nv, const uint32_t *__restrict__ outdeg, floa
     }
 }
 
-/* pagerank.cpp:80-85 (edge-value program, iteration 0): out-edges hold
- * (float)(1.0 / outdeg), the vertex 0.15 */
-__global__ void k_gs_edge_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float reset, float *c, float *val) {
+/* pagerank.cpp:80-83 (edge-value program, iteration 0): out-edges hold
+ * (float)(1.0 / outdeg) */
+__global__ void k_gs_edge_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float *c) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         const uint32_t oc = outdeg[v];
         c[v] = oc > 0 ? __double2float_rn(__ddiv_rn(1.0, (double)oc)) : 0.0f;
-        val[v] = reset;
     }
 }
 
 /* One level of a sweep. In-memory program (EDGE = false), pagerank.cpp:127-136:
  * pr = (float)((0.15 + 0.85 * (double)sum) / outc). Edge-value program (EDGE =
  * true), pagerank.cpp:89-111: pagerank = (float)(0.15 + 0.85 * (double)sum), the
- * out-edge value pagerank / outc in float, |pagerank - old| into delta[v]. */
-template <bool EDGE>
+ * out-edge value pagerank / outc in float. TRACK (always with EDGE): the vertex's
+ * pagerank goes to val[v] and |pagerank - previous| (float) to delta[v], for
+ * the progress log and the residual stop. Levels of sweeps queued after `done`
+ * was raised return at once. */
+template <bool EDGE, bool TRACK>
 __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, uint32_t end,
                            const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
                            const uint32_t *__restrict__ outdeg, const float *__restrict__ pr_old, float *pr_new,
-                           float *val, float *delta, double reset, double damping) {
+                           float *val, float *delta, const int *done, double reset, double damping) {
+    if (TRACK && *(volatile const int *)done) return;
     for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const uint32_t v = order[i];
         float sum = 0.0f;
@@ -111,36 +114,47 @@ __global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, u
          * the reference's separate double multiply and add */
         const int outc = (int)outdeg[v];
         const double t = __dadd_rn(reset, __dmul_rn(damping, (double)sum));
-        if (EDGE) {
+        if (EDGE) pr_new[v] = outc > 0 ? __fdiv_rn(__double2float_rn(t), (float)outc) : 0.0f;
+        else pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
+        if (TRACK) {
             const float pagerank = __double2float_rn(t);
-            pr_new[v] = outc > 0 ? __fdiv_rn(pagerank, (float)outc) : 0.0f;
             delta[v] = fabsf(__fsub_rn(pagerank, val[v]));
             val[v] = pagerank;
-        } else {
-            pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
         }
     }
 }
 
-/* The sweep's delta sum: each block adds a fixed slice in FP64, the last block
- * to finish adds the block sums in block order into log[*slot] and advances
- * *slot (the next sweep's entry). */
+/* The sweep's sums of delta[] and |val[]|: each block adds a fixed slice in
+ * FP64, the last block to finish adds the block sums in block order, logs
+ * delta_log[k] = sum delta and res_log[k] = sum delta / sum |val| for the k-th
+ * sweep (k = *slot, then advanced) and raises *done when the residual is <= tol. */
 constexpr int DSUM_BLOCKS = 256;
-__global__ void __launch_bounds__(256) k_gs_delta_sum(const float *__restrict__ delta, uint32_t nv, double *part,
-                                                      uint32_t *ticket, uint32_t *slot, double *log) {
-    __shared__ double s[8];
+__global__ void __launch_bounds__(256) k_gs_delta_sum(const float *__restrict__ delta, const float *__restrict__ val,
+                                                      uint32_t nv, double2 *part, uint32_t *ticket, uint32_t *slot,
+                                                      int *done, double tol, double *delta_log, double *res_log) {
+    if (*(volatile const int *)done) return;
+    __shared__ double2 s[8];
     __shared__ int s_last;
     const uint32_t per = (nv + gridDim.x - 1) / gridDim.x;
     const uint32_t b0 = blockIdx.x * per, b1 = min(nv, b0 + per);
-    double x = 0.0;
-    for (uint32_t v = b0 + threadIdx.x; v < b1; v += blockDim.x) x += (double)delta[v];
+    double x = 0.0, y = 0.0;
+    for (uint32_t v = b0 + threadIdx.x; v < b1; v += blockDim.x) {
+        x += (double)delta[v];
+        y += fabs((double)val[v]);
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
-    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = x;
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+        y += __shfl_down_sync(0xFFFFFFFFu, y, o);
+    }
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = make_double2(x, y);
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < 8; ++w) t += s[w];
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < 8; ++w) {
+            t.x += s[w].x;
+            t.y += s[w].y;
+        }
         part[blockIdx.x] = t;
         __threadfence();
         s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
@@ -148,12 +162,27 @@ __global__ void __launch_bounds__(256) k_gs_delta_sum(const float *__restrict__ 
     __syncthreads();
     if (!s_last || threadIdx.x != 0) return;
     __threadfence();
-    double t = 0.0;
-    for (uint32_t b = 0; b < gridDim.x; ++b) t += __ldcg(part + b);
+    double dx = 0.0, ny = 0.0;
+    for (uint32_t b = 0; b < gridDim.x; ++b) {
+        const double2 p = __ldcg(part + b);
+        dx += p.x;
+        ny += p.y;
+    }
     const uint32_t k = *slot;
-    log[k] = t;
+    const double res = ny > 0.0 ? dx / ny : 0.0;
+    delta_log[k] = dx;
+    res_log[k] = res;
     *slot = k + 1;
+    if (tol > 0.0 && res <= tol) *done = 1;
     *ticket = 0u;
+}
+
+/* the vertex values before the first sweep, for the progress log: the edge-value
+ * program's 0.15 (pagerank.cpp:84), the in-memory program's pr * outc = 1 (or
+ * 0.15 without out-edges, pagerank.cpp:137-139) */
+__global__ void k_gs_val_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float reset, int edge, float *val) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        val[v] = (edge || outdeg[v] == 0) ? reset : 1.0f;
 }
 
 /* pagerank.cpp:140-143: the stored value is pr * outc on the last iteration */
@@ -225,31 +254,38 @@ static int build_gs_plan(gcg_graph *g, GsPlan &pl) {
     return GCG_OK;
 }
 
-/* GCG_PR_GS_EXACT (in-memory program) and GCG_PR_GS_EDGE (edge-value program) */
+/* GCG_PR_GS_EXACT (in-memory program) and GCG_PR_GS_EDGE (edge-value program).
+ * With tol > 0, residuals or delta_log (always for GS_EDGE) every sweep also
+ * tracks the vertices' pageranks: delta_log gets sum |pagerank - previous| and
+ * residuals that sum over sum |pagerank| (the Jacobi residual's definition); the
+ * run stops after the first sweep whose residual is <= tol. */
 int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg_pr_stats *stats) {
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
     const bool edge = p->mode == GCG_PR_GS_EDGE;
+    const bool track = edge || p->tol > 0.0 || p->residuals || p->delta_log;
     GsPlan pl;
     GCG_TRY(build_gs_plan(g, pl));
     const int nsw = p->max_sweeps;
     tbuf<float> pr, val, delta;
-    tbuf<double> dlog, part;
-    tbuf<uint32_t> ctl; /* ticket, slot */
+    tbuf<double> logs; /* delta_log[nsw], res_log[nsw] */
+    tbuf<double2> part;
+    tbuf<uint32_t> ctl; /* ticket, slot, done */
     GCG_TRY(pr.alloc((size_t)2 * nv, s));
+    GCG_TRY(ctl.alloc(4, s));
+    GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 4 * sizeof(uint32_t), s));
+    int *done = (int *)(ctl.get() + 2);
     float *pr_old = pr.get(), *pr_new = pr.get() + nv;
     const float reset = (float)p->teleport;
-    if (edge) {
+    if (track) {
         GCG_TRY(val.alloc(nv, s));
         GCG_TRY(delta.alloc(nv, s));
-        GCG_TRY(dlog.alloc(std::max(1, nsw), s));
+        GCG_TRY(logs.alloc(2 * (size_t)std::max(1, nsw), s));
         GCG_TRY(part.alloc(DSUM_BLOCKS, s));
-        GCG_TRY(ctl.alloc(2, s));
-        GCG_CUDA(cudaMemsetAsync(ctl.get(), 0, 2 * sizeof(uint32_t), s));
-        k_gs_edge_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old, val.get());
-    } else {
-        k_gs_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old);
+        k_gs_val_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, edge ? 1 : 0, val.get());
     }
+    if (edge) k_gs_edge_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), pr_old);
+    else k_gs_init<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), reset, pr_old);
     GCG_LAUNCH_CHECK();
 
     cudaEvent_t ev0, ev1;
@@ -264,17 +300,21 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
     for (uint32_t l = 0; l < pl.nlev; ++l) {
         uint32_t b = pl.off[l], e = pl.off[l + 1];
         if (b == e) continue;
+        const unsigned gr = vgrid(e - b);
+        const uint32_t *rp = g->in_rowptr.get(), *cl = g->in_col.get(), *od = g->outdeg.get();
         if (edge)
-            k_gs_level<true><<<vgrid(e - b), 256, 0, cap>>>(pl.order.get(), b, e, g->in_rowptr.get(), g->in_col.get(),
-                                                           g->outdeg.get(), pr_old, pr_new, val.get(), delta.get(),
-                                                           p->teleport, p->damping);
+            k_gs_level<true, true><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, val.get(),
+                                                        delta.get(), done, p->teleport, p->damping);
+        else if (track)
+            k_gs_level<false, true><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, val.get(),
+                                                         delta.get(), done, p->teleport, p->damping);
         else
-            k_gs_level<false><<<vgrid(e - b), 256, 0, cap>>>(pl.order.get(), b, e, g->in_rowptr.get(),
-                                                            g->in_col.get(), g->outdeg.get(), pr_old, pr_new,
-                                                            nullptr, nullptr, p->teleport, p->damping);
+            k_gs_level<false, false><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, nullptr,
+                                                          nullptr, done, p->teleport, p->damping);
     }
-    if (edge)
-        k_gs_delta_sum<<<DSUM_BLOCKS, 256, 0, cap>>>(delta.get(), nv, part.get(), ctl.get(), ctl.get() + 1, dlog.get());
+    if (track)
+        k_gs_delta_sum<<<DSUM_BLOCKS, 256, 0, cap>>>(delta.get(), val.get(), nv, part.get(), ctl.get(), ctl.get() + 1,
+                                                     done, p->tol, logs.get(), logs.get() + std::max(1, nsw));
     cudaMemcpyAsync(pr_old, pr_new, (size_t)nv * 4, cudaMemcpyDeviceToDevice, cap);
     cudaError_t ce = cudaStreamEndCapture(cap, &graph);
     if (ce != cudaSuccess) {
@@ -287,39 +327,62 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
         cudaGraphDestroy(graph);
         return fail(GCG_ERR_CUDA, std::string("sweep graph instantiate: ") + cudaGetErrorString(ce));
     }
+    /* sweeps are queued in chunks of 8; with a tolerance the host checks the
+     * sweep count after each chunk (sweeps queued past convergence return at once) */
+    uint32_t h_ctl[4] = {0, 0, 0, 0};
     GCG_CUDA(cudaEventRecord(ev0, s));
-    for (int sw = 0; sw < nsw; ++sw) GCG_CUDA(cudaGraphLaunch(exec, s));
+    for (int sw = 0; sw < nsw;) {
+        const int n = std::min(8, nsw - sw);
+        for (int k = 0; k < n; ++k) GCG_CUDA(cudaGraphLaunch(exec, s));
+        sw += n;
+        if (p->tol > 0.0 && sw < nsw) {
+            GCG_CUDA(cudaMemcpyAsync(h_ctl, ctl.get(), sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
+            GCG_CUDA(cudaStreamSynchronize(s));
+            if (h_ctl[2]) break;
+        }
+    }
     GCG_CUDA(cudaEventRecord(ev1, s));
+    GCG_CUDA(cudaMemcpyAsync(h_ctl, ctl.get(), sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
     if (!edge) {
         k_gs_final<<<vgrid(nv), 256, 0, s>>>(nv, g->outdeg.get(), pr_old, pr_new);
         GCG_LAUNCH_CHECK();
     }
     GCG_CUDA(cudaEventSynchronize(ev1));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    const int sweeps = track ? (int)h_ctl[1] : nsw;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
+    double last_res = 0.0;
+    if (track && sweeps > 0)
+        GCG_CUDA(cudaMemcpy(&last_res, logs.get() + std::max(1, nsw) + sweeps - 1, sizeof(double),
+                            cudaMemcpyDeviceToHost));
     if (out_rank) GCG_TRY(copy_out(out_rank, edge ? val.get() : pr_new, (size_t)nv * 4, s));
-    if (edge && p->delta_log && nsw > 0) GCG_TRY(copy_out(p->delta_log, dlog.get(), (size_t)nsw * sizeof(double), s));
-    if (edge && p->work_log && nsw > 0) { /* every vertex updated, its in- and out-edges touched, per sweep */
-        std::vector<uint64_t> wl(2 * (size_t)nsw);
-        for (int i = 0; i < nsw; ++i) {
+    if (track && p->delta_log && sweeps > 0)
+        GCG_TRY(copy_out(p->delta_log, logs.get(), (size_t)sweeps * sizeof(double), s));
+    if (track && p->residuals && sweeps > 0)
+        GCG_TRY(copy_out(p->residuals, logs.get() + std::max(1, nsw), (size_t)sweeps * sizeof(double), s));
+    if (p->work_log && sweeps > 0) { /* every vertex updated per sweep; its in-edges (+ out-edges with edge values) */
+        std::vector<uint64_t> wl(2 * (size_t)sweeps);
+        for (int i = 0; i < sweeps; ++i) {
             wl[2 * i] = (uint64_t)nv * (uint64_t)(i + 1);
-            wl[2 * i + 1] = 2 * g->ne * (uint64_t)(i + 1);
+            wl[2 * i + 1] = (edge ? 2 : 1) * g->ne * (uint64_t)(i + 1);
         }
         GCG_TRY(copy_out(p->work_log, wl.data(), wl.size() * sizeof(uint64_t), s));
     }
     GCG_CUDA(cudaStreamSynchronize(s));
     if (stats) {
-        stats->sweeps = nsw;
-        stats->converged = 0;
-        stats->residual = 0.0;
+        stats->sweeps = sweeps;
+        stats->converged = (int)h_ctl[2];
+        stats->residual = last_res;
         stats->device_ms = ms;
         stats->sweep_kernel_ms = ms;
-        stats->timed_sweeps = nsw;
-        stats->kernel_launches = (edge ? 1 : 2) + ((int)pl.nlev + (edge ? 1 : 0)) * nsw;
+        stats->timed_sweeps = sweeps;
+        stats->kernel_launches = 1 + (track ? 1 : 0) + (edge ? 0 : 1) + ((int)pl.nlev + (track ? 1 : 0)) * sweeps;
+        stats->levels = (int)pl.nlev;
     }
     return GCG_OK;
 }

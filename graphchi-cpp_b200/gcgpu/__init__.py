@@ -88,7 +88,7 @@ NO_SOURCE = 0xFFFFFFFF
 class PrStats(C.Structure):
     _fields_ = [("sweeps", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("device_ms", C.c_double), ("sweep_kernel_ms", C.c_double), ("timed_sweeps", C.c_int),
-                ("kernel_launches", C.c_int)]
+                ("kernel_launches", C.c_int), ("levels", C.c_int)]
 
 
 class MlpTrainParams(C.Structure):

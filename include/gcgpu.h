@@ -218,6 +218,7 @@ typedef struct {
     double sweep_kernel_ms; /* with GCG_PR_TIME_SWEEPS: summed time of the main sweep kernel */
     int timed_sweeps;       /* launches summed into sweep_kernel_ms */
     int kernel_launches;    /* kernels this call launched (early-exit launches included) */
+    int levels;             /* GS modes: levels of the id-ordered dependency schedule (else 0) */
 } gcg_pr_stats;
 
 /* Fills params with the vertex-API defaults: Jacobi, teleport 0.15, damping 0.85,

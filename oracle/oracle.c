@@ -652,3 +652,62 @@ void orc_pagerank_gs_edge(uint32_t nv, const uint32_t *in_rowptr, const uint32_t
     free(c);
     free(val);
 }
+
+/* Either vertex-API program (edge = 0: in-memory, pagerank.cpp:121-146; edge =
+ * 1: edge values, :73-113) in the engine's id order, tracking each vertex's
+ * pagerank (float)(0.15 + 0.85 * (double)sum) from sweep to sweep: delta_log[k]
+ * = sum of |pagerank - previous| (float differences, added in double in vertex
+ * order), res_log[k] = delta_log[k] / sum |pagerank|. The previous value before
+ * the first sweep is the vertex value the app holds then: 0.15 for the edge
+ * program (:84), pr * outc = 1 (0.15 without out-edges) for the in-memory one
+ * (:137-139). Stops after the first sweep whose residual is <= tol (tol > 0) or
+ * after max_sweeps; out_values as the app stores them after the last sweep.
+ * Returns the sweeps run. */
+int orc_pagerank_gs_track(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                          const uint32_t *outdeg, int edge, int max_sweeps, double tol,
+                          float *out_values, double *delta_log, double *res_log) {
+    const double RESET = 0.15;
+    float *c = (float *)malloc((size_t)(nv ? nv : 1) * sizeof(float));
+    float *val = (float *)malloc((size_t)(nv ? nv : 1) * sizeof(float));
+    for (uint32_t v = 0; v < nv; ++v) {
+        const uint32_t outc = outdeg[v];
+        if (edge) {
+            c[v] = outc ? (float)(1.0 / (double)outc) : 0.0f;
+            val[v] = (float)RESET;
+        } else {
+            c[v] = outc ? 1.0f / (float)outc : (float)RESET;
+            val[v] = outc ? 1.0f : (float)RESET;
+        }
+    }
+    int sweeps = 0;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        double dsum = 0.0, nsum = 0.0;
+        for (uint32_t v = 0; v < nv; ++v) {
+            const uint32_t outc = outdeg[v];
+            float sum = 0.0f;
+            for (uint32_t j = in_rowptr[v]; j < in_rowptr[v + 1]; ++j) sum += c[in_col[j]];
+            const double t = RESET + (1 - RESET) * (double)sum;
+            const float pagerank = (float)t;
+            if (edge) {
+                if (outc > 0) c[v] = pagerank / (float)outc;
+            } else {
+                c[v] = outc > 0 ? (float)(t / (double)outc) : (float)t;
+            }
+            dsum += (double)fabsf(pagerank - val[v]);
+            nsum += fabs((double)pagerank);
+            val[v] = pagerank;
+        }
+        ++sweeps;
+        const double res = nsum > 0 ? dsum / nsum : 0.0;
+        if (delta_log) delta_log[sw] = dsum;
+        if (res_log) res_log[sw] = res;
+        if (tol > 0 && res <= tol) break;
+    }
+    for (uint32_t v = 0; v < nv; ++v) {
+        if (edge) out_values[v] = val[v];
+        else out_values[v] = outdeg[v] > 0 ? c[v] * (float)outdeg[v] : c[v];
+    }
+    free(c);
+    free(val);
+    return sweeps;
+}

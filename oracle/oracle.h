@@ -65,6 +65,16 @@ void orc_pagerank_gs_inmem(uint32_t nv, const uint32_t *in_rowptr, const uint32_
 void orc_pagerank_gs_edge(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
                           const uint32_t *outdeg, int niters, float *out_values, double *delta_log);
 
+/* Either vertex-API program (edge 0: in-memory, edge 1: edge values) with
+ * per-sweep tracking of the pageranks (float)(0.15 + 0.85*(double)sum):
+ * delta_log[k] = sum |pagerank - previous|, res_log[k] = that / sum |pagerank|
+ * (either may be NULL); stops after the first sweep with residual <= tol (tol >
+ * 0) or after max_sweeps sweeps (iterations after the initial one). out_values
+ * as the app stores them. Returns the sweeps run. */
+int orc_pagerank_gs_track(uint32_t nv, const uint32_t *in_rowptr, const uint32_t *in_col,
+                          const uint32_t *outdeg, int edge, int max_sweeps, double tol,
+                          float *out_values, double *delta_log, double *res_log);
+
 /* Bulk-synchronous PageRank with the functional kernel contract
  * (src/api/functional/functional_bulksync.hpp:91-113,
  * example_apps/pagerank_functional.cpp:51-81): init value `init`; each sweep

@@ -41,6 +41,7 @@ def lib():
             ("orc_auto_nshards", _u32, [_u64, _u32, _u32]),
             ("orc_pagerank_gs_inmem", None, [_u32, _vp, _vp, _vp, _i, _vp]),
             ("orc_pagerank_gs_edge", None, [_u32, _vp, _vp, _vp, _i, _vp, _vp]),
+            ("orc_pagerank_gs_track", _i, [_u32, _vp, _vp, _vp, _i, _i, _d, _vp, _vp, _vp]),
             ("orc_pagerank_jacobi", _i, [_u32, _vp, _vp, _vp, _d, _d, _f, _i, _d, _vp, _vp]),
             ("orc_pagerank_jacobi_f64", _i, [_u32, _vp, _vp, _vp, _d, _d, _d, _i, _d, _vp]),
             ("orc_cc", _i, [_u32, _vp, _vp, _vp, _vp, _vp]),
@@ -156,6 +157,15 @@ class OracleGraph:
         lib().orc_pagerank_gs_edge(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg), niters, _p(out),
                                    _p(log))
         return out, log[:niters].copy()
+
+    def pagerank_gs_track(self, edge, max_sweeps, tol=0.0):
+        """Vertex-API program with per-sweep tracking: (values, sweeps, delta log, residual log)."""
+        out = np.zeros(self.nv, np.float32)
+        dl = np.zeros(max(1, max_sweeps), np.float64)
+        rl = np.zeros(max(1, max_sweeps), np.float64)
+        n = lib().orc_pagerank_gs_track(self.nv, _p(self.in_rowptr), _p(self.in_col), _p(self.outdeg), int(edge),
+                                        max_sweeps, tol, _p(out), _p(dl), _p(rl))
+        return out, n, dl[:n].copy(), rl[:n].copy()
 
     def pagerank_jacobi(self, teleport=0.15, damping=0.85, init=1.0, max_sweeps=3, tol=0.0):
         out = np.zeros(self.nv, np.float32)

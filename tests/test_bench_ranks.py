@@ -69,7 +69,7 @@ def test_reference_arm_under_torchrun_runs_on_rank_zero_only():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-scale", "12", "--ref-iters", "2"]
+           "--gpus", "2", "--steps", "2", "--warmup", "1", "--scale", "12"]
     out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [line for line in out.stdout.splitlines() if line.startswith("{")]
@@ -78,3 +78,14 @@ def test_reference_arm_under_torchrun_runs_on_rank_zero_only():
     assert rec["impl"] == "reference" and rec["value"] > 0
     assert rec["cpu_baseline"]["kind"] == "reference"
     assert rec["e2e"]["h2d_bytes_per_step"] == 0 and rec["e2e"]["d2h_bytes_per_step"] == 0
+    # the same workload as the GPU arm (scale 12 here), one step = one timed iteration
+    assert rec["config"]["workload"] == "pagerank_rmat12_ef16_to_1e-08"
+    assert len(rec["cpu_baseline"]["iteration_s"]) == 2 and rec["ms_per_step"] > 0
+
+
+def test_reference_arm_loads_no_library_code():
+    # the reference arm makes its input with the oracle's generator restatement:
+    # nothing of the library under test runs on the reference's path
+    src = open(os.path.join(ROOT, "bench.py")).read()
+    body = src[src.index("def reference_iterations("):src.index("def oracle_check(")]
+    assert "gcgpu" not in body

@@ -96,6 +96,25 @@ def test_pagerank_gs_edge_bitexact_vs_reference(name):
         np.testing.assert_allclose(dl, deltas[1:], rtol=0, atol=1e-6 + 1e-12 * deltas.max())
 
 
+@pytest.mark.parametrize("name,mode", [("rmat_s16_ef16_seed1", "inmem"), ("rmat_s10_ef16_seed1", "inmem"),
+                                       ("er_n300000_m2400000_seed7", "edge")])
+def test_pagerank_gs_residual_stop_vs_oracle(name, mode):
+    """Both vertex-API programs run to residual 1e-8: the same sweep count as the
+    oracle's restatement, the same residual trace (FP64 sums in another order:
+    rtol 1e-9) and bit-identical values."""
+    z, spec, g, go = graph_for(name)
+    edge = mode == "edge"
+    res = np.zeros(1000, np.float64)
+    dl = np.zeros(1000, np.float64)
+    r, st = g.pagerank(mode=gcgpu.PR_GS_EDGE if edge else gcgpu.PR_GS_EXACT, max_sweeps=1000, tol=1e-8,
+                       residuals=res, delta_log=dl)
+    v, n, odl, orl = go.pagerank_gs_track(edge, 1000, 1e-8)
+    assert st.converged == 1 and st.sweeps == n and st.levels > 1
+    np.testing.assert_allclose(res[:n], orl, rtol=1e-9, atol=0)
+    np.testing.assert_allclose(dl[:n], odl, rtol=1e-9, atol=0)
+    assert np.array_equal(r, v)
+
+
 def test_pagerank_gs_exact_scale20_vs_reference():
     """The in-memory program at scale 20 (V far above the edge kernel's hub), 4
     iterations, bit for bit against the reference's digest."""

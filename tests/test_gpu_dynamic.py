@@ -1,8 +1,8 @@
 """Dynamic graphs through the C ABI (gcg_graph_add_edges / gcg_graph_delete_edges,
 the batched counterpart of graphchi_dynamicgraph_engine's edge insertion and
-deletion): after each batch the resident graph equals a graph built from scratch
-on the resulting edge list (CSRs, degrees, intervals bit-exact), and algorithms
-on it give the same answers."""
+deletion): after each batch the resident graph equals the oracle's graph of the
+resulting edge list (CSRs, degrees, intervals bit-exact) and a graph built from
+scratch on it, and algorithms on it give the oracle's answers."""
 import numpy as np
 import pytest
 
@@ -22,6 +22,19 @@ def same_graph(a, b):
         assert np.array_equal(ra, rb) and np.array_equal(ca, cb)
     assert np.array_equal(a.degrees(), b.degrees())
     assert np.array_equal(a.intervals(), b.intervals())
+
+
+def same_as_oracle(g, s, d, sym, nshards):
+    go = O.OracleGraph(s, d, symmetrise=sym, nv=g.num_vertices)
+    assert g.num_edges == go.ne
+    rp, col = g.csr(gcgpu.CSR_IN)
+    assert np.array_equal(rp, go.in_rowptr) and np.array_equal(col, go.in_col)
+    if g.info().has_out_csr:
+        rp, col = g.csr(gcgpu.CSR_OUT)
+        assert np.array_equal(rp, go.out_rowptr) and np.array_equal(col, go.out_col)
+    assert np.array_equal(g.degrees(), go.degrees())
+    assert np.array_equal(g.intervals(), go.intervals(nshards))
+    return go
 
 
 def remove_pairs(s, d, ds, dd):
@@ -50,6 +63,7 @@ def test_add_then_delete_equals_fresh_build(sym, device_input):
         with gcgpu.Graph.from_edges(s2, d2, dedup=True, symmetrise=sym, nshards=8) as ref:
             same_graph(g, ref)
             assert g.num_vertices == max(int(s2.max()), int(d2.max())) + 1
+        same_as_oracle(g, s2, d2, sym, 8)
         g.delete_edges(conv(del_s), conv(del_d))
         if sym:  # an undirected edge goes in both directions
             del_s, del_d = np.concatenate([del_s, del_d]), np.concatenate([del_d, del_s])
@@ -67,6 +81,10 @@ def test_add_then_delete_equals_fresh_build(sym, device_input):
             l1, _ = g.connected_components()
             l2, _ = ref.connected_components()
             assert np.array_equal(l1, l2)
+        go = same_as_oracle(g, s3, d3, sym, 8)
+        o32, _, _ = go.pagerank_jacobi(max_sweeps=10)
+        assert np.abs(r1.astype(np.float64) - o32).sum() / np.abs(o32).sum() <= 1e-6
+        assert np.array_equal(l1, go.cc()[0])
 
 
 def test_updates_after_a_solve_and_nothing_to_delete():

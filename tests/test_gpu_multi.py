@@ -1,5 +1,6 @@
 """Many graphs in one persistent launch (gcg_batch_pagerank) through the C ABI:
-each graph's ranks against its own single-graph solve, and the bounded
+each graph's ranks against the oracle (FP32 iteration at fixed sweeps, FP64 fixed
+point at the tolerance) and against its own single-graph solve, and the bounded
 grid-barrier wait (failure detection without a GPU fault)."""
 import numpy as np
 import pytest
@@ -10,19 +11,45 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 
+SPECS = [("rmat", 12, 1), ("er", 3000, 2), ("rmat", 9, 3), ("empty", 0, 0), ("er", 20000, 4),
+         ("rmat", 14, 5), ("er", 700, 6)]
+
+
+def edges(kind, n, seed):
+    if kind == "rmat":
+        return O.rmat_numpy(n, 16 << n, seed=seed)
+    if kind == "er":
+        return O.er_numpy(n, 8 * n, seed=seed)
+    return np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+
+
 def make_graphs():
-    specs = [("rmat", 12, 1), ("er", 3000, 2), ("rmat", 9, 3), ("empty", 0, 0), ("er", 20000, 4),
-             ("rmat", 14, 5), ("er", 700, 6)]
-    gs = []
-    for kind, n, seed in specs:
-        if kind == "rmat":
-            s, d = O.rmat_numpy(n, 16 << n, seed=seed)
-        elif kind == "er":
-            s, d = O.er_numpy(n, 8 * n, seed=seed)
-        else:
-            s = d = np.zeros(0, np.uint32)
-        gs.append(gcgpu.Graph.from_edges(s, d, dedup=True))
-    return gs
+    return [gcgpu.Graph.from_edges(*edges(*sp), dedup=True) for sp in SPECS]
+
+
+def nl1(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b).sum() / np.abs(b).sum()
+
+
+def test_batch_against_oracle():
+    gs = make_graphs()
+    oracles = [O.OracleGraph(*edges(*sp)) for sp in SPECS]
+    with gcgpu.Batch(gs) as b:
+        r, sw, res, st = b.pagerank(max_sweeps=20, tol=0.0)
+        for g, go, part in zip(gs, oracles, b.split(r)):
+            assert g.num_vertices == go.nv and g.num_edges == go.ne
+            ref, n, _ = go.pagerank_jacobi(max_sweeps=20)
+            assert nl1(part, ref) <= 1e-6
+        r, sw, res, st = b.pagerank(max_sweeps=1000, tol=1e-8)
+        assert st.converged == 1
+        for k, (go, part) in enumerate(zip(oracles, b.split(r))):
+            f64, _ = go.pagerank_jacobi_f64(max_sweeps=3000, tol=1e-12)
+            assert nl1(part, f64) <= 1e-6, k
+            o32, n32, _ = go.pagerank_jacobi(max_sweeps=1000, tol=1e-8)
+            assert nl1(part, o32) <= 1e-6 and abs(int(sw[k]) - n32) <= max(3, n32 // 10), (k, sw[k], n32)
+    for g in gs:
+        g.free()
 
 
 def test_batch_fixed_sweeps_equal_single_graph_solves():
