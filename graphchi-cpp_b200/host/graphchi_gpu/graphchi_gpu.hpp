@@ -290,6 +290,34 @@ class graphchi_engine {
         fclose(f);
     }
 
+    /* The .deltalog the reference's engine writes for the app's vertex programs
+     * after `niters` iterations (iteration 0 = initialisation). With one shard and
+     * fewer than 80M vertices the engine runs in its in-memory mode
+     * (graphchi_engine.hpp:299-301, maxwindow 40M :199) and writes one line after
+     * all iterations, with the counters of all of them (:465-506; no edges counted
+     * for an adjacency-only program) and every iteration's changes summed;
+     * otherwise one line per iteration with cumulative counters (:540-569): vertex
+     * updates, and in-edges (in-memory program, out-edges disabled) or in- plus
+     * out-edges (edge-value program). delta[i]: the change logged in iteration i
+     * (0 for the in-memory program, which calls no log_change). */
+    void write_vertex_program_log(bool edge_values, const std::vector<double> &delta, int niters) {
+        const uint64_t nv = num_vertices(), ne = num_edges();
+        const bool engine_inmem = entry_->nshards == 1 && nv < 2ull * 40000000ull;
+        FILE *f = fopen((base_ + ".deltalog").c_str(), "w");
+        if (!f) return;
+        if (engine_inmem) {
+            double d = 0.0;
+            for (int i = 0; i < niters; ++i) d += delta[i];
+            fprintf(f, "%d,%lu,%lu,%lf\n", niters - 1, (unsigned long)(nv * niters),
+                    (unsigned long)(edge_values ? ne * niters : 0), d);
+        } else {
+            for (int i = 0; i < niters; ++i)
+                fprintf(f, "%d,%lu,%lu,%lf\n", i, (unsigned long)(nv * (i + 1)),
+                        (unsigned long)((edge_values ? 2 : 1) * ne * (i + 1)), delta[i]);
+        }
+        fclose(f);
+    }
+
 public:
     graphchi_engine(std::string base, int nshards, bool selective_scheduling, metrics &m)
         : base_(std::move(base)), nshards_(nshards), m_(m), membudget_mb_(get_option_int("membudget_mb", 1024)),
@@ -370,17 +398,13 @@ public:
                 for (uint32_t v = 0; v < nv; ++v) values[v] = (VertexDataType)r[v];
                 last = st.sweeps;
                 ctx_.last_residual = st.residual;
-                if (p.mode == GCG_PR_GS_EDGE) {
-                    /* the engine logs iteration 0 (the initialisation: every vertex and
-                     * its in- and out-edges, no change) before the sweeps */
-                    dl.insert(dl.begin(), 0.0);
-                    wl.insert(wl.begin(), {(uint64_t)nv, 2 * (uint64_t)num_edges()});
-                    for (int i = 1; i <= st.sweeps; ++i) {
-                        wl[2 * i] += (uint64_t)nv;
-                        wl[2 * i + 1] += 2 * (uint64_t)num_edges();
-                    }
-                    write_delta_log(dl, wl, st.sweeps + 1);
-                    ctx_.last_deltasum = dl[st.sweeps];
+                if (p.mode == GCG_PR_GS_EDGE || p.mode == GCG_PR_GS_EXACT) {
+                    /* iteration 0 (the initialisation) logs no change */
+                    std::vector<double> it_delta(1 + (size_t)st.sweeps, 0.0);
+                    if (p.mode == GCG_PR_GS_EDGE)
+                        for (int i = 0; i < st.sweeps; ++i) it_delta[1 + i] = dl[i];
+                    write_vertex_program_log(p.mode == GCG_PR_GS_EDGE, it_delta, st.sweeps + 1);
+                    ctx_.last_deltasum = it_delta.back();
                 } else if (logged && st.sweeps > 0) {
                     write_delta_log(dl, wl, st.sweeps);
                     ctx_.last_deltasum = dl[st.sweeps - 1];

@@ -103,6 +103,8 @@ def run_case(name, spec, tasks, store_full, merge=False):
                     opts["membudget_mb"] = budget
                 O.run_ref("pagerank", el, opts, THREADS)
                 put(f"pr_gs_{niters}_{P}_{budget}", O.read_vout(el, np.float32, nv))
+                rec[f"pr_gs_{niters}_{P}_{budget}_deltalog"] = np.frombuffer(open(el + ".deltalog", "rb").read(),
+                                                                            np.uint8)
         if "pr_edge" in tasks:
             # the edge-value program (pagerank.cpp:73-113): the app takes it when
             # num_vertices * 4 >= membudget; one exec thread keeps the delta sums in

@@ -134,3 +134,21 @@ def test_pagerank_app_edge_program_matches_reference_files(tmp_path):
     ref = [ln.split(",") for ln in bytes(g["pr_edge_5_4_1_deltalog"]).decode().split()]
     assert [r[:3] for r in got] == [r[:3] for r in ref]
     np.testing.assert_allclose([float(r[3]) for r in got], [float(r[3]) for r in ref], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("tag", ["pr_gs_4_1_0", "pr_gs_4_4_1", "pr_gs_6_2_0"])
+def test_pagerank_app_in_memory_program_matches_reference_files(tmp_path, tag):
+    # the in-memory program as the reference app ran it (niters, nshards, membudget
+    # from the tag): the .vout bit for bit and the .deltalog byte for byte (one line
+    # when the engine ran in its single-shard in-memory mode, one per iteration else)
+    g = np.load(os.path.join(ROOT, "tests", "golden", "rmat_s10_ef16_seed1.npz"))
+    s, d = O.rmat_numpy(10, 16 << 10, seed=1)
+    cs, cd = O.canonical_edges(s, d, symmetrise=False, dedup=True)
+    path = str(tmp_path / "g.el")
+    O.write_edgelist(path, cs, cd)
+    niters, P, budget = (int(x) for x in tag.split("_")[2:])
+    opts = [f"file={path}", f"niters={niters}", f"nshards={P}"] + ([f"membudget_mb={budget}"] if budget else [])
+    out = run("pagerank", *opts)
+    assert "in-memory mode" in out
+    assert np.array_equal(O.read_vout(path, np.float32)[: int(g["nv"])], g[tag])
+    assert open(path + ".deltalog", "rb").read() == bytes(g[tag + "_deltalog"])
