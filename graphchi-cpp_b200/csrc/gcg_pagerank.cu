@@ -245,7 +245,19 @@ __global__ void __launch_bounds__(256) k_pr_vertex(SweepArgs a, int sweep, int c
         for (int u = 0; u < VB; ++u) {
             const uint64_t i = (uint64_t)i0 + (uint64_t)u * nth;
             if (i < a.nnz) {
-                sum[u] = a.nzsum[i];
+                if (a.ntiers > 1) { /* the row's tier partial sums, in tier order */
+                    float t = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < MAX_TIERS; ++k) {
+                        if (k < (int)a.ntiers) {
+                            const uint32_t j = a.tier_idx[(uint64_t)k * a.nnz + i];
+                            if (j != GCG_NO_SOURCE) t += a.tier_sum[k][j];
+                        }
+                    }
+                    sum[u] = t;
+                } else {
+                    sum[u] = a.nzsum[i];
+                }
                 ro[u] = a.r_nz_old[i];
                 od[u] = a.od_nz[i];
                 cid[u] = a.nz_cidx[i];
@@ -380,6 +392,56 @@ __global__ void k_long_list(const uint4 *__restrict__ split, uint32_t nsplit, ui
     }
 }
 
+/* ---- source tiers ---------------------------------------------------------- */
+/* tier of each edge: k >= 1 when its relabelled source lies in [k w, (k+1) w)
+ * for k < ntiers, else 0 */
+__global__ void k_edge_tier(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
+                            uint32_t width, uint32_t ntiers, uint8_t *__restrict__ tier) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = newid[col[e]] / width;
+        tier[e] = (uint8_t)(k < ntiers ? k : 0u);
+    }
+}
+
+/* f[e] = (tier[e] == k) for e < ne, f[ne] = 0 (so the exclusive scan ends with the total) */
+__global__ void k_tier_flags(const uint8_t *__restrict__ tier, uint64_t ne, uint8_t k, uint32_t *__restrict__ f) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e <= ne; e += (uint64_t)gridDim.x * blockDim.x)
+        f[e] = e < ne && tier[e] == k ? 1u : 0u;
+}
+
+/* rows of tier k: a global nz row has tier-k edges when the scanned positions
+ * at its two ends differ */
+__global__ void k_tier_row_flags(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ nz_rows, uint32_t nnz,
+                                 const uint32_t *__restrict__ epos, uint32_t *__restrict__ rf) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        const uint32_t v = nz_rows[i];
+        rf[i] = epos[rowptr[v + 1]] > epos[rowptr[v]] ? 1u : 0u;
+    }
+}
+
+__global__ void k_tier_rows(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ nz_rows, uint32_t nnz,
+                            const uint32_t *__restrict__ epos, const uint32_t *__restrict__ rpos,
+                            uint32_t *__restrict__ idx, uint32_t *__restrict__ start) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
+        const uint32_t v = nz_rows[i];
+        const uint32_t b = epos[rowptr[v]];
+        if (epos[rowptr[v + 1]] > b) {
+            idx[i] = rpos[i];
+            start[rpos[i]] = b;
+        } else {
+            idx[i] = GCG_NO_SOURCE;
+        }
+    }
+}
+
+/* tier k's columns in the chunk layout, relative to the tier's first id */
+__global__ void k_tier_cols(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
+                            const uint8_t *__restrict__ tier, uint8_t k, uint32_t first,
+                            const uint32_t *__restrict__ epos, uint32_t *__restrict__ out) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x)
+        if (tier[e] == k) out[chunk_slot(epos[e])] = newid[col[e]] - first;
+}
+
 inline unsigned grid1d(uint64_t n, uint64_t cap_per_sm = 16) {
     uint64_t b = (n + 255) / 256;
     uint64_t cap = (uint64_t)num_sms() * cap_per_sm;
@@ -399,6 +461,45 @@ int pr_init_state(gcg_graph *g, float init, const float *init_dev, float *r, flo
     k_pr_init<<<grid1d(g->nv, 8), 256, 0, s>>>(g->nv, g->outdeg.get(), pl.newid.get(), init, init_dev, GCG_NO_SOURCE,
                                                r, c);
     k_pr_init_nz<<<grid1d(pl.nnz, 8), 256, 0, s>>>(pl.nnz, pl.nz_rows.get(), r, rnz);
+    GCG_LAUNCH_CHECK();
+    return GCG_OK;
+}
+
+/* Row structure of an edge array grouped by row (nrows non-empty rows starting
+ * at edge positions nz_start[], ne edges): the 1-bit-per-edge row-start bitmap,
+ * each 256-edge chunk's starting row, the rows crossing chunk boundaries and,
+ * among them, those spanning more than LONG_SPAN chunks. */
+static int build_segments(const uint32_t *nz_start, uint32_t nrows, uint64_t ne, cudaStream_t s, uint32_t &nchunks,
+                          dbuf<uint32_t> &head_bits, dbuf<uint32_t> &chunk_nz, dbuf<uint4> &split,
+                          dbuf<uint32_t> &long_split, uint32_t &nsplit, uint32_t &nlong) {
+    nchunks = (uint32_t)((ne + CH - 1) / CH);
+    nsplit = nlong = 0;
+    /* head bitmap covers whole chunks plus one spare word (read of the next chunk's first bit) */
+    const uint64_t words = ((uint64_t)nchunks * CH) / 32 + 8;
+    GCG_TRY(head_bits.alloc(words));
+    GCG_TRY(chunk_nz.alloc(std::max<uint32_t>(nchunks, 1)));
+    GCG_CUDA(cudaMemsetAsync(head_bits.get(), 0, words * 4, s));
+    if (!nrows) return split.alloc(1);
+    tbuf<uint32_t> flags, pos, total;
+    GCG_TRY(flags.alloc(nrows, s));
+    GCG_TRY(pos.alloc(nrows, s));
+    GCG_TRY(total.alloc(1, s));
+    k_head_bits<<<grid1d(nrows), 256, 0, s>>>(nz_start, nrows, head_bits.get());
+    k_chunk_nz<<<grid1d(nchunks), 256, 0, s>>>(nz_start, nrows, nchunks, chunk_nz.get());
+    k_split_flags<<<grid1d(nrows), 256, 0, s>>>(nz_start, nrows, ne, flags.get());
+    GCG_TRY(scan_u32(flags.get(), pos.get(), nrows, total.get(), s));
+    GCG_CUDA(cudaMemcpyAsync(&nsplit, total.get(), 4, cudaMemcpyDeviceToHost, s));
+    GCG_CUDA(cudaStreamSynchronize(s));
+    GCG_TRY(split.alloc(std::max<uint32_t>(nsplit, 1)));
+    k_split_list<<<grid1d(nrows), 256, 0, s>>>(nz_start, nrows, ne, pos.get(), split.get());
+    /* the long split rows, each summed by a block of the fix-up (any order) */
+    if (nsplit) {
+        GCG_CUDA(cudaMemsetAsync(total.get(), 0, 4, s));
+        GCG_TRY(long_split.alloc(nsplit));
+        k_long_list<<<grid1d(nsplit), 256, 0, s>>>(split.get(), nsplit, total.get(), long_split.get());
+        GCG_CUDA(cudaMemcpyAsync(&nlong, total.get(), 4, cudaMemcpyDeviceToHost, s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+    }
     GCG_LAUNCH_CHECK();
     return GCG_OK;
 }
@@ -427,40 +528,15 @@ int ensure_chunk_plan(gcg_graph *g) {
         return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
     p->nnz = nnz;
     p->nzero = nv - nnz;
-    /* head bitmap covers whole chunks plus one spare word (read of the next chunk's first bit) */
-    const uint64_t words = ((uint64_t)p->nchunks * CH) / 32 + 8;
     if (p->nz_rows.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_rows.alloc(std::max<uint32_t>(p->nzero, 1)) ||
-        p->od_nz.alloc(std::max<uint32_t>(nnz, 1)) ||
-        p->head_bits.alloc(words) || p->chunk_nz.alloc(std::max<uint32_t>(p->nchunks, 1)))
+        p->od_nz.alloc(std::max<uint32_t>(nnz, 1)))
         return bail(GCG_ERR_NOMEM);
     k_split_rows<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, pos.get(), p->nz_rows.get(), nz_start.get(),
                                             p->zero_rows.get());
-    cudaMemsetAsync(p->head_bits.get(), 0, words * 4, s);
-    if (nnz) {
-        k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), g->outdeg.get(), p->od_nz.get());
-        k_head_bits<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, p->head_bits.get());
-        k_chunk_nz<<<grid1d(p->nchunks), 256, 0, s>>>(nz_start.get(), nnz, p->nchunks, p->chunk_nz.get());
-        k_split_flags<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, ne, flags.get());
-        if ((st = scan_u32(flags.get(), pos.get(), nnz, total.get(), s))) return bail(st);
-        uint32_t nsplit = 0;
-        if (cudaMemcpyAsync(&nsplit, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess)
-            return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
-        p->nsplit = nsplit;
-        if (p->split.alloc(std::max<uint32_t>(nsplit, 1))) return bail(GCG_ERR_NOMEM);
-        k_split_list<<<grid1d(nnz), 256, 0, s>>>(nz_start.get(), nnz, ne, pos.get(), p->split.get());
-        /* the long split rows, each summed by a block of the fix-up (any order) */
-        if (nsplit) {
-            GCG_CUDA(cudaMemsetAsync(total.get(), 0, 4, s));
-            if (p->long_split.alloc(nsplit)) return bail(GCG_ERR_NOMEM);
-            k_long_list<<<grid1d(nsplit), 256, 0, s>>>(p->split.get(), nsplit, total.get(), p->long_split.get());
-            uint32_t nlong = 0;
-            if (cudaMemcpyAsync(&nlong, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess)
-                return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
-            p->nlong = nlong;
-        }
-    }
+    if (nnz) k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), g->outdeg.get(), p->od_nz.get());
+    if ((st = build_segments(nz_start.get(), nnz, ne, s, p->nchunks, p->head_bits, p->chunk_nz, p->split,
+                             p->long_split, p->nsplit, p->nlong)))
+        return bail(st);
     /* relabel sources by out-degree so the hottest contribs sit at ids [0, hub) */
     {
         tbuf<uint32_t> dmax;
@@ -495,6 +571,70 @@ int ensure_chunk_plan(gcg_graph *g) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bail(fail(GCG_ERR_CUDA, std::string("chunk plan: ") + cudaGetErrorString(e)));
     g->cplan = p;
+    return GCG_OK;
+}
+
+int ensure_tier_plan(gcg_graph *g, int ntiers, uint32_t width) {
+    GCG_TRY(ensure_chunk_plan(g));
+    ChunkPlan &pl = *g->cplan;
+    TierPlan &tp = pl.tiers;
+    if (tp.ntiers == ntiers && tp.width == width) return GCG_OK;
+    if (ntiers < 2 || ntiers > MAX_TIERS || width == 0 || (width & 3u))
+        return fail(GCG_ERR_INVALID, "source tiers: 2..4 tiers of a width that is a multiple of 4");
+    tp.ntiers = 0;
+    cudaStream_t s = g->stream;
+    const uint64_t ne = g->ne;
+    const uint32_t nnz = pl.nnz;
+    if (ne >= 0xFFFFFFFFull) return fail(GCG_ERR_UNSUPPORTED, "source tiers: too many edges");
+    tbuf<uint8_t> tier;
+    tbuf<uint32_t> epos, rflag, rpos, start, total;
+    GCG_TRY(tier.alloc(std::max<uint64_t>(ne, 1), s));
+    GCG_TRY(epos.alloc(ne + 1, s));
+    GCG_TRY(rflag.alloc(std::max<uint32_t>(nnz, 1), s));
+    GCG_TRY(rpos.alloc(std::max<uint32_t>(nnz, 1), s));
+    GCG_TRY(start.alloc(std::max<uint32_t>(nnz, 1), s));
+    GCG_TRY(total.alloc(1, s));
+    GCG_TRY(tp.idx.alloc((size_t)ntiers * std::max<uint32_t>(nnz, 1)));
+    if (ne)
+        k_edge_tier<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, pl.newid.get(), width, (uint32_t)ntiers,
+                                                   tier.get());
+    for (int k = 0; k < ntiers; ++k) {
+        EdgeTier &t = tp.t[k];
+        k_tier_flags<<<grid1d(ne + 1, 32), 256, 0, s>>>(tier.get(), ne, (uint8_t)k, epos.get());
+        GCG_TRY(scan_u32(epos.get(), epos.get(), ne + 1, total.get(), s));
+        uint32_t tne = 0;
+        GCG_CUDA(cudaMemcpyAsync(&tne, total.get(), 4, cudaMemcpyDeviceToHost, s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+        t.ne = tne;
+        t.first = k == 0 ? 0u : (uint32_t)k * width;
+        t.hub = k == 0 ? std::min(width, g->nv)
+                       : (t.first < g->nv ? std::min<uint32_t>(width, g->nv - t.first) : 0u); /* empty past nv */
+        uint32_t nrows = 0;
+        if (nnz) {
+            k_tier_row_flags<<<grid1d(nnz), 256, 0, s>>>(g->in_rowptr.get(), pl.nz_rows.get(), nnz, epos.get(),
+                                                        rflag.get());
+            GCG_TRY(scan_u32(rflag.get(), rpos.get(), nnz, total.get(), s));
+            GCG_CUDA(cudaMemcpyAsync(&nrows, total.get(), 4, cudaMemcpyDeviceToHost, s));
+            GCG_CUDA(cudaStreamSynchronize(s));
+            k_tier_rows<<<grid1d(nnz), 256, 0, s>>>(g->in_rowptr.get(), pl.nz_rows.get(), nnz, epos.get(), rpos.get(),
+                                                   tp.idx.get() + (size_t)k * nnz, start.get());
+        }
+        t.nrows = nrows;
+        GCG_TRY(build_segments(start.get(), nrows, tne, s, t.nchunks, t.head_bits, t.chunk_nz, t.split, t.long_split,
+                               t.nsplit, t.nlong));
+        const uint64_t slots = std::max<uint64_t>((uint64_t)t.nchunks * CH, CH);
+        GCG_TRY(t.col.alloc(slots));
+        GCG_CUDA(cudaMemsetAsync(t.col.get(), 0, slots * 4, s));
+        if (ne)
+            k_tier_cols<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, pl.newid.get(), tier.get(), (uint8_t)k,
+                                                       t.first, epos.get(), t.col.get());
+        GCG_TRY(t.nzsum.alloc(std::max<uint32_t>(nrows, 1)));
+        GCG_TRY(t.parts.alloc((size_t)2 * t.nchunks + 2));
+        GCG_LAUNCH_CHECK();
+    }
+    GCG_CUDA(cudaStreamSynchronize(s));
+    tp.ntiers = ntiers;
+    tp.width = width;
     return GCG_OK;
 }
 
@@ -612,7 +752,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     k_pr_init_nz<<<grid1d(pl.nnz, 8), 256, 0, s>>>(pl.nnz, pl.nz_rows.get(), r.get(), rnz.get());
     GCG_LAUNCH_CHECK();
 
-    SweepArgs a;
+    SweepArgs a{};
     a.col = pl.col_r.get();
     a.hub = std::min(pl.hub, pl.tune_hub);
     a.run = std::max(1u, pl.tune_run);
@@ -657,6 +797,40 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     }
     const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 32) + (int)pl.nlong; /* + a block per long row */
 
+    /* source tiers: one edge pass per tier, each with its tier's contributions in
+     * shared memory (tier 0: the hub plus every source past the last tier) */
+    const int ntiers = (pl.tune_tiers > 1 && hub_bytes > 0) ? (int)std::min<uint32_t>(pl.tune_tiers, MAX_TIERS) : 1;
+    SweepArgs at[MAX_TIERS];
+    int ge_t[MAX_TIERS], fg_t[MAX_TIERS];
+    if (ntiers > 1) {
+        GCG_TRY(ensure_tier_plan(g, ntiers, hub_bytes / 4u));
+        const TierPlan &tp = g->cplan->tiers;
+        a.ntiers = (uint32_t)ntiers;
+        a.tier_idx = tp.idx.get();
+        for (int k = 0; k < ntiers; ++k) {
+            const EdgeTier &t = tp.t[k];
+            SweepArgs &b = at[k];
+            b = a;
+            b.col = t.col.get();
+            b.heads = (const uint8_t *)t.head_bits.get();
+            b.chunk_nz = t.chunk_nz.get();
+            b.split = t.split.get();
+            b.long_split = t.long_split.get();
+            b.nlong = t.nlong;
+            b.nsplit = t.nsplit;
+            b.nchunks = t.nchunks;
+            b.ne = t.ne;
+            b.hub = t.hub;
+            b.nzsum = t.nzsum.get();
+            b.head_part = t.parts.get();
+            b.tail_part = t.parts.get() + t.nchunks + 1;
+            a.tier_sum[k] = t.nzsum.get();
+            ge_t[k] = std::max(1, (int)std::min<uint64_t>((uint64_t)edge_grid(hub_bytes),
+                                                        (t.nchunks + 32 * run - 1) / (32 * run)));
+            fg_t[k] = (int)grid1d(std::max<uint32_t>(t.nsplit, 1), 32) + (int)t.nlong;
+        }
+    }
+
     cudaEvent_t ev0, ev1;
     GCG_CUDA(cudaEventCreate(&ev0));
     GCG_CUDA(cudaEventCreate(&ev1));
@@ -681,19 +855,32 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
             a.c_new = c.get() + (size_t)((sw + 1) & 1) * cstride;
             a.r_nz_old = rnz.get() + (size_t)(sw & 1) * pl.nnz;
             a.r_nz_new = rnz.get() + (size_t)((sw + 1) & 1) * pl.nnz;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
             if (time_sweeps) {
-                cudaEvent_t e0, e1;
                 cudaEventCreate(&e0);
                 cudaEventCreate(&e1);
                 cudaEventRecord(e0, s);
-                launch_edges(ge, hub_bytes, s, a);
-                cudaEventRecord(e1, s);
-                sweep_ev.push_back(e0);
-                sweep_ev.push_back(e1);
+            }
+            if (ntiers > 1) { /* every tier's edge pass, then every tier's fix-up */
+                for (int k = 0; k < ntiers; ++k) {
+                    at[k].c_old = a.c_old + g->cplan->tiers.t[k].first;
+                    at[k].tex_old = k == 0 ? a.tex_old : 0ull;
+                    at[k].done = a.done;
+                    launch_edges(ge_t[k], hub_bytes, s, at[k]);
+                }
             } else {
                 launch_edges(ge, hub_bytes, s, a);
             }
-            launch_pdl(k_pr_fix, fg, 256, 0, s, a);
+            if (time_sweeps) {
+                cudaEventRecord(e1, s);
+                sweep_ev.push_back(e0);
+                sweep_ev.push_back(e1);
+            }
+            if (ntiers > 1) {
+                for (int k = 0; k < ntiers; ++k) launch_pdl(k_pr_fix, fg_t[k], 256, 0, s, at[k]);
+            } else {
+                launch_pdl(k_pr_fix, fg, 256, 0, s, a);
+            }
             launch_pdl(k_pr_vertex, gv, 256, 0, s, a, sw, sw < 2 ? 1 : 0);
         }
         launched += n;
@@ -774,7 +961,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         stats->device_ms = ms;
         stats->sweep_kernel_ms = sweep_ms;
         stats->timed_sweeps = timed;
-        stats->kernel_launches = 1 + 3 * launched;
+        stats->kernel_launches = 1 + (2 * ntiers + 1) * launched;
     }
     return GCG_OK;
 }
@@ -809,6 +996,21 @@ int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_r
     GCG_TRY(ensure_chunk_plan(g));
     g->cplan->tune_hub = hub_entries;
     g->cplan->tune_run = chunk_run;
+    return GCG_OK;
+}
+
+int gcg_pagerank_set_tiers(gcg_graph *g, uint32_t tiers) {
+    if (!g) return fail(GCG_ERR_INVALID, "gcg_pagerank_set_tiers: null graph");
+    if (tiers < 1 || tiers > (uint32_t)MAX_TIERS) return fail(GCG_ERR_INVALID, "gcg_pagerank_set_tiers: tiers must be 1..4");
+    GCG_TRY(ensure_chunk_plan(g));
+    g->cplan->tune_tiers = tiers;
+    return GCG_OK;
+}
+
+int gcg_pagerank_get_tiers(gcg_graph *g, uint32_t *tiers) {
+    if (!g || !tiers) return fail(GCG_ERR_INVALID, "gcg_pagerank_get_tiers: null argument");
+    GCG_TRY(ensure_chunk_plan(g));
+    *tiers = g->cplan->tune_tiers;
     return GCG_OK;
 }
 

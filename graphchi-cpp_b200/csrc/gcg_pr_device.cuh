@@ -68,6 +68,12 @@ struct SweepArgs {
     uint32_t run;    /* edge kernel: each warp takes runs of this many consecutive chunks (>= 1) */
     double *delta_log; /* optional: per sweep, sum |r' - r| (FP64) */
     unsigned long long tex_old; /* texture object over c_old (edge kernel's texture-path gathers) */
+    /* source tiers (vertex kernel): a row's sum is the sum over tiers k of
+     * tier_sum[k][tier_idx[k * nnz + i]] (entries equal to GCG_NO_SOURCE: no
+     * in-edge of the row in that tier), tiers added in order; ntiers <= 1: nzsum */
+    uint32_t ntiers;
+    const uint32_t *tier_idx;
+    const float *tier_sum[4];
 };
 
 /* Column layout of a chunk. Lane l owns the 8 consecutive edges 8l..8l+7 of a
@@ -294,8 +300,35 @@ __device__ __forceinline__ float long_row_sum_warp(const float *head_part, uint3
     return t;
 }
 
+/* Source tiers of the edge phase. The sources (relabelled by out-degree) are cut
+ * into tiers of `width` ids: tier k >= 1 holds the edges whose source lies in
+ * [k * width, (k + 1) * width), tier 0 every other edge (the hub [0, width) and
+ * the sources past the last tier). Each tier is its own edge array grouped by
+ * row (columns relative to the tier's first id) with its own chunk structure,
+ * so its edge pass keeps the tier's contributions in shared memory: tier k >= 1
+ * needs no global gathers at all. A row's sum is its tiers' partial sums added
+ * in tier order. */
+constexpr int MAX_TIERS = 4;
+struct EdgeTier {
+    uint64_t ne = 0;
+    uint32_t nchunks = 0, nrows = 0, nsplit = 0, nlong = 0;
+    uint32_t first = 0; /* relabelled id of column value 0 */
+    uint32_t hub = 0;   /* contributions [first, first + hub) staged in shared memory */
+    dbuf<uint32_t> col, head_bits, chunk_nz, long_split;
+    dbuf<uint4> split;
+    dbuf<float> nzsum, parts;
+};
+struct TierPlan {
+    int ntiers = 0; /* built for this many tiers (0: not built) */
+    uint32_t width = 0;
+    EdgeTier t[MAX_TIERS];
+    dbuf<uint32_t> idx; /* ntiers x nnz: each row's index in tier k's rows, or GCG_NO_SOURCE */
+};
+
 struct ChunkPlan {
     PrWork work;
+    TierPlan tiers;
+    uint32_t tune_tiers = 1; /* source tiers of the edge phase (1: one pass) */
     uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
     dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
     dbuf<uint4> split;
@@ -311,6 +344,8 @@ struct ChunkPlan {
 
 /* builds (once per graph) the chunk plan and the out-degree relabelling */
 int ensure_chunk_plan(gcg_graph *g);
+/* builds (or keeps) the plan's source tiers for ntiers tiers of width ids */
+int ensure_tier_plan(gcg_graph *g, int ntiers, uint32_t width);
 int pr_init_state(gcg_graph *g, float init, const float *init_dev, float *r, float *c, float *rnz);
 
 /* separate round-to-nearest multiply and add (no FMA contraction), as the

@@ -249,6 +249,18 @@ int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_r
 int gcg_pagerank_get_config(gcg_graph *g, uint32_t *hub_entries, uint32_t *chunk_run);
 int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint32_t *chunk_run, double *ms_per_sweep);
 
+/* Source tiers of the Jacobi edge phase (no counterpart in the reference; the
+ * answers agree within float rounding: a row's sum is formed per tier, then the
+ * tiers' partial sums are added in tier order). With `tiers` = t > 1 the
+ * sources, relabelled by out-degree, are cut into tiers of hub_entries ids;
+ * tier k >= 1 (ids [k h, (k+1) h)) gets its own edge array and edge pass with
+ * its contributions in shared memory, tier 0 keeps the hub and every source past
+ * the last tier. It trades one edge pass per tier for fewer scattered global
+ * gathers. 1..4; 1 = one pass (the default). The tier arrays are built on the
+ * first solve that uses them (one more copy of the column array). */
+int gcg_pagerank_set_tiers(gcg_graph *g, uint32_t tiers);
+int gcg_pagerank_get_tiers(gcg_graph *g, uint32_t *tiers);
+
 /* Batched personalised PageRank (the engine's addition beside the reference's
  * one-vector runs of example_apps/pagerank.cpp): nsources sources solved together
  * as a vertex-major rank matrix. For source s: r_s starts at the indicator of

@@ -322,3 +322,30 @@ def test_scale20_cc_tc_bitexact(name):
         assert total == int(z["tc_total"])
         check(z, "tc_per_rank", per)
         check(z, "tc_vertexmap", vm)
+
+
+@pytest.mark.parametrize("scale,hub", [(14, 1024), (16, 4096)])
+def test_pagerank_source_tiers_vs_oracle(scale, hub):
+    """The edge phase cut into source tiers (one pass per tier of `hub` relabelled
+    ids, each tier's contributions in shared memory): fixed sweeps and converged
+    answers against the oracle for 1 to 4 tiers, tiers past the last vertex
+    included."""
+    s, d = O.rmat_numpy(scale, 16 << scale, seed=21)
+    go = O.OracleGraph(s, d)
+    ref, _, _ = go.pagerank_jacobi(max_sweeps=12)
+    f64, _ = go.pagerank_jacobi_f64(max_sweeps=3000, tol=1e-12)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=False) as g:
+        g.pagerank_config(hub_entries=hub)
+        base, _ = g.pagerank(max_sweeps=12)
+        for t in (1, 2, 3, 4):
+            assert g.pagerank_tiers(t) == t
+            r, st = g.pagerank(max_sweeps=12)
+            assert st.kernel_launches == 1 + (2 * t + 1) * 12
+            assert nl1(r, ref) <= 1e-6 and nl1(r, base) <= 1e-6, t
+            r, st = g.pagerank(max_sweeps=1000, tol=1e-8)
+            assert st.converged == 1 and nl1(r, f64) <= 1e-6, t
+        # a tier width past the vertex count leaves tiers 2.. empty
+        g.pagerank_config(hub_entries=(g.num_vertices + 4) & ~3)
+        g.pagerank_tiers(3)
+        r, st = g.pagerank(max_sweeps=12)
+        assert nl1(r, ref) <= 1e-6
