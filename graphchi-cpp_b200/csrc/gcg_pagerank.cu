@@ -1036,29 +1036,48 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
     gcg_pr_params_default(&p);
     p.max_sweeps = sweeps;
     p.tol = 0.0;
-    p.flags = GCG_PR_TIME_SWEEPS;
     tbuf<float> out;
     GCG_TRY(out.alloc(std::max<uint32_t>(g->nv, 1), g->stream));
+    /* each candidate: the device time of `sweeps` whole sweeps (edge pass(es),
+     * fix-ups, vertex pass), best of two runs (the first also warms caches) */
+    auto time_config = [&](double &t) -> int {
+        t = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            gcg_pr_stats st;
+            GCG_TRY(pagerank_jacobi(g, &p, out.get(), &st));
+            if (st.sweeps > 0) t = std::min(t, st.device_ms / st.sweeps);
+        }
+        return GCG_OK;
+    };
     double best = 1e300;
-    uint32_t bh = std::min(pl.hub, HUB_DEFAULT), br = RUN_DEFAULT;
+    uint32_t bh = std::min(pl.hub, HUB_DEFAULT), br = RUN_DEFAULT, bt = 1;
+    pl.tune_tiers = 1;
     for (uint32_t h : hubs)
         for (uint32_t r : runs) {
             pl.tune_hub = h;
             pl.tune_run = r;
-            double t = 1e300;
-            for (int rep = 0; rep < 2; ++rep) { /* the first run warms caches */
-                gcg_pr_stats st;
-                GCG_TRY(pagerank_jacobi(g, &p, out.get(), &st));
-                if (st.timed_sweeps > 0) t = std::min(t, st.sweep_kernel_ms / st.timed_sweeps);
-            }
+            double t;
+            GCG_TRY(time_config(t));
             if (t < best) {
                 best = t;
                 bh = h;
                 br = r;
             }
         }
+    /* then source tiers of the chosen hub width, when the graph has sources past it */
     pl.tune_hub = bh;
     pl.tune_run = br;
+    const uint32_t w = std::min(pl.hub, bh);
+    for (uint32_t tiers = 2; w > 0 && tiers <= (uint32_t)MAX_TIERS && (uint64_t)(tiers - 1) * w < g->nv; ++tiers) {
+        pl.tune_tiers = tiers;
+        double t;
+        GCG_TRY(time_config(t));
+        if (t < best) {
+            best = t;
+            bt = tiers;
+        }
+    }
+    pl.tune_tiers = bt;
     if (hub_entries) *hub_entries = bh;
     if (chunk_run) *chunk_run = br;
     if (ms_per_sweep) *ms_per_sweep = best;

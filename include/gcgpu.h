@@ -242,9 +242,11 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * (1 = warps stride chunk by chunk). Default: 41728 entries (the largest hub
  * that leaves the SM its 164 KB shared-memory carve-out, so L1 keeps ~92 KB) and
  * chunk_run 1, the fastest measured at R-MAT scale 24. gcg_pagerank_autotune
- * times `sweeps` fixed sweeps of each candidate (hub entries {0, 16384, 32768,
- * 41728, 49152, the plan's} x runs {1, 2, 4, 16}), keeps the fastest for later
- * calls on this graph and reports it (outputs may be NULL). */
+ * times `sweeps` fixed sweeps (the whole sweep, device time) of each candidate
+ * (hub entries {0, 16384, 32768, 41728, 49152, the plan's} x runs {1, 2, 4, 16},
+ * then 2..4 source tiers of the chosen hub, gcg_pagerank_set_tiers), keeps the
+ * fastest for later calls on this graph and reports it (outputs may be NULL;
+ * gcg_pagerank_get_tiers gives the tier count chosen). */
 int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_run);
 int gcg_pagerank_get_config(gcg_graph *g, uint32_t *hub_entries, uint32_t *chunk_run);
 int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint32_t *chunk_run, double *ms_per_sweep);
