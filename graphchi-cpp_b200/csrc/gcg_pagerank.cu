@@ -113,12 +113,7 @@ __device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol
  * object over c_old) instead of plain loads. The edge kernel is bound by the
  * L1TEX tag stage on these scattered gathers; at R-MAT scale 24 texture fetches
  * finish a launch ~6 % sooner than the same gathers as loads (same values). */
-/* GM: how the gathers that miss the hub are made. 0: plain loads (kept in L2);
- * 1: the texture path; 2: L1-partitioned loads: sources [hub, l1_end) are loaded
- * with L1 evict-last priority and every other global load of the kernel bypasses
- * L1, so L1 serves as a second hub for the next-hottest sources (a hit costs no
- * request to L2). */
-template <int GM>
+template <bool TEX>
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     pdl_wait();
     pdl_launch_next();
@@ -142,24 +137,12 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     if (ch < end) load_chunk(a, (uint32_t)ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
     while (ch < end) {
         float val[EPL];
-        if (GM == 1) {
+        if (TEX) {
 #pragma unroll
             for (int j = 0; j < EPL; ++j) {
                 const uint32_t x = col[j];
                 float v = 0.0f;
                 if ((uint32_t)j < nvalid) v = x < a.hub ? s_hub[x] : tex1Dfetch<float>(a.tex_old, (int)x);
-                val[j] = v;
-            }
-        } else if (GM == 2) {
-#pragma unroll
-            for (int j = 0; j < EPL; ++j) {
-                const uint32_t x = col[j];
-                float v = 0.0f;
-                if ((uint32_t)j < nvalid) {
-                    if (x < a.hub) v = s_hub[x];
-                    else if (x < a.l1_end) v = ld_l1keep_f32(a.c_old + x, pol_keep);
-                    else v = ld_l1skip_f32(a.c_old + x, pol_keep);
-                }
                 val[j] = v;
             }
         } else {
@@ -674,24 +657,21 @@ static void launch_pdl(void (*kern)(K...), int grid, int block, size_t smem, cud
 
 /* one CTA of EDGE_THREADS per SM (the hub cache takes most of shared memory) */
 static void launch_edges(int ge, uint32_t hub_bytes, cudaStream_t s, const SweepArgs &a) {
-    if (a.l1_end > a.hub)
-        launch_pdl(k_pr_edges<2>, ge, EDGE_THREADS, hub_bytes, s, a);
-    else if (a.tex_old)
-        launch_pdl(k_pr_edges<1>, ge, EDGE_THREADS, hub_bytes, s, a);
+    if (a.tex_old)
+        launch_pdl(k_pr_edges<true>, ge, EDGE_THREADS, hub_bytes, s, a);
     else
-        launch_pdl(k_pr_edges<0>, ge, EDGE_THREADS, hub_bytes, s, a);
+        launch_pdl(k_pr_edges<false>, ge, EDGE_THREADS, hub_bytes, s, a);
 }
 
 static int edge_grid(uint32_t hub_bytes) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_pr_edges<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
-        cudaFuncSetAttribute(k_pr_edges<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
-        cudaFuncSetAttribute(k_pr_edges<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
+        cudaFuncSetAttribute(k_pr_edges<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
+        cudaFuncSetAttribute(k_pr_edges<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4));
         attr = true;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_edges<0>, EDGE_THREADS, hub_bytes) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_edges<false>, EDGE_THREADS, hub_bytes) != cudaSuccess ||
         per_sm <= 0) {
         cudaGetLastError();
         per_sm = 1;
@@ -775,7 +755,6 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     SweepArgs a{};
     a.col = pl.col_r.get();
     a.hub = std::min(pl.hub, pl.tune_hub);
-    a.l1_end = pl.tune_l1 ? (uint32_t)std::min<uint64_t>((uint64_t)a.hub + pl.tune_l1, nv) : 0u;
     a.run = std::max(1u, pl.tune_run);
     a.nz_cidx = pl.nz_cidx.get();
     a.zero_cidx = pl.zero_cidx.get();
@@ -886,7 +865,6 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
                 for (int k = 0; k < ntiers; ++k) {
                     at[k].c_old = a.c_old + g->cplan->tiers.t[k].first;
                     at[k].tex_old = k == 0 ? a.tex_old : 0ull;
-                    at[k].l1_end = k == 0 ? a.l1_end : 0u;
                     at[k].done = a.done;
                     launch_edges(ge_t[k], hub_bytes, s, at[k]);
                 }
@@ -1018,20 +996,6 @@ int gcg_pagerank_set_config(gcg_graph *g, uint32_t hub_entries, uint32_t chunk_r
     GCG_TRY(ensure_chunk_plan(g));
     g->cplan->tune_hub = hub_entries;
     g->cplan->tune_run = chunk_run;
-    return GCG_OK;
-}
-
-int gcg_pagerank_set_l1_sources(gcg_graph *g, uint32_t entries) {
-    if (!g) return fail(GCG_ERR_INVALID, "gcg_pagerank_set_l1_sources: null graph");
-    GCG_TRY(ensure_chunk_plan(g));
-    g->cplan->tune_l1 = entries;
-    return GCG_OK;
-}
-
-int gcg_pagerank_get_l1_sources(gcg_graph *g, uint32_t *entries) {
-    if (!g || !entries) return fail(GCG_ERR_INVALID, "gcg_pagerank_get_l1_sources: null argument");
-    GCG_TRY(ensure_chunk_plan(g));
-    *entries = g->cplan->tune_l1;
     return GCG_OK;
 }
 

@@ -37,29 +37,6 @@ __device__ __forceinline__ float ld_keep_f32(const float *p, uint64_t pol) {
     asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
     return r;
 }
-/* the same gather, kept in L1 with priority over everything else loaded there */
-__device__ __forceinline__ float ld_l1keep_f32(const float *p, uint64_t pol) {
-    float r;
-    asm("ld.global.nc.L1::evict_last.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
-    return r;
-}
-/* the same gather, not allocated in L1 */
-__device__ __forceinline__ float ld_l1skip_f32(const float *p, uint64_t pol) {
-    float r;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
-    return r;
-}
-/* streamed plan data (head bitmap bytes, chunk starts): not allocated in L1 */
-__device__ __forceinline__ uint32_t ld_stream_u8(const uint8_t *p) {
-    uint32_t r;
-    asm("ld.global.nc.L1::no_allocate.u8 %0, [%1];" : "=r"(r) : "l"(p));
-    return r;
-}
-__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p) {
-    uint32_t r;
-    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(r) : "l"(p));
-    return r;
-}
 
 /* ---- sweep kernels ------------------------------------------------------ */
 struct SweepArgs {
@@ -97,9 +74,6 @@ struct SweepArgs {
     uint32_t ntiers;
     const uint32_t *tier_idx;
     const float *tier_sum[4];
-    /* edge kernel, L1-partitioned gathers: sources [hub, l1_end) are loaded to
-     * stay in L1, sources from l1_end on bypass it (0: texture or plain gathers) */
-    uint32_t l1_end;
 };
 
 /* Column layout of a chunk. Lane l owns the 8 consecutive edges 8l..8l+7 of a
@@ -130,8 +104,8 @@ __device__ __forceinline__ void load_chunk(const A &a, uint32_t ch, uint32_t lan
         for (int j = 0; j < EPL; ++j)
             if ((uint32_t)j >= nvalid) col[j] = 0u;
     }
-    flags = nvalid ? (ld_stream_u8(a.heads + (e >> 3)) & ((1u << nvalid) - 1u)) : 0u;
-    base = ld_stream_u32(a.chunk_nz + ch);
+    flags = nvalid ? ((uint32_t)a.heads[e >> 3] & ((1u << nvalid) - 1u)) : 0u;
+    base = a.chunk_nz[ch];
 }
 
 /* L2-coherent load (no non-coherent texture path) for data that the same
@@ -366,9 +340,6 @@ struct ChunkPlan {
     /* launch configuration of the edge kernel (gcg_pagerank_autotune):
      * shared-memory hub entries (capped at hub) and chunks per warp run */
     uint32_t tune_hub = HUB_DEFAULT, tune_run = RUN_DEFAULT;
-    /* sources past the hub whose gathers are kept in L1 (0: none; the other
-     * gathers then go through the texture path) */
-    uint32_t tune_l1 = 0;
 };
 
 /* builds (once per graph) the chunk plan and the out-degree relabelling */

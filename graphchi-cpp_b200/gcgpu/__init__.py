@@ -51,8 +51,7 @@ EXPORTED = [
     "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
-    "gcg_pagerank_set_tiers", "gcg_pagerank_get_tiers", "gcg_pagerank_set_l1_sources",
-    "gcg_pagerank_get_l1_sources",
+    "gcg_pagerank_set_tiers", "gcg_pagerank_get_tiers",
     "gcg_connected_components_ex", "gcg_graph_get_device_view", "gcg_graph_add_edges", "gcg_graph_delete_edges",
     "gcg_mlp_create", "gcg_mlp_free", "gcg_mlp_get", "gcg_mlp_set", "gcg_mlp_fit_normalisation",
     "gcg_warm_features", "gcg_mlp_forward", "gcg_mlp_gradient", "gcg_mlp_train_params_default", "gcg_mlp_train",
@@ -150,8 +149,6 @@ _pr_set_config = _sig("gcg_pagerank_set_config", _i, _vp, _u32, _u32)
 _pr_get_config = _sig("gcg_pagerank_get_config", _i, _vp, C.POINTER(_u32), C.POINTER(_u32))
 _pr_set_tiers = _sig("gcg_pagerank_set_tiers", _i, _vp, _u32)
 _pr_get_tiers = _sig("gcg_pagerank_get_tiers", _i, _vp, C.POINTER(_u32))
-_pr_set_l1 = _sig("gcg_pagerank_set_l1_sources", _i, _vp, _u32)
-_pr_get_l1 = _sig("gcg_pagerank_get_l1_sources", _i, _vp, C.POINTER(_u32))
 _pr_autotune = _sig("gcg_pagerank_autotune", _i, _vp, _i, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(C.c_double))
 _ppr = _sig("gcg_ppr_batched", _i, _vp, _vp, _u32, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
 _batch_create = _sig("gcg_batch_create", _i, C.POINTER(_vp), _u32, C.POINTER(_vp))
@@ -361,14 +358,6 @@ class Graph:
             check(_pr_set_tiers(self._h, int(tiers)))
         t = _u32(0)
         check(_pr_get_tiers(self._h, C.byref(t)))
-        return t.value
-
-    def pagerank_l1_sources(self, entries=None):
-        """Sets (when given) and returns the sources kept in L1 after the hub (0: texture gathers)."""
-        if entries is not None:
-            check(_pr_set_l1(self._h, int(entries)))
-        t = _u32(0)
-        check(_pr_get_l1(self._h, C.byref(t)))
         return t.value
 
     def pagerank_autotune(self, sweeps=8):

@@ -263,15 +263,6 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
 int gcg_pagerank_set_tiers(gcg_graph *g, uint32_t tiers);
 int gcg_pagerank_get_tiers(gcg_graph *g, uint32_t *tiers);
 
-/* L1 as a second contribution cache of the Jacobi edge kernel (no counterpart
- * in the reference; results do not depend on it): with entries > 0 the gathers
- * of the next `entries` sources after the shared-memory hub (by out-degree
- * rank) are loaded with L1 evict-last priority and every other global load of
- * the kernel bypasses L1, so those sources stay in each SM's L1 (a hit sends no
- * request to L2); with 0 the gathers past the hub go through the texture path. */
-int gcg_pagerank_set_l1_sources(gcg_graph *g, uint32_t entries);
-int gcg_pagerank_get_l1_sources(gcg_graph *g, uint32_t *entries);
-
 /* Batched personalised PageRank (the engine's addition beside the reference's
  * one-vector runs of example_apps/pagerank.cpp): nsources sources solved together
  * as a vertex-major rank matrix. For source s: r_s starts at the indicator of
