@@ -799,11 +799,13 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
 
     /* source tiers: one edge pass per tier, each with its tier's contributions in
      * shared memory (tier 0: the hub plus every source past the last tier) */
-    const int ntiers = (pl.tune_tiers > 1 && hub_bytes > 0) ? (int)std::min<uint32_t>(pl.tune_tiers, MAX_TIERS) : 1;
+    const uint32_t tier_width = (hub_bytes / 4u) & ~3u; /* a multiple of 4: tier hubs load as float4 */
+    const int ntiers =
+        (pl.tune_tiers > 1 && tier_width > 0) ? (int)std::min<uint32_t>(pl.tune_tiers, MAX_TIERS) : 1;
     SweepArgs at[MAX_TIERS];
     int ge_t[MAX_TIERS], fg_t[MAX_TIERS];
     if (ntiers > 1) {
-        GCG_TRY(ensure_tier_plan(g, ntiers, hub_bytes / 4u));
+        GCG_TRY(ensure_tier_plan(g, ntiers, tier_width));
         const TierPlan &tp = g->cplan->tiers;
         a.ntiers = (uint32_t)ntiers;
         a.tier_idx = tp.idx.get();
@@ -1067,7 +1069,7 @@ int gcg_pagerank_autotune(gcg_graph *g, int sweeps, uint32_t *hub_entries, uint3
     /* then source tiers of the chosen hub width, when the graph has sources past it */
     pl.tune_hub = bh;
     pl.tune_run = br;
-    const uint32_t w = std::min(pl.hub, bh);
+    const uint32_t w = std::min(pl.hub, bh) & ~3u;
     for (uint32_t tiers = 2; w > 0 && tiers <= (uint32_t)MAX_TIERS && (uint64_t)(tiers - 1) * w < g->nv; ++tiers) {
         pl.tune_tiers = tiers;
         double t;

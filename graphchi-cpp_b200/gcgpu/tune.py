@@ -1,0 +1,68 @@
+"""Launch-configuration report of the Jacobi PageRank edge phase on a seeded
+R-MAT graph: for each configuration, the edge phase and the whole sweep per
+sweep (CUDA events on the graph's stream, best of three 20-sweep runs) and the
+edge phase's share of the HBM roofline (8E + 16V bytes per sweep against the
+measured copy bandwidth in MEASURED_PEAKS.json, else 6650 GB/s). Every
+configuration computes the same sums in the same order except source tiers
+(tiers > 1), whose rows add per-tier partial sums.
+
+    python -m gcgpu.tune --scale 24 [--tiers 1 2 3 4] [--hub 41728 32768]
+
+(run with graphchi-cpp_b200 on PYTHONPATH)."""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+
+def peak_gbs():
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    try:
+        with open(os.path.join(root, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def main():
+    import torch
+    import gcgpu
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scale", type=int, nargs="+", default=[24])
+    ap.add_argument("--ef", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--hub", type=int, nargs="+", default=[41728])
+    ap.add_argument("--tiers", type=int, nargs="+", default=[1])
+    args = ap.parse_args()
+    peak = peak_gbs()
+    for scale in args.scale:
+        m = args.ef << scale
+        s = torch.empty(m, dtype=torch.int32, device="cuda")
+        d = torch.empty_like(s)
+        gcgpu.generate_rmat(scale, m, 0.57, 0.19, 0.19, seed=args.seed, src=s, dst=d)
+        g = gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=False)
+        del s, d
+        torch.cuda.empty_cache()
+        out = torch.empty(g.num_vertices, dtype=torch.float32, device="cuda")
+        E, V = g.num_edges, g.num_vertices
+        for hub in args.hub:
+            for t in args.tiers:
+                g.pagerank_config(hub, 1)
+                g.pagerank_tiers(t)
+                g.pagerank(max_sweeps=4, out=out)
+                best = None
+                for _ in range(3):
+                    _, st = g.pagerank(max_sweeps=20, out=out, time_sweeps=True)
+                    e = st.sweep_kernel_ms / st.timed_sweeps
+                    if best is None or e < best[0]:
+                        best = (e, st.device_ms / st.sweeps)
+                print(json.dumps({"scale": scale, "vertices": V, "edges": E, "hub": hub, "tiers": t,
+                                  "edge_phase_us": round(best[0] * 1e3, 1), "sweep_us": round(best[1] * 1e3, 1),
+                                  "edge_frac_of_hbm": round((8 * E + 16 * V) / best[0] / 1e6 / peak, 3)}),
+                      flush=True)
+        g.free()
+
+
+if __name__ == "__main__":
+    main()

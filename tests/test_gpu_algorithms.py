@@ -239,7 +239,11 @@ def test_pagerank_launch_configs_and_autotune_keep_results():
     hub, run, ms = g.pagerank_autotune(sweeps=3)
     assert ms > 0 and run in (1, 2, 4, 16) and g.pagerank_config() == (hub, run)
     r, _ = g.pagerank(max_sweeps=20)
-    assert np.array_equal(r, ref)
+    if g.pagerank_tiers() == 1:
+        assert np.array_equal(r, ref)
+    else:  # source tiers add each row's tier sums: float rounding may differ
+        assert nl1(r, ref) <= 1e-6
+    g.pagerank_tiers(1)
     with pytest.raises(gcgpu.GcgError):
         g.pagerank_config(hub, 0)
 
