@@ -164,31 +164,28 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
  * each lane finishes its own row when it spans few chunks, and the warp sums the
  * partials of each long (hub) row cooperatively: lane-strided partial sums, then
  * a fixed xor-shuffle tree, so the order is fixed. */
-/* Blocks [0, nlong) take one long row each (a warp per group of the fixed
- * long-row order); the other blocks take the short rows, one per lane, in
- * chunk order. */
+/* Blocks [0, nlb) take the long rows, one warp per row (the fixed long-row
+ * order: LONG_GROUPS lane-strided groups, each reduced by an xor tree, added in
+ * group order); the other blocks take the short rows, one per lane, in chunk
+ * order. */
+constexpr uint32_t FIX_WARPS = 8; /* 256-thread blocks */
 __global__ void __launch_bounds__(256) k_pr_fix(SweepArgs a) {
     pdl_wait();
     pdl_launch_next();
     if (*(volatile const int *)a.done) return;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    static_assert(LONG_GROUPS == 256 / 32, "one warp per group");
-    if (blockIdx.x < a.nlong) {
-        __shared__ float s_grp[LONG_GROUPS];
-        const uint4 sp = a.split[a.long_split[blockIdx.x]];
-        const float g = long_row_group<false>(a.head_part, sp.y, sp.z, (int)warp, lane);
-        if (lane == 0) s_grp[warp] = g;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float t = 0.0f;
-#pragma unroll
-            for (int w = 0; w < LONG_GROUPS; ++w) t += s_grp[w];
-            a.nzsum[sp.x] = a.tail_part[sp.y] + t;
+    const uint32_t nlb = (a.nlong + FIX_WARPS - 1) / FIX_WARPS;
+    if (blockIdx.x < nlb) {
+        const uint32_t r = blockIdx.x * FIX_WARPS + warp;
+        if (r < a.nlong) {
+            const uint4 sp = a.split[a.long_split[r]];
+            const float t = long_row_sum_warp<false>(a.head_part, sp.y, sp.z, lane);
+            if (lane == 0) a.nzsum[sp.x] = a.tail_part[sp.y] + t;
         }
         return;
     }
-    const uint32_t nwarps = ((gridDim.x - a.nlong) * blockDim.x) >> 5;
-    for (uint32_t wb = (((blockIdx.x - a.nlong) * blockDim.x + threadIdx.x) >> 5) * 32u; wb < a.nsplit;
+    const uint32_t nwarps = ((gridDim.x - nlb) * blockDim.x) >> 5;
+    for (uint32_t wb = (((blockIdx.x - nlb) * blockDim.x + threadIdx.x) >> 5) * 32u; wb < a.nsplit;
          wb += nwarps * 32u) {
         const uint32_t k = wb + lane;
         if (k < a.nsplit) {
@@ -795,7 +792,8 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         GCG_CUDA(cudaMemcpy(&sdeg, g->indeg.get() + p->source, 4, cudaMemcpyDeviceToHost));
         a.norm_const = sdeg == 0 ? fabs((double)(float)p->teleport) : 0.0;
     }
-    const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 32) + (int)pl.nlong; /* + a block per long row */
+    /* + a block per FIX_WARPS long rows */
+    const int fg = (int)grid1d(std::max<uint32_t>(pl.nsplit, 1), 32) + (int)((pl.nlong + FIX_WARPS - 1) / FIX_WARPS);
 
     /* source tiers: one edge pass per tier, each with its tier's contributions in
      * shared memory (tier 0: the hub plus every source past the last tier) */
@@ -829,7 +827,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
             a.tier_sum[k] = t.nzsum.get();
             ge_t[k] = std::max(1, (int)std::min<uint64_t>((uint64_t)edge_grid(hub_bytes),
                                                         (t.nchunks + 32 * run - 1) / (32 * run)));
-            fg_t[k] = (int)grid1d(std::max<uint32_t>(t.nsplit, 1), 32) + (int)t.nlong;
+            fg_t[k] = (int)grid1d(std::max<uint32_t>(t.nsplit, 1), 32) + (int)((t.nlong + FIX_WARPS - 1) / FIX_WARPS);
         }
     }
 

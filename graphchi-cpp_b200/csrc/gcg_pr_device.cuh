@@ -270,9 +270,8 @@ struct PrWork {
 
 /* Rows that cross chunk boundaries: a row spanning at most LONG_SPAN chunks is
  * summed by one thread in chunk order (tail part, then the head parts). A longer
- * row is summed in one fixed order, the same whether a whole block computes it
- * (the single-graph fix-up, one warp per group) or one warp does (the batch
- * kernel): LONG_GROUPS groups of 32 lanes; lane l of group g adds the head parts
+ * row is summed by one warp in one fixed order (the single-graph fix-up and the
+ * batch kernel alike): LONG_GROUPS groups of 32 lanes; lane l of group g adds the head parts
  * of chunks cs+1+32g+l, cs+1+32g+l+256, ... in order; each group is reduced by
  * an xor tree over its 32 lanes; the group sums are added in group order, and
  * the tail part last. */
