@@ -46,6 +46,7 @@ namespace {
 constexpr uint32_t VROWS = 4;                 /* rows per thread in a vertex tile */
 constexpr uint32_t VT = EDGE_THREADS * VROWS; /* rows per vertex tile */
 constexpr uint32_t NG_MAX = 1024;     /* graphs per batch */
+static_assert(NG_MAX <= EDGE_THREADS, "active_prefix gives each graph one thread of the CTA");
 
 /* per-graph ranges in the union */
 struct GRange {
@@ -114,25 +115,48 @@ __device__ bool grid_sync(const MultiArgs &m, uint32_t &gen) {
     return s_ok != 0;
 }
 
-/* prefix over the active graphs of a per-graph count, in shared memory;
- * *nactive receives the number of active graphs */
-__device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pref, uint32_t *nactive = nullptr) {
-    __shared__ uint32_t s_nact;
-    if (threadIdx.x == 0) {
-        uint32_t t = 0, na = 0;
-        for (uint32_t g = 0; g < m.ng; ++g) {
-            s_pref[g] = t;
-            if (*(volatile int *)(m.active + g)) {
-                const GRange r = m.gr[g];
-                t += which == 0 ? r.ce - r.cs : which == 1 ? r.se - r.ss : 0u;
-                ++na;
-            }
+/* Exclusive prefix over the active graphs of a per-graph count (which: 0 edge
+ * chunks, 1 split rows, 2 vertex tiles), in shared memory: thread g of the CTA
+ * reads graph g's flag and range (ng <= the block size), a block-wide scan adds
+ * them up. *nactive receives the number of active graphs. Every CTA computes
+ * the same prefix: the flags change only between grid barriers. */
+__device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pref, int const_pass,
+                                  uint32_t *nactive = nullptr) {
+    __shared__ uint32_t s_wsum[EDGE_THREADS / 32];
+    const uint32_t g = threadIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t cnt = 0;
+    int act = 0;
+    if (g < m.ng && *(volatile const int *)(m.active + g)) {
+        act = 1;
+        const GRange r = m.gr[g];
+        cnt = which == 0 ? r.ce - r.cs
+            : which == 1 ? r.se - r.ss
+                         : (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
+    }
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= (uint32_t)d) incl += y;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    const int na = __syncthreads_count(act);
+    if (warp == 0) {
+        const uint32_t w = lane < blockDim.x / 32 ? s_wsum[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, d);
+            if (lane >= (uint32_t)d) wi += y;
         }
-        s_pref[m.ng] = t;
-        s_nact = na;
+        if (lane < blockDim.x / 32) s_wsum[lane] = wi - w; /* exclusive warp offsets */
     }
     __syncthreads();
-    if (nactive) *nactive = s_nact;
+    const uint32_t excl = incl - cnt + s_wsum[warp];
+    if (g < m.ng) s_pref[g] = excl;
+    if (g + 1 == m.ng) s_pref[m.ng] = excl + cnt;
+    __syncthreads();
+    if (nactive) *nactive = (uint32_t)na;
     return s_pref[m.ng];
 }
 
@@ -169,7 +193,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         /* ---- A: edge chunks of the active graphs, grid-strided over their
          *         concatenation (chunks are equal-sized), loads one chunk ahead ---- */
         uint32_t nact = 0;
-        const uint32_t totA = active_prefix(m, 0, s_pref, &nact);
+        const uint32_t totA = active_prefix(m, 0, s_pref, const_pass, &nact);
         if (nact == 0) break; /* every graph has stopped: the same answer in every CTA */
         load_hub(a, s_hub);
         __syncthreads();
@@ -216,7 +240,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
          *         single-graph fix-up does (k_pr_fix): short rows by one lane in
          *         chunk order, long rows by the warp in the fixed group order of
          *         long_row_sum_warp ---- */
-        const uint32_t totB = active_prefix(m, 1, s_pref);
+        const uint32_t totB = active_prefix(m, 1, s_pref, const_pass);
         for (uint32_t wb = gwarp * 32u; wb < totB; wb += nwarps * 32u) {
             const uint32_t x = wb + lane;
             uint4 sp = make_uint4(0, 0, 0, 0);
@@ -246,19 +270,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
 
         /* ---- C: vertex tiles of the active graphs (work queue), one residual
          *         partial per tile ---- */
-        if (threadIdx.x == 0) {
-            uint32_t t = 0;
-            for (uint32_t g = 0; g < m.ng; ++g) {
-                s_pref[g] = t;
-                if (*(volatile int *)(m.active + g)) {
-                    const GRange r = m.gr[g];
-                    t += (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
-                }
-            }
-            s_pref[m.ng] = t;
-        }
-        __syncthreads();
-        const uint32_t totC = s_pref[m.ng];
+        const uint32_t totC = active_prefix(m, 2, s_pref, const_pass);
         for (;;) {
             if (threadIdx.x == 0) s_item = atomicAdd(qC, 1u);
             __syncthreads();

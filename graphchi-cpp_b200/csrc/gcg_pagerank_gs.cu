@@ -45,12 +45,26 @@ __global__ void k_level_relax(const uint32_t *__restrict__ rowptr, const uint32_
     }
 }
 
-__global__ void k_level_keys(const uint32_t *__restrict__ level, uint32_t nv, uint32_t vbits, uint64_t *keys) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        keys[v] = ((uint64_t)level[v] << vbits) | v;
+/* Vertex classes of a level, by in-degree: a thread sums a row of at most
+ * GS_THREAD_MAX in-edges, a warp one of at most GS_WARP_MAX, a block a longer
+ * one. Every class adds the in-edges one after another in ascending source
+ * order (a float sum is not associative); the cooperating threads only load. */
+constexpr uint32_t GS_THREAD_MAX = 32, GS_WARP_MAX = 1024;
+constexpr int GS_CLASSES = 4; /* segments per level: thread, warp, block, (unused) */
+
+/* sort key: level, class, vertex id */
+__global__ void k_level_keys(const uint32_t *__restrict__ level, const uint32_t *__restrict__ rowptr, uint32_t nv,
+                             uint32_t vbits, uint64_t *keys) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const uint32_t d = rowptr[v + 1] - rowptr[v];
+        const uint64_t cls = d <= GS_THREAD_MAX ? 0u : d <= GS_WARP_MAX ? 1u : 2u;
+        keys[v] = ((((uint64_t)level[v] << 2) | cls) << vbits) | v;
+    }
 }
 
-__global__ void k_level_bounds(const uint64_t *__restrict__ keys, uint32_t nv, uint32_t vbits, uint32_t nlev,
+/* order[i] = vertex of sorted key i; off[x] = first i whose segment
+ * (level * GS_CLASSES + class) is >= x, for x in [0, nseg] */
+__global__ void k_level_bounds(const uint64_t *__restrict__ keys, uint32_t nv, uint32_t vbits, uint32_t nseg,
                                uint32_t *__restrict__ off, uint32_t *__restrict__ order) {
     const uint64_t mask = (1ull << vbits) - 1ull;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
@@ -60,7 +74,7 @@ __global__ void k_level_bounds(const uint64_t *__restrict__ keys, uint32_t nv, u
         int64_t prev = i == 0 ? -1 : (int64_t)(keys[i - 1] >> vbits);
         for (int64_t x = prev + 1; x <= l; ++x) off[x] = i;
         if (i == nv - 1)
-            for (int64_t x = l + 1; x <= (int64_t)nlev; ++x) off[x] = nv;
+            for (int64_t x = l + 1; x <= (int64_t)nseg; ++x) off[x] = nv;
     }
 }
 
@@ -89,38 +103,109 @@ __global__ void k_gs_edge_init(uint32_t nv, const uint32_t *__restrict__ outdeg,
     }
 }
 
-/* One level of a sweep. In-memory program (EDGE = false), pagerank.cpp:127-136:
+/* value of in-edge (u -> v): this sweep's for u < v (an earlier level, written
+ * by an earlier launch), the previous sweep's otherwise */
+__device__ __forceinline__ float gs_in_value(uint32_t u, uint32_t v, const float *__restrict__ pr_old,
+                                             const float *__restrict__ pr_new) {
+    return u < v ? __ldg(pr_new + u) : __ldg(pr_old + u);
+}
+
+/* The apply of one vertex. In-memory program (EDGE = false), pagerank.cpp:127-136:
  * pr = (float)((0.15 + 0.85 * (double)sum) / outc). Edge-value program (EDGE =
  * true), pagerank.cpp:89-111: pagerank = (float)(0.15 + 0.85 * (double)sum), the
  * out-edge value pagerank / outc in float. TRACK (always with EDGE): the vertex's
  * pagerank goes to val[v] and |pagerank - previous| (float) to delta[v], for
- * the progress log and the residual stop. Levels of sweeps queued after `done`
- * was raised return at once. */
+ * the progress log and the residual stop. Explicit round-to-nearest ops: no FMA
+ * contraction, the same rounding as the reference's separate double multiply
+ * and add. */
 template <bool EDGE, bool TRACK>
-__global__ void k_gs_level(const uint32_t *__restrict__ order, uint32_t begin, uint32_t end,
-                           const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
-                           const uint32_t *__restrict__ outdeg, const float *__restrict__ pr_old, float *pr_new,
-                           float *val, float *delta, const int *done, double reset, double damping) {
+__device__ __forceinline__ void gs_apply(uint32_t v, float sum, const uint32_t *__restrict__ outdeg, float *pr_new,
+                                         float *val, float *delta, double reset, double damping) {
+    const int outc = (int)outdeg[v];
+    const double t = __dadd_rn(reset, __dmul_rn(damping, (double)sum));
+    if (EDGE) pr_new[v] = outc > 0 ? __fdiv_rn(__double2float_rn(t), (float)outc) : 0.0f;
+    else pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
+    if (TRACK) {
+        const float pagerank = __double2float_rn(t);
+        delta[v] = fabsf(__fsub_rn(pagerank, val[v]));
+        val[v] = pagerank;
+    }
+}
+
+/* One level of a sweep: the level's vertices are independent. Blocks
+ * [0, nb) take the block-class vertices (one each: every thread loads one
+ * in-edge value of a 256-edge batch into shared memory, thread 0 adds the batch
+ * in order while the next batch is being loaded); the next blocks take the
+ * warp-class vertices (one per warp: 32 values per batch, lane 0 adds them in
+ * order from shuffles, the next batch already loading); the rest take the
+ * thread-class vertices (eight loads in flight, then eight adds in order).
+ * Levels of sweeps queued after `done` was raised return at once. */
+template <bool EDGE, bool TRACK>
+__global__ void __launch_bounds__(256) k_gs_level(const uint32_t *__restrict__ order, uint32_t tb, uint32_t wb,
+                                                  uint32_t bb, uint32_t be, const uint32_t *__restrict__ rowptr,
+                                                  const uint32_t *__restrict__ col,
+                                                  const uint32_t *__restrict__ outdeg,
+                                                  const float *__restrict__ pr_old, float *pr_new, float *val,
+                                                  float *delta, const int *done, double reset, double damping) {
     if (TRACK && *(volatile const int *)done) return;
-    for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        const uint32_t v = order[i];
-        float sum = 0.0f;
+    const uint32_t nb = be - bb, nwb = (bb - wb + 7) / 8;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (blockIdx.x < nb) { /* block class */
+        __shared__ float s_val[2][256];
+        const uint32_t v = order[bb + blockIdx.x];
         const uint32_t jb = rowptr[v], je = rowptr[v + 1];
-        for (uint32_t j = jb; j < je; ++j) {
-            const uint32_t u = __ldg(col + j);
-            sum += (u < v) ? ((volatile const float *)pr_new)[u] : __ldg(pr_old + u);
+        const uint32_t nbatch = (je - jb + 255) / 256;
+        float sum = 0.0f;
+        if (jb + tid < je) s_val[0][tid] = gs_in_value(__ldg(col + jb + tid), v, pr_old, pr_new);
+        __syncthreads();
+        for (uint32_t b = 0; b < nbatch; ++b) {
+            const uint32_t nj = jb + (b + 1) * 256 + tid;
+            if (b + 1 < nbatch && nj < je) s_val[(b + 1) & 1][tid] = gs_in_value(__ldg(col + nj), v, pr_old, pr_new);
+            if (tid == 0) {
+                const uint32_t n = min(256u, je - (jb + b * 256));
+                const float *sv = s_val[b & 1];
+                for (uint32_t k = 0; k < n; ++k) sum += sv[k];
+            }
+            __syncthreads();
         }
-        /* explicit round-to-nearest ops: no FMA contraction, the same rounding as
-         * the reference's separate double multiply and add */
-        const int outc = (int)outdeg[v];
-        const double t = __dadd_rn(reset, __dmul_rn(damping, (double)sum));
-        if (EDGE) pr_new[v] = outc > 0 ? __fdiv_rn(__double2float_rn(t), (float)outc) : 0.0f;
-        else pr_new[v] = outc > 0 ? (float)__ddiv_rn(t, (double)outc) : (float)t;
-        if (TRACK) {
-            const float pagerank = __double2float_rn(t);
-            delta[v] = fabsf(__fsub_rn(pagerank, val[v]));
-            val[v] = pagerank;
+        if (tid == 0) gs_apply<EDGE, TRACK>(v, sum, outdeg, pr_new, val, delta, reset, damping);
+        return;
+    }
+    if (blockIdx.x < nb + nwb) { /* warp class */
+        const uint32_t i = wb + (blockIdx.x - nb) * 8 + warp;
+        if (i >= bb) return;
+        const uint32_t v = order[i];
+        const uint32_t jb = rowptr[v], je = rowptr[v + 1];
+        float sum = 0.0f;
+        float x = jb + lane < je ? gs_in_value(__ldg(col + jb + lane), v, pr_old, pr_new) : 0.0f;
+        for (uint32_t j0 = jb; j0 < je; j0 += 32) {
+            const uint32_t nj = j0 + 32 + lane;
+            const float y = nj < je ? gs_in_value(__ldg(col + nj), v, pr_old, pr_new) : 0.0f;
+            const uint32_t n = min(32u, je - j0);
+            for (uint32_t k = 0; k < n; ++k) {
+                const float z = __shfl_sync(0xFFFFFFFFu, x, (int)k);
+                sum += z; /* every lane keeps the same running sum, in order */
+            }
+            x = y;
         }
+        if (lane == 0) gs_apply<EDGE, TRACK>(v, sum, outdeg, pr_new, val, delta, reset, damping);
+        return;
+    }
+    /* thread class */
+    const uint32_t nth = (gridDim.x - nb - nwb) * blockDim.x;
+    for (uint32_t i = tb + (blockIdx.x - nb - nwb) * blockDim.x + tid; i < wb; i += nth) {
+        const uint32_t v = order[i];
+        const uint32_t jb = rowptr[v], je = rowptr[v + 1];
+        float sum = 0.0f;
+        for (uint32_t j0 = jb; j0 < je; j0 += 8) {
+            float x[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = j0 + k < je ? gs_in_value(__ldg(col + j0 + k), v, pr_old, pr_new) : 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (j0 + k < je) sum += x[k];
+        }
+        gs_apply<EDGE, TRACK>(v, sum, outdeg, pr_new, val, delta, reset, damping);
     }
 }
 
@@ -202,7 +287,8 @@ inline unsigned vgrid(uint32_t n) {
 }  // namespace
 
 /* Level schedule of the id-ordered dependency DAG: order[] (vertices by
- * (level, id)) and off[l] = first index of level l, nlev levels. */
+ * (level, class, id)) and off[GS_CLASSES * l + c] = first index of class c of
+ * level l, nlev levels. */
 struct GsPlan {
     uint32_t nlev = 0;
     dbuf<uint32_t> order;
@@ -237,19 +323,21 @@ static int build_gs_plan(gcg_graph *g, GsPlan &pl) {
     pl.nlev = maxl + 1;
     uint32_t lbits = 1;
     while (lbits < 32 && (1ull << lbits) <= maxl) ++lbits;
+    if (g->vbits + 2 + lbits > 64) return fail(GCG_ERR_UNSUPPORTED, "level schedule: too many levels");
     tbuf<uint64_t> keys, tmp;
     GCG_TRY(keys.alloc(nv, s));
     GCG_TRY(tmp.alloc(nv, s));
-    k_level_keys<<<vgrid(nv), 256, 0, s>>>(level.get(), nv, g->vbits, keys.get());
+    k_level_keys<<<vgrid(nv), 256, 0, s>>>(level.get(), g->in_rowptr.get(), nv, g->vbits, keys.get());
     uint64_t *sorted = nullptr;
-    GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + lbits), &sorted, s));
+    GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + 2 + lbits), &sorted, s));
+    const size_t nseg = (size_t)GS_CLASSES * pl.nlev;
     tbuf<uint32_t> doff;
-    GCG_TRY(doff.alloc((size_t)pl.nlev + 1, s));
+    GCG_TRY(doff.alloc(nseg + 1, s));
     GCG_TRY(pl.order.alloc(nv));
-    k_level_bounds<<<vgrid(nv), 256, 0, s>>>(sorted, nv, g->vbits, pl.nlev, doff.get(), pl.order.get());
+    k_level_bounds<<<vgrid(nv), 256, 0, s>>>(sorted, nv, g->vbits, (uint32_t)nseg, doff.get(), pl.order.get());
     GCG_LAUNCH_CHECK();
-    pl.off.resize((size_t)pl.nlev + 1);
-    GCG_CUDA(cudaMemcpyAsync(pl.off.data(), doff.get(), ((size_t)pl.nlev + 1) * 4, cudaMemcpyDeviceToHost, s));
+    pl.off.resize(nseg + 1);
+    GCG_CUDA(cudaMemcpyAsync(pl.off.data(), doff.get(), (nseg + 1) * 4, cudaMemcpyDeviceToHost, s));
     GCG_CUDA(cudaStreamSynchronize(s));
     return GCG_OK;
 }
@@ -298,19 +386,23 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
     GCG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     GCG_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     for (uint32_t l = 0; l < pl.nlev; ++l) {
-        uint32_t b = pl.off[l], e = pl.off[l + 1];
-        if (b == e) continue;
-        const unsigned gr = vgrid(e - b);
+        const uint32_t *o = pl.off.data() + (size_t)GS_CLASSES * l;
+        const uint32_t tb = o[0], wb = o[1], bb = o[2], be = o[3];
+        if (tb == be) continue;
+        /* blocks: one per block-class vertex, one per 8 warp-class vertices, then
+         * the thread-class vertices (grid-strided) */
+        const uint64_t nthr = wb - tb;
+        const unsigned gr = (unsigned)((be - bb) + (bb - wb + 7) / 8 + (nthr ? vgrid((uint32_t)nthr) : 0));
         const uint32_t *rp = g->in_rowptr.get(), *cl = g->in_col.get(), *od = g->outdeg.get();
         if (edge)
-            k_gs_level<true, true><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, val.get(),
-                                                        delta.get(), done, p->teleport, p->damping);
+            k_gs_level<true, true><<<gr, 256, 0, cap>>>(pl.order.get(), tb, wb, bb, be, rp, cl, od, pr_old, pr_new,
+                                                        val.get(), delta.get(), done, p->teleport, p->damping);
         else if (track)
-            k_gs_level<false, true><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, val.get(),
-                                                         delta.get(), done, p->teleport, p->damping);
+            k_gs_level<false, true><<<gr, 256, 0, cap>>>(pl.order.get(), tb, wb, bb, be, rp, cl, od, pr_old, pr_new,
+                                                         val.get(), delta.get(), done, p->teleport, p->damping);
         else
-            k_gs_level<false, false><<<gr, 256, 0, cap>>>(pl.order.get(), b, e, rp, cl, od, pr_old, pr_new, nullptr,
-                                                          nullptr, done, p->teleport, p->damping);
+            k_gs_level<false, false><<<gr, 256, 0, cap>>>(pl.order.get(), tb, wb, bb, be, rp, cl, od, pr_old, pr_new,
+                                                          nullptr, nullptr, done, p->teleport, p->damping);
     }
     if (track)
         k_gs_delta_sum<<<DSUM_BLOCKS, 256, 0, cap>>>(delta.get(), val.get(), nv, part.get(), ctl.get(), ctl.get() + 1,

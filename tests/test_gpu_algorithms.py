@@ -314,7 +314,7 @@ def test_tc_directed_input_vs_oracle():
 # ---- full-size configs (digests) -------------------------------------------
 
 @pytest.mark.slow
-@pytest.mark.parametrize("name", [n for n in golden_names() if "s20" in n])
+@pytest.mark.parametrize("name", [n for n in golden_names() if "s20" in n and "sym" in n])
 def test_scale20_cc_tc_bitexact(name):
     z, spec = load_golden(name)
     s, d = golden_input(spec)
