@@ -365,6 +365,7 @@ gcg_graph::~gcg_graph() {
     delete plan;
     gcg::free_chunk_plan(cplan);
     gcg::free_ppr_plan(pplan);
+    gcg::free_gs_plan(gsplan);
     free(intervals_host);
 }
 

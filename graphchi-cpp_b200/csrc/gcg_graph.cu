@@ -629,6 +629,7 @@ void swap_graph(gcg_graph *g, gcg_graph *ng) {
     std::swap(g->plan, ng->plan);
     std::swap(g->cplan, ng->cplan);
     std::swap(g->pplan, ng->pplan);
+    std::swap(g->gsplan, ng->gsplan);
 }
 
 int rebuild_from(gcg_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t nv) {

@@ -140,6 +140,8 @@ struct ChunkPlan;
 void free_chunk_plan(ChunkPlan *p);
 struct PprPlan;
 void free_ppr_plan(PprPlan *p);
+struct GsPlan;
+void free_gs_plan(GsPlan *p);
 
 }  // namespace gcg
 
@@ -167,6 +169,8 @@ struct gcg_graph {
     gcg::ChunkPlan *cplan = nullptr;
     /* row segments for batched personalised PageRank, built on first use */
     gcg::PprPlan *pplan = nullptr;
+    /* level schedule of the exact Gauss-Seidel modes, built on first use */
+    gcg::GsPlan *gsplan = nullptr;
 
     ~gcg_graph();
 };

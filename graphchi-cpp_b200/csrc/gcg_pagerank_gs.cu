@@ -28,19 +28,76 @@
 namespace gcg {
 namespace {
 
-__global__ void k_level_relax(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
-                              uint32_t *level, int *changed) {
+/* Levels of the id-ordered dependency DAG (edges u -> v with u < v) by
+ * topological rounds (Kahn): a vertex's level is 1 + the largest level of its
+ * smaller-id in-neighbours, i.e. the round after its last such neighbour's. */
+
+/* pending[v] = number of in-neighbours u < v (sources ascending: a binary search) */
+__global__ void k_gs_pending(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
+                             uint32_t *__restrict__ pending) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        uint32_t l = 0;
-        for (uint32_t j = rowptr[v]; j < rowptr[v + 1]; ++j) {
-            uint32_t u = col[j];
-            if (u >= v) break; /* sources ascending */
-            uint32_t lu = ((volatile uint32_t *)level)[u] + 1u;
-            l = lu > l ? lu : l;
+        uint32_t lo = rowptr[v], hi = rowptr[v + 1]; /* first position with col >= v */
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            if (col[mid] < v) lo = mid + 1; else hi = mid;
         }
-        if (l > level[v]) {
-            level[v] = l;
-            *changed = 1;
+        pending[v] = lo - rowptr[v];
+    }
+}
+
+/* keys (u << vbits) | v of the edges u -> v with u < v, compacted by a scan
+ * over the per-vertex counts */
+__global__ void k_gs_fwd_keys(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col, uint32_t nv,
+                              const uint32_t *__restrict__ pending, const uint32_t *__restrict__ pos, uint32_t vbits,
+                              uint64_t *__restrict__ keys) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const uint32_t b = rowptr[v], n = pending[v], o = pos[v];
+        for (uint32_t j = 0; j < n; ++j) keys[o + j] = ((uint64_t)col[b + j] << vbits) | v;
+    }
+}
+
+/* fwd_off[u] = first sorted key with source >= u (keys sorted by source) */
+__global__ void k_gs_fwd_off(const uint64_t *__restrict__ keys, uint64_t n, uint32_t vbits, uint32_t nv,
+                             uint32_t *__restrict__ off, uint32_t *__restrict__ dst) {
+    const uint64_t mask = (1ull << vbits) - 1ull;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys[i];
+        dst[i] = (uint32_t)(k & mask);
+        const int64_t u = (int64_t)(k >> vbits);
+        const int64_t prev = i == 0 ? -1 : (int64_t)(keys[i - 1] >> vbits);
+        for (int64_t x = prev + 1; x <= u; ++x) off[x] = (uint32_t)i;
+        if (i == n - 1)
+            for (int64_t x = u + 1; x <= (int64_t)nv; ++x) off[x] = (uint32_t)n;
+    }
+}
+
+/* round 0: the vertices without smaller-id in-neighbours */
+__global__ void k_gs_roots(const uint32_t *__restrict__ pending, uint32_t nv, uint32_t *__restrict__ front,
+                           uint32_t *__restrict__ count) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+        if (pending[v] == 0) front[atomicAdd(count, 1u)] = v;
+}
+
+/* one round: a warp per vertex of the current frontier (level r) releases its
+ * forward edges; a vertex whose last pending in-neighbour this is joins the next
+ * frontier with level r + 1. Counts per round: cnt[r] = frontier size of round
+ * r; rounds whose frontier is empty return at once (several are queued). */
+__global__ void __launch_bounds__(256) k_gs_round(uint32_t r, const uint32_t *__restrict__ fwd_off,
+                                                  const uint32_t *__restrict__ fwd_dst, uint32_t *pending,
+                                                  uint32_t *level, const uint32_t *__restrict__ front_cur,
+                                                  uint32_t *front_next, uint32_t *cnt) {
+    const uint32_t n = *(volatile const uint32_t *)(cnt + r);
+    if (n == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const uint32_t u = front_cur[i];
+        for (uint32_t j = fwd_off[u] + lane; j < fwd_off[u + 1]; j += 32) {
+            const uint32_t v = fwd_dst[j];
+            if (atomicSub(pending + v, 1u) == 1u) {
+                level[v] = r + 1;
+                front_next[atomicAdd(cnt + r + 1, 1u)] = v;
+            }
         }
     }
 }
@@ -78,13 +135,6 @@ __global__ void k_level_bounds(const uint64_t *__restrict__ keys, uint32_t nv, u
     }
 }
 
-__global__ void k_max_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t *out) {
-    uint32_t m = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, a[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xFFFFFFFFu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
 
 /* pagerank.cpp:124,137-139: pr starts at 0.15; iteration 0 sets 1/outc when outc > 0 */
 __global__ void k_gs_init(uint32_t nv, const uint32_t *__restrict__ outdeg, float reset, float *pr) {
@@ -295,31 +345,70 @@ struct GsPlan {
     std::vector<uint32_t> off;
 };
 
+void free_gs_plan(GsPlan *p) { delete p; }
+
 static int build_gs_plan(gcg_graph *g, GsPlan &pl) {
     cudaStream_t s = g->stream;
     const uint32_t nv = g->nv;
-    tbuf<uint32_t> level;
-    tbuf<int> changed;
+    tbuf<uint32_t> level, pending, pos, total;
     GCG_TRY(level.alloc(nv, s));
-    GCG_TRY(changed.alloc(1, s));
+    GCG_TRY(pending.alloc(nv, s));
+    GCG_TRY(pos.alloc(nv, s));
+    GCG_TRY(total.alloc(1, s));
     GCG_CUDA(cudaMemsetAsync(level.get(), 0, (size_t)nv * 4, s));
-    for (int it = 0;; ++it) {
-        int h = 0;
-        GCG_CUDA(cudaMemsetAsync(changed.get(), 0, sizeof(int), s));
-        k_level_relax<<<vgrid(nv), 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), nv, level.get(), changed.get());
-        GCG_LAUNCH_CHECK();
-        GCG_CUDA(cudaMemcpyAsync(&h, changed.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        GCG_CUDA(cudaStreamSynchronize(s));
-        if (!h) break;
-        if (it > (int)nv + 1) return fail(GCG_ERR_CUDA, "level relaxation did not converge");
-    }
-    tbuf<uint32_t> dmax;
-    GCG_TRY(dmax.alloc(1, s));
-    GCG_CUDA(cudaMemsetAsync(dmax.get(), 0, 4, s));
-    k_max_u32<<<vgrid(nv), 256, 0, s>>>(level.get(), nv, dmax.get());
-    uint32_t maxl = 0;
-    GCG_CUDA(cudaMemcpyAsync(&maxl, dmax.get(), 4, cudaMemcpyDeviceToHost, s));
+    k_gs_pending<<<vgrid(nv), 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), nv, pending.get());
+    GCG_TRY(scan_u32(pending.get(), pos.get(), nv, total.get(), s));
+    uint32_t nfwd = 0;
+    GCG_CUDA(cudaMemcpyAsync(&nfwd, total.get(), 4, cudaMemcpyDeviceToHost, s));
     GCG_CUDA(cudaStreamSynchronize(s));
+    uint32_t maxl = 0;
+    if (nfwd) {
+        /* the forward (u < v) edges grouped by source */
+        tbuf<uint64_t> keys, tmp;
+        tbuf<uint32_t> fwd_off, fwd_dst, front, cnt;
+        GCG_TRY(keys.alloc(nfwd, s));
+        GCG_TRY(tmp.alloc(nfwd, s));
+        GCG_TRY(fwd_off.alloc((size_t)nv + 1, s));
+        GCG_TRY(fwd_dst.alloc(nfwd, s));
+        GCG_TRY(front.alloc((size_t)2 * nv, s));
+        k_gs_fwd_keys<<<vgrid(nv), 256, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), nv, pending.get(), pos.get(),
+                                                g->vbits, keys.get());
+        uint64_t *sorted = nullptr;
+        GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nfwd, (int)g->vbits, (int)(2 * g->vbits), &sorted, s));
+        k_gs_fwd_off<<<vgrid(nfwd), 256, 0, s>>>(sorted, nfwd, g->vbits, nv, fwd_off.get(), fwd_dst.get());
+        /* rounds, queued in batches of 64 (empty rounds return at once); the host
+         * checks the last frontier count of each batch. A vertex joins a frontier
+         * once, so at most nv rounds. */
+        const uint32_t CAP = nv + 2;
+        GCG_TRY(cnt.alloc(CAP, s));
+        GCG_CUDA(cudaMemsetAsync(cnt.get(), 0, (size_t)CAP * 4, s));
+        k_gs_roots<<<vgrid(nv), 256, 0, s>>>(pending.get(), nv, front.get(), cnt.get());
+        GCG_LAUNCH_CHECK();
+        uint32_t r = 0;
+        for (;;) {
+            const uint32_t nb = std::min<uint32_t>(64, CAP - 2 - r);
+            for (uint32_t k = 0; k < nb; ++k, ++r) {
+                uint32_t *cur = front.get() + (size_t)(r & 1) * nv, *nxt = front.get() + (size_t)((r + 1) & 1) * nv;
+                k_gs_round<<<vgrid(nv), 256, 0, s>>>(r, fwd_off.get(), fwd_dst.get(), pending.get(), level.get(), cur,
+                                                     nxt, cnt.get());
+            }
+            GCG_LAUNCH_CHECK();
+            uint32_t last = 0;
+            GCG_CUDA(cudaMemcpyAsync(&last, cnt.get() + r, 4, cudaMemcpyDeviceToHost, s));
+            GCG_CUDA(cudaStreamSynchronize(s));
+            if (last == 0 || r + 2 >= CAP) break;
+        }
+        /* the deepest non-empty round */
+        std::vector<uint32_t> hc(r + 1);
+        GCG_CUDA(cudaMemcpyAsync(hc.data(), cnt.get(), (size_t)(r + 1) * 4, cudaMemcpyDeviceToHost, s));
+        GCG_CUDA(cudaStreamSynchronize(s));
+        uint64_t placed = 0;
+        for (uint32_t k = 0; k <= r; ++k) {
+            placed += hc[k];
+            if (hc[k]) maxl = k;
+        }
+        if (placed != nv) return fail(GCG_ERR_CUDA, "level schedule: a vertex was not reached");
+    }
     pl.nlev = maxl + 1;
     uint32_t lbits = 1;
     while (lbits < 32 && (1ull << lbits) <= maxl) ++lbits;
@@ -352,8 +441,16 @@ int pagerank_gs_exact(gcg_graph *g, const gcg_pr_params *p, float *out_rank, gcg
     const uint32_t nv = g->nv;
     const bool edge = p->mode == GCG_PR_GS_EDGE;
     const bool track = edge || p->tol > 0.0 || p->residuals || p->delta_log;
-    GsPlan pl;
-    GCG_TRY(build_gs_plan(g, pl));
+    if (!g->gsplan) { /* built once per graph, dropped when its edges change */
+        GsPlan *np = new GsPlan();
+        const int st = build_gs_plan(g, *np);
+        if (st != GCG_OK) {
+            delete np;
+            return st;
+        }
+        g->gsplan = np;
+    }
+    const GsPlan &pl = *g->gsplan;
     const int nsw = p->max_sweeps;
     tbuf<float> pr, val, delta;
     tbuf<double> logs; /* delta_log[nsw], res_log[nsw] */

@@ -58,6 +58,7 @@ def test_add_then_delete_equals_fresh_build(sym, device_input):
         import torch
         conv = (lambda x: torch.from_numpy(x.astype(np.int32)).cuda())
     with gcgpu.Graph.from_edges(s, d, dedup=True, symmetrise=sym, nshards=8) as g:
+        g.pagerank(mode=gcgpu.PR_GS_EXACT, max_sweeps=2)  # builds the level schedule of the old edges
         g.add_edges(conv(a_s), conv(a_d))
         s2, d2 = np.concatenate([s, a_s]), np.concatenate([d, a_d])
         with gcgpu.Graph.from_edges(s2, d2, dedup=True, symmetrise=sym, nshards=8) as ref:
@@ -82,6 +83,8 @@ def test_add_then_delete_equals_fresh_build(sym, device_input):
             l2, _ = ref.connected_components()
             assert np.array_equal(l1, l2)
         go = same_as_oracle(g, s3, d3, sym, 8)
+        # the exact Gauss-Seidel mode rebuilds its schedule for the new edges
+        assert np.array_equal(g.pagerank(mode=gcgpu.PR_GS_EXACT, max_sweeps=3)[0], go.pagerank_gs_inmem(4))
         o32, _, _ = go.pagerank_jacobi(max_sweeps=10)
         assert np.abs(r1.astype(np.float64) - o32).sum() / np.abs(o32).sum() <= 1e-6
         assert np.array_equal(l1, go.cc()[0])
