@@ -121,7 +121,7 @@ __device__ bool grid_sync(const MultiArgs &m, uint32_t &gen) {
  * them up. *nactive receives the number of active graphs. Every CTA computes
  * the same prefix: the flags change only between grid barriers. */
 __device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pref, int const_pass,
-                                  uint32_t *nactive = nullptr) {
+                                  uint32_t *nactive = nullptr, uint32_t *s_cs = nullptr) {
     __shared__ uint32_t s_wsum[EDGE_THREADS / 32];
     const uint32_t g = threadIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t cnt = 0;
@@ -129,6 +129,7 @@ __device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pre
     if (g < m.ng && *(volatile const int *)(m.active + g)) {
         act = 1;
         const GRange r = m.gr[g];
+        if (s_cs) s_cs[g] = r.cs; /* first chunk of each active graph, for the edge phase */
         cnt = which == 0 ? r.ce - r.cs
             : which == 1 ? r.se - r.ss
                          : (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
@@ -173,6 +174,7 @@ __device__ __forceinline__ uint32_t find_graph(const uint32_t *s_pref, uint32_t 
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m) {
     extern __shared__ float s_hub[];
     __shared__ uint32_t s_pref[NG_MAX + 1];
+    __shared__ uint32_t s_cs[NG_MAX];
     __shared__ uint32_t s_item;
     __shared__ double2 s_red[EDGE_THREADS / 32];
     const uint32_t FULL = 0xFFFFFFFFu;
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         /* ---- A: edge chunks of the active graphs, grid-strided over their
          *         concatenation (chunks are equal-sized), loads one chunk ahead ---- */
         uint32_t nact = 0;
-        const uint32_t totA = active_prefix(m, 0, s_pref, const_pass, &nact);
+        const uint32_t totA = active_prefix(m, 0, s_pref, const_pass, &nact, s_cs);
         if (nact == 0) break; /* every graph has stopped: the same answer in every CTA */
         load_hub(a, s_hub);
         __syncthreads();
@@ -214,24 +216,24 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
             };
             item = 0xFFFFFFFFu;
             next_run(item, item_end);
+            /* A graph's last chunk may end in filler edges: they form the row of
+             * the graph's padding vertex (its own head, never read), so chunks
+             * are reduced up to the union's end like the single-graph kernel's */
             uint32_t col[EPL], flags = 0, nvalid = 0, base = 0, ch = 0;
-            uint64_t gend = 0;
             auto load_item = [&](uint32_t it) {
                 const uint32_t g = find_graph(s_pref, m.ng, it);
-                ch = m.gr[g].cs + (it - s_pref[g]);
-                gend = m.gr[g].gend;
-                load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, gend);
+                ch = s_cs[g] + (it - s_pref[g]);
+                load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
             };
             if (item < item_end) load_item(item);
             while (item < item_end) {
                 float val[EPL];
                 gather_chunk<true>(a, col, nvalid, s_hub, pol_keep, val);
                 const uint32_t cch = ch, cf = flags, cn = nvalid, cb = base;
-                const uint64_t cend = gend;
                 ++item;
                 if (item >= item_end) next_run(item, item_end);
                 if (item < item_end) load_item(item);
-                reduce_chunk(a, cch, lane, val, cf, cn, cb, cend);
+                reduce_chunk(a, cch, lane, val, cf, cn, cb, a.ne);
             }
         }
         if (!grid_sync(m, gen)) return;
