@@ -171,6 +171,9 @@ struct gcg_graph {
     gcg::PprPlan *pplan = nullptr;
     /* level schedule of the exact Gauss-Seidel modes, built on first use */
     gcg::GsPlan *gsplan = nullptr;
+    /* PageRank plan option: relabel sources by out-degree within each interval
+     * (the many-graph union: every graph keeps its own id range) */
+    bool relabel_per_interval = false;
 
     ~gcg_graph();
 };

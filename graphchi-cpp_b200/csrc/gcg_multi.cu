@@ -75,8 +75,10 @@ struct MultiArgs {
     int *err;
     long long spin_limit;
     uint32_t extra_arrivals; /* test hook: the barrier waits for this many more CTAs */
-    uint32_t grab;           /* edge phase: 0 = warps stride over the chunks; g > 0 = warps take runs
-                                of g chunks from a device work queue (an autotuned choice) */
+    uint32_t grab;           /* edge phase without per-graph hubs: 0 = warps stride over the chunks;
+                                g > 0 = warps take runs of g chunks from a device work queue */
+    const uint32_t *voff;    /* per-graph hubs: first union vertex of each graph (ng + 1
+                                entries), NULL = one hub over the union's hottest sources */
 };
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
@@ -171,6 +173,8 @@ __device__ __forceinline__ uint32_t find_graph(const uint32_t *s_pref, uint32_t 
     return lo;
 }
 
+/* PG: per-graph hubs (m.voff set), else one hub over the union's hottest sources */
+template <bool PG>
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m) {
     extern __shared__ float s_hub[];
     __shared__ uint32_t s_pref[NG_MAX + 1];
@@ -197,9 +201,55 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         uint32_t nact = 0;
         const uint32_t totA = active_prefix(m, 0, s_pref, const_pass, &nact, s_cs);
         if (nact == 0) break; /* every graph has stopped: the same answer in every CTA */
-        load_hub(a, s_hub);
-        __syncthreads();
-        {
+        if (PG) {
+            /* Per-graph hubs: every graph's sources are relabelled by out-degree
+             * within its own id range, so a graph's hottest sources are the first
+             * ids of its range. CTA b takes the b-th equal share of the active
+             * chunks (in graph order); for each graph its share touches, the CTA
+             * loads that graph's hub into shared memory and its warps stride over
+             * the graph's chunks there, one chunk loaded ahead. */
+            const uint32_t lo = (uint32_t)((uint64_t)totA * blockIdx.x / gridDim.x);
+            const uint32_t hi = (uint32_t)((uint64_t)totA * (blockIdx.x + 1) / gridDim.x);
+            for (uint32_t x = lo; x < hi;) {
+                const uint32_t g = find_graph(s_pref, m.ng, x);
+                const uint32_t send = min(hi, s_pref[g + 1]);
+                const uint32_t v0 = m.voff[g], v1 = m.voff[g + 1];
+                const uint32_t hb = v0 & ~3u;                      /* 16-byte aligned start */
+                const uint32_t hn = min(a.hub + (v0 - hb), v1 - hb); /* entries [hb, hb + hn) */
+                __syncthreads(); /* the previous graph's gathers are done */
+                {
+                    const float4 *src4 = (const float4 *)(a.c_old + hb);
+                    float4 *dst4 = (float4 *)s_hub;
+                    const uint32_t n4 = hn >> 2;
+                    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
+                    for (uint32_t i = (n4 << 2) + threadIdx.x; i < hn; i += blockDim.x)
+                        s_hub[i] = __ldcg(a.c_old + hb + i);
+                }
+                __syncthreads();
+                uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
+                uint32_t pos = x + warp;
+                const uint32_t cs0 = s_cs[g] - s_pref[g];
+                if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                while (pos < send) {
+                    float val[EPL];
+#pragma unroll
+                    for (int j = 0; j < EPL; ++j) {
+                        const uint32_t d = col[j] - hb;
+                        float v = 0.0f;
+                        if ((uint32_t)j < nvalid) v = d < hn ? s_hub[d] : ld_cg_keep_f32(a.c_old + col[j], pol_keep);
+                        val[j] = v;
+                    }
+                    const uint32_t cch = cs0 + pos, cf = flags, cn = nvalid, cb = base;
+                    pos += EDGE_THREADS / 32;
+                    if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                    reduce_chunk(a, cch, lane, val, cf, cn, cb, a.ne);
+                }
+                x = send;
+            }
+        } else {
+            /* one hub over the union's hottest sources */
+            load_hub(a, s_hub);
+            __syncthreads();
             /* runs of chunks: [item, item_end) is this warp's current run; the
              * next chunk is loaded while the current one is gathered */
             const uint32_t run = m.grab ? m.grab : 1u;
@@ -576,6 +626,7 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
     u->intervals_host = (uint32_t *)malloc((size_t)ng * 4);
     for (uint32_t g = 0; g < ng; ++g) u->intervals_host[g] = b->voff[g + 1] - 1;
     GCG_CUDA(cudaMemcpy(u->intervals_dev.get(), u->intervals_host, (size_t)ng * 4, cudaMemcpyHostToDevice));
+    u->relabel_per_interval = true; /* every graph keeps its id range: per-graph hubs */
     GCG_TRY(ensure_chunk_plan(u));
     const ChunkPlan &pl = *u->cplan;
     /* per-graph ranges (padding vertices excluded) by binary search on the device:
@@ -655,7 +706,8 @@ static int enqueue_solve(gcg_batch *b, MultiArgs &m, const gcg_pr_params *p, con
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t le = cudaLaunchKernelEx(&cfg, k_multi_pagerank, m);
+    cudaError_t le = m.voff ? cudaLaunchKernelEx(&cfg, k_multi_pagerank<true>, m)
+                            : cudaLaunchKernelEx(&cfg, k_multi_pagerank<false>, m);
     if (le != cudaSuccess)
         return fail(GCG_ERR_CUDA, std::string("gcg_batch_pagerank: cooperative launch: ") + cudaGetErrorString(le));
     dim3 sg((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv / ng + 255) / 256, 64)),
@@ -746,12 +798,18 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
     m.spin_limit = test_timeout ? (1ll << 14) : (1ll << 25);
     m.extra_arrivals = test_timeout ? 1u : 0u;
     m.grab = b->tune_grab;
+    m.voff = pl.per_interval ? b->d_voff.get() : nullptr;
 
-    /* one cooperative launch: one CTA per SM, all resident */
-    const uint32_t hub_bytes = a.hub * 4u;
-    GCG_CUDA(cudaFuncSetAttribute(k_multi_pagerank, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(HUB_MAX * 4)));
+    /* one cooperative launch: one CTA per SM, all resident; per-graph hubs may
+     * start up to 3 entries before a graph's first id (16-byte alignment) */
+    const uint32_t hub_bytes = (a.hub + (m.voff && a.hub ? 4u : 0u)) * 4u;
+    GCG_CUDA(cudaFuncSetAttribute(k_multi_pagerank<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((HUB_MAX + 4) * 4)));
+    GCG_CUDA(cudaFuncSetAttribute(k_multi_pagerank<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((HUB_MAX + 4) * 4)));
     int per_sm = 0;
-    GCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multi_pagerank, EDGE_THREADS, hub_bytes));
+    GCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, m.voff ? k_multi_pagerank<true> : k_multi_pagerank<false>, EDGE_THREADS, hub_bytes));
     if (per_sm < 1) return fail(GCG_ERR_UNSUPPORTED, "gcg_batch_pagerank: persistent kernel does not fit an SM");
     const unsigned grid = (unsigned)num_sms();
 
@@ -874,7 +932,10 @@ static int batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_out, uint32_t 
     for (uint32_t h : {0u, 8192u, 16384u, 32768u, HUB_DEFAULT, HUB_MAX})
         if (h <= pl.hub && std::find(hubs.begin(), hubs.end(), h) == hubs.end()) hubs.push_back(h);
     if (std::find(hubs.begin(), hubs.end(), pl.hub) == hubs.end()) hubs.push_back(pl.hub);
-    const uint32_t grabs[] = {0u, 1u, 4u, 16u};
+    /* with per-graph hubs the edge phase partitions the chunks statically: the
+     * queue-run choice applies only to the one-hub layout */
+    const std::vector<uint32_t> grabs = pl.per_interval ? std::vector<uint32_t>{0u}
+                                                        : std::vector<uint32_t>{0u, 1u, 4u, 16u};
     gcg_pr_params p;
     gcg_pr_params_default(&p);
     p.max_sweeps = sweeps;

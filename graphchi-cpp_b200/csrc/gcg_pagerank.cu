@@ -334,6 +334,21 @@ __global__ void k_outdeg_keys(const uint32_t *__restrict__ outdeg, uint32_t nv, 
         keys[v] = ((uint64_t)(maxdeg - outdeg[v]) << vbits) | v;
 }
 
+/* the same keys led by the vertex's interval (last vertex ids ascending), so the
+ * relabelling keeps every interval's id range */
+__global__ void k_outdeg_keys_iv(const uint32_t *__restrict__ outdeg, uint32_t nv, uint32_t maxdeg, uint32_t vbits,
+                                 uint32_t dbits, const uint32_t *__restrict__ last, uint32_t nint,
+                                 uint64_t *__restrict__ keys) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nint - 1; /* first interval whose last vertex is >= v */
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (last[mid] < v) lo = mid + 1; else hi = mid;
+        }
+        keys[v] = ((uint64_t)lo << (dbits + vbits)) | ((uint64_t)(maxdeg - outdeg[v]) << vbits) | v;
+    }
+}
+
 __global__ void k_newid(const uint64_t *__restrict__ sorted, uint32_t nv, uint32_t vbits, uint32_t *__restrict__ newid) {
     const uint64_t mask = (1ull << vbits) - 1ull;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
@@ -550,10 +565,22 @@ int ensure_chunk_plan(gcg_graph *g) {
             return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
         uint32_t dbits = 1;
         while (dbits < 32 && (1ull << dbits) <= maxdeg) ++dbits;
-        k_outdeg_keys<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, maxdeg, g->vbits, keys.get());
+        uint32_t ibits = 1;
+        while (ibits < 32 && (1ull << ibits) < g->nshards) ++ibits;
+        p->per_interval = g->relabel_per_interval && g->nshards > 1 && g->intervals_dev.get() &&
+                          g->vbits + dbits + ibits <= 64;
         uint64_t *sorted = nullptr;
-        if ((st = radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + dbits), &sorted, s)))
-            return bail(st);
+        if (p->per_interval) {
+            k_outdeg_keys_iv<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, maxdeg, g->vbits, dbits,
+                                                        g->intervals_dev.get(), g->nshards, keys.get());
+            if ((st = radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + dbits + ibits),
+                                     &sorted, s)))
+                return bail(st);
+        } else {
+            k_outdeg_keys<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, maxdeg, g->vbits, keys.get());
+            if ((st = radix_sort_u64(keys.get(), tmp.get(), nv, (int)g->vbits, (int)(g->vbits + dbits), &sorted, s)))
+                return bail(st);
+        }
         k_newid<<<grid1d(nv), 256, 0, s>>>(sorted, nv, g->vbits, p->newid.get());
         if (ne)
             k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, (uint64_t)p->nchunks * CH, p->newid.get(),

@@ -339,6 +339,8 @@ struct ChunkPlan {
     /* launch configuration of the edge kernel (gcg_pagerank_autotune):
      * shared-memory hub entries (capped at hub) and chunks per warp run */
     uint32_t tune_hub = HUB_DEFAULT, tune_run = RUN_DEFAULT;
+    /* sources relabelled within each interval (each interval keeps its id range) */
+    bool per_interval = false;
 };
 
 /* builds (once per graph) the chunk plan and the out-degree relabelling */
