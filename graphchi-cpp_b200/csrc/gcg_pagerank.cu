@@ -334,20 +334,6 @@ __global__ void k_outdeg_keys(const uint32_t *__restrict__ outdeg, uint32_t nv, 
         keys[v] = ((uint64_t)(maxdeg - outdeg[v]) << vbits) | v;
 }
 
-/* The sources past the largest hub keep their id order (the hottest HUB_MAX keep
- * their out-degree ranks): flags of the vertices past it, then their new ids
- * HUB_MAX + (their rank in id order). The vertex pass, which visits the vertices
- * with in-edges in id order, then writes their contributions nearly in sequence
- * instead of scattered. */
-__global__ void k_past_hub_flags(const uint32_t *__restrict__ newid, uint32_t nv, uint32_t *__restrict__ f) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        f[v] = newid[v] >= HUB_MAX ? 1u : 0u;
-}
-__global__ void k_past_hub_ids(uint32_t *__restrict__ newid, uint32_t nv, const uint32_t *__restrict__ pos) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        if (newid[v] >= HUB_MAX) newid[v] = HUB_MAX + pos[v];
-}
-
 /* the same keys led by the vertex's interval (last vertex ids ascending), so the
  * relabelling keeps every interval's id range */
 __global__ void k_outdeg_keys_iv(const uint32_t *__restrict__ outdeg, uint32_t nv, uint32_t maxdeg, uint32_t vbits,
@@ -596,13 +582,6 @@ int ensure_chunk_plan(gcg_graph *g) {
                 return bail(st);
         }
         k_newid<<<grid1d(nv), 256, 0, s>>>(sorted, nv, g->vbits, p->newid.get());
-        if (!p->per_interval && nv > HUB_MAX) {
-            /* keys no longer needed: reuse them as the flags and their scan */
-            uint32_t *fl = (uint32_t *)keys.get(), *ps = (uint32_t *)tmp.get();
-            k_past_hub_flags<<<grid1d(nv), 256, 0, s>>>(p->newid.get(), nv, fl);
-            if ((st = scan_u32(fl, ps, nv, nullptr, s))) return bail(st);
-            k_past_hub_ids<<<grid1d(nv), 256, 0, s>>>(p->newid.get(), nv, ps);
-        }
         if (ne)
             k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, (uint64_t)p->nchunks * CH, p->newid.get(),
                                                      p->col_r.get());
