@@ -117,8 +117,11 @@ __device__ bool grid_sync(const MultiArgs &m, uint32_t &gen) {
     return s_ok != 0;
 }
 
+/* chunks per edge-phase work item with per-graph hubs (4 per warp of the CTA) */
+constexpr uint32_t EDGE_ITEM = 128;
+
 /* Exclusive prefix over the active graphs of a per-graph count (which: 0 edge
- * chunks, 1 split rows, 2 vertex tiles), in shared memory: thread g of the CTA
+ * chunks, 1 split rows, 2 vertex tiles, 3 edge work items), in shared memory: thread g of the CTA
  * reads graph g's flag and range (ng <= the block size), a block-wide scan adds
  * them up. *nactive receives the number of active graphs. Every CTA computes
  * the same prefix: the flags change only between grid barriers. */
@@ -128,13 +131,18 @@ __device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pre
     const uint32_t g = threadIdx.x, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t cnt = 0;
     int act = 0;
+    if (s_cs && g < m.ng) { /* chunk range of every graph, for the edge phase: [s_cs[g], s_cs[g + 1]) */
+        const GRange r = m.gr[g];
+        s_cs[g] = r.cs;
+        if (g + 1 == m.ng) s_cs[m.ng] = r.ce;
+    }
     if (g < m.ng && *(volatile const int *)(m.active + g)) {
         act = 1;
         const GRange r = m.gr[g];
-        if (s_cs) s_cs[g] = r.cs; /* first chunk of each active graph, for the edge phase */
         cnt = which == 0 ? r.ce - r.cs
             : which == 1 ? r.se - r.ss
-                         : (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
+            : which == 2 ? (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u)
+                         : (r.ce - r.cs + EDGE_ITEM - 1) / EDGE_ITEM;
     }
     uint32_t incl = cnt;
 #pragma unroll
@@ -178,7 +186,7 @@ template <bool PG>
 __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m) {
     extern __shared__ float s_hub[];
     __shared__ uint32_t s_pref[NG_MAX + 1];
-    __shared__ uint32_t s_cs[NG_MAX];
+    __shared__ uint32_t s_cs[NG_MAX + 1];
     __shared__ uint32_t s_item;
     __shared__ double2 s_red[EDGE_THREADS / 32];
     const uint32_t FULL = 0xFFFFFFFFu;
@@ -204,33 +212,40 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         if (PG) {
             /* Per-graph hubs: every graph's sources are relabelled by out-degree
              * within its own id range, so a graph's hottest sources are the first
-             * ids of its range. CTA b takes the b-th equal share of the active
-             * chunks (in graph order); for each graph its share touches, the CTA
-             * loads that graph's hub into shared memory and its warps stride over
-             * the graph's chunks there, one chunk loaded ahead. */
-            const uint32_t lo = (uint32_t)((uint64_t)totA * blockIdx.x / gridDim.x);
-            const uint32_t hi = (uint32_t)((uint64_t)totA * (blockIdx.x + 1) / gridDim.x);
-            for (uint32_t x = lo; x < hi;) {
-                const uint32_t g = find_graph(s_pref, m.ng, x);
-                const uint32_t send = min(hi, s_pref[g + 1]);
-                const uint32_t v0 = m.voff[g], v1 = m.voff[g + 1];
-                const uint32_t hb = v0 & ~3u;                      /* 16-byte aligned start */
-                const uint32_t hn = min(a.hub + (v0 - hb), v1 - hb); /* entries [hb, hb + hn) */
-                __syncthreads(); /* the previous graph's gathers are done */
-                {
+             * ids of its range. The active graphs' chunks are cut into items of
+             * EDGE_ITEM chunks (in graph order) that CTAs take from a device work
+             * queue; a CTA loads the hub of an item's graph into shared memory when
+             * the graph changes, and its warps take the item's chunks in turn, one
+             * chunk loaded ahead. */
+            const uint32_t totI = active_prefix(m, 3, s_pref, const_pass, nullptr, s_cs);
+            uint32_t *qA = m.qctr + 2 * (sweep & 1);
+            uint32_t cur = 0xFFFFFFFFu, hb = 0, hn = 0;
+            for (;;) {
+                if (threadIdx.x == 0) s_item = atomicAdd(qA, 1u);
+                __syncthreads(); /* also: every warp is done with the previous item */
+                const uint32_t it = s_item;
+                __syncthreads();
+                if (it >= totI) break;
+                const uint32_t g = find_graph(s_pref, m.ng, it);
+                if (g != cur) {
+                    const uint32_t v0 = m.voff[g], v1 = m.voff[g + 1];
+                    hb = v0 & ~3u;                      /* 16-byte aligned start */
+                    hn = min(a.hub + (v0 - hb), v1 - hb); /* entries [hb, hb + hn) */
                     const float4 *src4 = (const float4 *)(a.c_old + hb);
                     float4 *dst4 = (float4 *)s_hub;
                     const uint32_t n4 = hn >> 2;
                     for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
                     for (uint32_t i = (n4 << 2) + threadIdx.x; i < hn; i += blockDim.x)
                         s_hub[i] = __ldcg(a.c_old + hb + i);
+                    __syncthreads();
+                    cur = g;
                 }
-                __syncthreads();
+                const uint32_t c0 = s_cs[g] + (it - s_pref[g]) * EDGE_ITEM;
+                const uint32_t c1 = min(c0 + EDGE_ITEM, s_cs[g + 1]);
                 uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
-                uint32_t pos = x + warp;
-                const uint32_t cs0 = s_cs[g] - s_pref[g];
-                if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
-                while (pos < send) {
+                uint32_t ch = c0 + warp;
+                if (ch < c1) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                while (ch < c1) {
                     float val[EPL];
 #pragma unroll
                     for (int j = 0; j < EPL; ++j) {
@@ -239,12 +254,11 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
                         if ((uint32_t)j < nvalid) v = d < hn ? s_hub[d] : ld_cg_keep_f32(a.c_old + col[j], pol_keep);
                         val[j] = v;
                     }
-                    const uint32_t cch = cs0 + pos, cf = flags, cn = nvalid, cb = base;
-                    pos += EDGE_THREADS / 32;
-                    if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                    const uint32_t cch = ch, cf = flags, cn = nvalid, cb = base;
+                    ch += EDGE_THREADS / 32;
+                    if (ch < c1) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
                     reduce_chunk(a, cch, lane, val, cf, cn, cb, a.ne);
                 }
-                x = send;
             }
         } else {
             /* one hub over the union's hottest sources */

@@ -309,13 +309,18 @@ int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ran
                        double *residuals, gcg_pr_stats *stats);
 /* Autotuner of the persistent launch: times `sweeps` fixed sweeps of each
  * candidate configuration and keeps the fastest for later solves (results do not
- * depend on it). Candidates: shared-memory hub entries (sources whose out-degree
- * rank is below it are read from shared memory: the degree threshold of the
- * cache) in {0, 8192, 16384, 32768, 41728, 49152, the plan's}, and the edge phase's work
- * distribution: warps striding over the chunks (queue_run 0) or taking runs of
- * 1, 4 or 16 chunks from a device work queue. Outputs may be NULL. */
+ * depend on it). Candidates: shared-memory hub entries per graph (each graph's
+ * sources whose out-degree rank within the graph is below it are read from
+ * shared memory: the degree threshold of the cache) in {0, 8192, 16384, 32768,
+ * 41728, 49152, the plan's}. Each CTA takes an equal share of the active graphs'
+ * chunks. Only when the union's ids are too wide for per-graph relabelling
+ * (more than 64 sort-key bits) is there one hub over the union's hottest sources
+ * and the edge phase's work distribution a second candidate: warps striding over
+ * the chunks (queue_run 0) or taking runs of 1, 4 or 16 chunks from a device
+ * work queue. Outputs may be NULL. */
 int gcg_batch_autotune(gcg_batch *b, int sweeps, uint32_t *hub_entries, uint32_t *queue_run, double *ms_per_sweep);
-/* Sets the configuration by hand (hub entries are capped at the plan's). */
+/* Sets the configuration by hand (hub entries are capped at the plan's;
+ * queue_run applies to the one-hub layout only). */
 int gcg_batch_set_config(gcg_batch *b, uint32_t hub_entries, uint32_t queue_run);
 /* The configuration in use, and whether a captured solve is ready to replay. */
 int gcg_batch_get_config(const gcg_batch *b, uint32_t *hub_entries, uint32_t *queue_run, int *graph_ready);
