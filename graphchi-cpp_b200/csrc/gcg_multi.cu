@@ -117,11 +117,12 @@ __device__ bool grid_sync(const MultiArgs &m, uint32_t &gen) {
     return s_ok != 0;
 }
 
-/* chunks per edge-phase work item with per-graph hubs (4 per warp of the CTA) */
-constexpr uint32_t EDGE_ITEM = 128;
+/* smallest range of chunks a CTA takes at a time in the edge phase with
+ * per-graph hubs (two per warp of the CTA) */
+constexpr uint32_t GRAB_MIN = 64;
 
 /* Exclusive prefix over the active graphs of a per-graph count (which: 0 edge
- * chunks, 1 split rows, 2 vertex tiles, 3 edge work items), in shared memory: thread g of the CTA
+ * chunks, 1 split rows, 2 vertex tiles), in shared memory: thread g of the CTA
  * reads graph g's flag and range (ng <= the block size), a block-wide scan adds
  * them up. *nactive receives the number of active graphs. Every CTA computes
  * the same prefix: the flags change only between grid barriers. */
@@ -141,8 +142,7 @@ __device__ uint32_t active_prefix(const MultiArgs &m, int which, uint32_t *s_pre
         const GRange r = m.gr[g];
         cnt = which == 0 ? r.ce - r.cs
             : which == 1 ? r.se - r.ss
-            : which == 2 ? (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u)
-                         : (r.ce - r.cs + EDGE_ITEM - 1) / EDGE_ITEM;
+                         : (r.ne - r.ns + VT - 1) / VT + (const_pass ? (r.ze - r.zs + VT - 1) / VT : 0u);
     }
     uint32_t incl = cnt;
 #pragma unroll
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
     extern __shared__ float s_hub[];
     __shared__ uint32_t s_pref[NG_MAX + 1];
     __shared__ uint32_t s_cs[NG_MAX + 1];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_grab;
     __shared__ double2 s_red[EDGE_THREADS / 32];
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -212,52 +212,63 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         if (PG) {
             /* Per-graph hubs: every graph's sources are relabelled by out-degree
              * within its own id range, so a graph's hottest sources are the first
-             * ids of its range. The active graphs' chunks are cut into items of
-             * EDGE_ITEM chunks (in graph order) that CTAs take from a device work
-             * queue; a CTA loads the hub of an item's graph into shared memory when
-             * the graph changes, and its warps take the item's chunks in turn, one
-             * chunk loaded ahead. */
-            const uint32_t totI = active_prefix(m, 3, s_pref, const_pass, nullptr, s_cs);
-            uint32_t *qA = m.qctr + 2 * (sweep & 1);
+             * ids of its range. CTAs take ranges of the active graphs' chunks (in
+             * graph order) from a device cursor, guided: a grab is 1/(2 x CTAs) of
+             * what is left, at least GRAB_MIN chunks, so early grabs are large and
+             * the last ones small. For each graph a range touches, the CTA loads
+             * that graph's hub into shared memory (unless it holds it already) and
+             * its warps stride over the graph's chunks, one chunk loaded ahead. */
+            uint32_t *cursor = m.qctr + 2 * (sweep & 1);
             uint32_t cur = 0xFFFFFFFFu, hb = 0, hn = 0;
             for (;;) {
-                if (threadIdx.x == 0) s_item = atomicAdd(qA, 1u);
-                __syncthreads(); /* also: every warp is done with the previous item */
-                const uint32_t it = s_item;
-                __syncthreads();
-                if (it >= totI) break;
-                const uint32_t g = find_graph(s_pref, m.ng, it);
-                if (g != cur) {
-                    const uint32_t v0 = m.voff[g], v1 = m.voff[g + 1];
-                    hb = v0 & ~3u;                      /* 16-byte aligned start */
-                    hn = min(a.hub + (v0 - hb), v1 - hb); /* entries [hb, hb + hn) */
-                    const float4 *src4 = (const float4 *)(a.c_old + hb);
-                    float4 *dst4 = (float4 *)s_hub;
-                    const uint32_t n4 = hn >> 2;
-                    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
-                    for (uint32_t i = (n4 << 2) + threadIdx.x; i < hn; i += blockDim.x)
-                        s_hub[i] = __ldcg(a.c_old + hb + i);
-                    __syncthreads();
-                    cur = g;
+                if (threadIdx.x == 0) {
+                    const uint32_t seen = *(volatile uint32_t *)cursor;
+                    const uint32_t left = seen < totA ? totA - seen : 0u;
+                    const uint32_t want = max(GRAB_MIN, left / (2u * gridDim.x));
+                    s_item = atomicAdd(cursor, want);
+                    s_grab = want;
                 }
-                const uint32_t c0 = s_cs[g] + (it - s_pref[g]) * EDGE_ITEM;
-                const uint32_t c1 = min(c0 + EDGE_ITEM, s_cs[g + 1]);
-                uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
-                uint32_t ch = c0 + warp;
-                if (ch < c1) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
-                while (ch < c1) {
-                    float val[EPL];
-#pragma unroll
-                    for (int j = 0; j < EPL; ++j) {
-                        const uint32_t d = col[j] - hb;
-                        float v = 0.0f;
-                        if ((uint32_t)j < nvalid) v = d < hn ? s_hub[d] : ld_cg_keep_f32(a.c_old + col[j], pol_keep);
-                        val[j] = v;
+                __syncthreads(); /* also: every warp is done with the previous range */
+                const uint32_t lo = s_item, hi = min(totA, lo + s_grab);
+                __syncthreads();
+                if (lo >= totA) break;
+                for (uint32_t x = lo; x < hi;) {
+                    const uint32_t g = find_graph(s_pref, m.ng, x);
+                    const uint32_t send = min(hi, s_pref[g + 1]);
+                    if (g != cur) {
+                        if (x != lo) __syncthreads(); /* the previous graph's gathers are done */
+                        const uint32_t v0 = m.voff[g], v1 = m.voff[g + 1];
+                        hb = v0 & ~3u;                      /* 16-byte aligned start */
+                        hn = min(a.hub + (v0 - hb), v1 - hb); /* entries [hb, hb + hn) */
+                        const float4 *src4 = (const float4 *)(a.c_old + hb);
+                        float4 *dst4 = (float4 *)s_hub;
+                        const uint32_t n4 = hn >> 2;
+                        for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) dst4[i] = __ldcg(src4 + i);
+                        for (uint32_t i = (n4 << 2) + threadIdx.x; i < hn; i += blockDim.x)
+                            s_hub[i] = __ldcg(a.c_old + hb + i);
+                        __syncthreads();
+                        cur = g;
                     }
-                    const uint32_t cch = ch, cf = flags, cn = nvalid, cb = base;
-                    ch += EDGE_THREADS / 32;
-                    if (ch < c1) load_chunk(a, ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
-                    reduce_chunk(a, cch, lane, val, cf, cn, cb, a.ne);
+                    const uint32_t cs0 = s_cs[g] - s_pref[g]; /* chunk = cs0 + position */
+                    uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
+                    uint32_t pos = x + warp;
+                    if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                    while (pos < send) {
+                        float val[EPL];
+#pragma unroll
+                        for (int j = 0; j < EPL; ++j) {
+                            const uint32_t d = col[j] - hb;
+                            float v = 0.0f;
+                            if ((uint32_t)j < nvalid)
+                                v = d < hn ? s_hub[d] : ld_cg_keep_f32(a.c_old + col[j], pol_keep);
+                            val[j] = v;
+                        }
+                        const uint32_t cch = cs0 + pos, cf = flags, cn = nvalid, cb = base;
+                        pos += EDGE_THREADS / 32;
+                        if (pos < send) load_chunk(a, cs0 + pos, lane, pol_stream, col, flags, nvalid, base, a.ne);
+                        reduce_chunk(a, cch, lane, val, cf, cn, cb, a.ne);
+                    }
+                    x = send;
                 }
             }
         } else {
