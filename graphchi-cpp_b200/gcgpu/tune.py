@@ -8,6 +8,11 @@ configuration computes the same sums in the same order except source tiers
 
     python -m gcgpu.tune --scale 24 [--tiers 1 2 3 4] [--hub 41728 32768]
 
+With --batch LO HI it reports the many-graph persistent launch instead: 64
+graphs, vertex counts log-uniform in [LO, HI] (seeded), alternating
+Erdos-Renyi (mean degree 8) and R-MAT (edge factor 8), solved to 1e-8 in one
+launch for each --hub value, against one gcg_pagerank solve per graph.
+
 (run with graphchi-cpp_b200 on PYTHONPATH)."""
 from __future__ import annotations
 
@@ -25,6 +30,50 @@ def peak_gbs():
         return 6650.0
 
 
+def batch_report(lo, hi, hubs, peak):
+    import math
+    import numpy as np
+    import torch
+    import gcgpu
+    rng = np.random.default_rng(5)
+    ns = np.exp(rng.uniform(math.log(lo), math.log(hi), 64)).astype(int)
+    gs = []
+    for i, nn in enumerate(ns):
+        if i % 2 == 0:
+            mm = 8 * int(nn)
+            s = torch.empty(mm, dtype=torch.int32, device="cuda")
+            d = torch.empty_like(s)
+            gcgpu.generate_er(int(nn), mm, 100 + i, s, d)
+            gs.append(gcgpu.Graph.from_edges(s, d, num_vertices=int(nn), dedup=True, out_csr=False))
+        else:
+            sc = max(1, round(math.log2(nn)))
+            s = torch.empty(8 << sc, dtype=torch.int32, device="cuda")
+            d = torch.empty_like(s)
+            gcgpu.generate_rmat(sc, 8 << sc, 0.57, 0.19, 0.19, seed=100 + i, src=s, dst=d)
+            gs.append(gcgpu.Graph.from_edges(s, d, num_vertices=1 << sc, dedup=True, out_csr=False))
+    seq = 0.0
+    for g in gs:
+        o = torch.empty(g.num_vertices, dtype=torch.float32, device="cuda")
+        g.pagerank(max_sweeps=1000, tol=1e-8, out=o)
+        seq += g.pagerank(max_sweeps=1000, tol=1e-8, out=o)[1].device_ms
+    with gcgpu.Batch(gs) as b:
+        allr = torch.empty(int(b.offsets[-1]), dtype=torch.float32, device="cuda")
+        for hub in hubs:
+            b.set_config(hub, 0)
+            b.pagerank(max_sweeps=1000, tol=1e-8, out=allr)
+            best = min((b.pagerank(max_sweeps=1000, tol=1e-8, out=allr) for _ in range(3)),
+                       key=lambda x: x[3].device_ms)
+            st, gsw = best[3], best[1]
+            byt = float(sum(int(n) * (8.0 * g.num_edges + 16.0 * g.num_vertices) for n, g in zip(gsw, gs)))
+            print(json.dumps({"batch": [lo, hi], "graphs": 64, "vertices": int(b.offsets[-1]),
+                              "edges": int(sum(g.num_edges for g in gs)), "hub": hub,
+                              "max_sweeps": int(gsw.max()), "ms_one_launch": round(st.device_ms, 2),
+                              "ms_one_solve_per_graph": round(seq, 2), "speedup": round(seq / st.device_ms, 2),
+                              "frac_of_hbm": round(byt / st.device_ms / 1e6 / peak, 3)}), flush=True)
+    for g in gs:
+        g.free()
+
+
 def main():
     import torch
     import gcgpu
@@ -34,8 +83,12 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--hub", type=int, nargs="+", default=[41728])
     ap.add_argument("--tiers", type=int, nargs="+", default=[1])
+    ap.add_argument("--batch", type=float, nargs=2, default=None, metavar=("LO", "HI"))
     args = ap.parse_args()
     peak = peak_gbs()
+    if args.batch:
+        batch_report(args.batch[0], args.batch[1], args.hub, peak)
+        return
     for scale in args.scale:
         m = args.ef << scale
         s = torch.empty(m, dtype=torch.int32, device="cuda")
