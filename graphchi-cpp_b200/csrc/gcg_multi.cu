@@ -79,6 +79,8 @@ struct MultiArgs {
                                 g > 0 = warps take runs of g chunks from a device work queue */
     const uint32_t *voff;    /* per-graph hubs: first union vertex of each graph (ng + 1
                                 entries), NULL = one hub over the union's hottest sources */
+    const uint32_t *long_g;  /* graph of each long split row (a.long_split order) */
+    uint32_t nlong;
 };
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
@@ -314,9 +316,17 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
         if (!grid_sync(m, gen)) return;
 
         /* ---- B: rows crossing chunk boundaries, summed exactly as the
-         *         single-graph fix-up does (k_pr_fix): short rows by one lane in
-         *         chunk order, long rows by the warp in the fixed group order of
-         *         long_row_sum_warp ---- */
+         *         single-graph fix-up does (k_pr_fix): long rows one per warp over
+         *         the grid in the fixed group order of long_row_sum_warp (rows
+         *         in relabelled order put a graph's long rows next to each other),
+         *         short rows by one lane in chunk order ---- */
+        for (uint32_t k = gwarp; k < m.nlong; k += nwarps) {
+            const uint32_t g = m.long_g[k];
+            if (g >= m.ng || !*(volatile const int *)(m.active + g)) continue;
+            const uint4 sp = a.split[a.long_split[k]];
+            const float s = long_row_sum_warp<true>(a.head_part, sp.y, sp.z, lane);
+            if (lane == 0) a.nzsum[sp.x] = __ldcg(a.tail_part + sp.y) + s;
+        }
         const uint32_t totB = active_prefix(m, 1, s_pref, const_pass);
         for (uint32_t wb = gwarp * 32u; wb < totB; wb += nwarps * 32u) {
             const uint32_t x = wb + lane;
@@ -326,21 +336,10 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_multi_pagerank(MultiArgs m)
                 const uint32_t g = find_graph(s_pref, m.ng, x);
                 sp = a.split[m.gr[g].ss + (x - s_pref[g])];
             }
-            const bool lng = valid && (sp.z - sp.y) > LONG_SPAN;
-            if (valid && !lng) {
+            if (valid && (sp.z - sp.y) <= LONG_SPAN) {
                 float s = __ldcg(a.tail_part + sp.y);
                 for (uint32_t c = sp.y + 1; c <= sp.z; ++c) s += __ldcg(a.head_part + c);
                 a.nzsum[sp.x] = s;
-            }
-            uint32_t msk = __ballot_sync(FULL, lng);
-            while (msk) {
-                const int srcl = __ffs(msk) - 1;
-                msk &= msk - 1;
-                const uint32_t row = __shfl_sync(FULL, sp.x, srcl);
-                const uint32_t cs = __shfl_sync(FULL, sp.y, srcl);
-                const uint32_t ce = __shfl_sync(FULL, sp.z, srcl);
-                const float s = long_row_sum_warp<true>(a.head_part, cs, ce, lane);
-                if (lane == 0) a.nzsum[row] = __ldcg(a.tail_part + cs) + s;
             }
         }
         if (!grid_sync(m, gen)) return;
@@ -571,6 +570,7 @@ struct gcg_batch {
     std::vector<uint32_t> roff;         /* offset of each graph in the callers' arrays (no padding) */
     std::vector<gcg::GRange> gr_host;
     gcg::dbuf<uint32_t> d_roff, d_voff;
+    gcg::dbuf<uint32_t> long_g; /* graph of each long split row of the union (or ng: none) */
     uint32_t ntiles = 0;
     gcg::dbuf<gcg::GRange> gr;
     /* workspace, allocated on the first solve */
@@ -655,7 +655,11 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
     GCG_TRY(ensure_chunk_plan(u));
     const ChunkPlan &pl = *u->cplan;
     /* per-graph ranges (padding vertices excluded) by binary search on the device:
-     * query 2g = first vertex of graph g, 2g+1 = its padding vertex */
+     * query 2g = first vertex of graph g, 2g+1 = its padding vertex. The plan's
+     * rows are in relabelled order, which keeps every graph's id range and puts
+     * the padding vertex (no out-edges, the range's largest id) last, so the
+     * search runs on the relabelled ids (on the original ids for a union whose
+     * rows kept the original order) */
     const uint32_t nq = 2 * ng;
     std::vector<uint32_t> q(nq);
     for (uint32_t g = 0; g < ng; ++g) {
@@ -669,8 +673,9 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
     GCG_TRY(sb.alloc(nq));
     GCG_CUDA(cudaMemcpy(dq.get(), q.data(), nq * 4, cudaMemcpyHostToDevice));
     const unsigned gb = (nq + 255) / 256;
-    k_bounds<<<gb, 256>>>(pl.nz_rows.get(), pl.nnz, dq.get(), nq, nzb.get());
-    k_bounds<<<gb, 256>>>(pl.zero_rows.get(), pl.nzero, dq.get(), nq, zb.get());
+    k_bounds<<<gb, 256>>>(pl.rows_relabelled ? pl.nz_cidx.get() : pl.nz_rows.get(), pl.nnz, dq.get(), nq, nzb.get());
+    k_bounds<<<gb, 256>>>(pl.rows_relabelled ? pl.zero_cidx.get() : pl.zero_rows.get(), pl.nzero, dq.get(), nq,
+                          zb.get());
     k_split_bounds<<<gb, 256>>>(pl.split.get(), pl.nsplit, nzb.get(), nq, sb.get());
     GCG_LAUNCH_CHECK();
     std::vector<uint32_t> hn(nq), hz(nq), hs(nq);
@@ -697,6 +702,22 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
         r.pad1 = 0;
     }
     b->ntiles = tiles;
+    /* the graph of each long split row (the padding rows never span that far) */
+    {
+        std::vector<uint32_t> ls(pl.nlong), lg(std::max<uint32_t>(pl.nlong, 1), ng);
+        if (pl.nlong)
+            GCG_CUDA(cudaMemcpy(ls.data(), pl.long_split.get(), (size_t)pl.nlong * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t k = 0; k < pl.nlong; ++k) {
+            uint32_t lo = 0, hi = ng; /* last graph whose split range starts at or before ls[k] */
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (b->gr_host[mid].ss <= ls[k]) lo = mid; else hi = mid;
+            }
+            if (b->gr_host[lo].ss <= ls[k] && ls[k] < b->gr_host[lo].se) lg[k] = lo;
+        }
+        GCG_TRY(b->long_g.alloc(lg.size()));
+        GCG_CUDA(cudaMemcpy(b->long_g.get(), lg.data(), lg.size() * 4, cudaMemcpyHostToDevice));
+    }
     GCG_TRY(b->gr.alloc(ng));
     GCG_CUDA(cudaMemcpy(b->gr.get(), b->gr_host.data(), ng * sizeof(GRange), cudaMemcpyHostToDevice));
     GCG_TRY(b->d_roff.alloc(ng + 1));
@@ -824,6 +845,9 @@ static int batch_pagerank(gcg_batch *b, const gcg_pr_params *p, float *out, int3
     m.extra_arrivals = test_timeout ? 1u : 0u;
     m.grab = b->tune_grab;
     m.voff = pl.per_interval ? b->d_voff.get() : nullptr;
+    m.a.long_split = pl.long_split.get();
+    m.long_g = b->long_g.get();
+    m.nlong = pl.nlong;
 
     /* one cooperative launch: one CTA per SM, all resident; per-graph hubs may
      * start up to 3 entries before a graph's first id (16-byte alignment) */

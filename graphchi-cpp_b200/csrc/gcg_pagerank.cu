@@ -41,21 +41,36 @@ namespace {
 
 
 /* ---- per-graph plan kernels -------------------------------------------- */
-__global__ void k_nonzero_flags(const uint32_t *__restrict__ rowptr, uint32_t nv, uint32_t *__restrict__ f) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        f[v] = rowptr[v + 1] > rowptr[v] ? 1u : 0u;
+/* row_of[newid[v]] = v: the vertex at each position of the relabelled order */
+__global__ void k_invert(const uint32_t *__restrict__ newid, uint32_t nv, uint32_t *__restrict__ row_of) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) row_of[newid[v]] = v;
 }
 
-__global__ void k_split_rows(const uint32_t *__restrict__ rowptr, uint32_t nv, const uint32_t *__restrict__ pos,
+/* in-degree of the row at each position j of the plan order (row_of[j], or j
+ * when row_of is null) and whether it has in-edges */
+__global__ void k_order_deg(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ row_of, uint32_t nv,
+                            uint32_t *__restrict__ nzf, uint32_t *__restrict__ deg) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += gridDim.x * blockDim.x) {
+        const uint32_t v = row_of ? row_of[j] : j;
+        const uint32_t d = rowptr[v + 1] - rowptr[v];
+        nzf[j] = d ? 1u : 0u;
+        deg[j] = d;
+    }
+}
+
+/* nz and zero rows in plan order; an nz row's edges start at the scanned
+ * degree of its position (start[]) */
+__global__ void k_split_rows(const uint32_t *__restrict__ row_of, const uint32_t *__restrict__ nzf, uint32_t nv,
+                             const uint32_t *__restrict__ pos, const uint32_t *__restrict__ start,
                              uint32_t *__restrict__ nz_rows, uint32_t *__restrict__ nz_start,
                              uint32_t *__restrict__ zero_rows) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        uint32_t b = rowptr[v], e = rowptr[v + 1];
-        if (e > b) {
-            nz_rows[pos[v]] = v;
-            nz_start[pos[v]] = b;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += gridDim.x * blockDim.x) {
+        const uint32_t v = row_of ? row_of[j] : j;
+        if (nzf[j]) {
+            nz_rows[pos[j]] = v;
+            nz_start[pos[j]] = start[j];
         } else {
-            zero_rows[v - pos[v]] = v;
+            zero_rows[j - pos[j]] = v;
         }
     }
 }
@@ -355,13 +370,29 @@ __global__ void k_newid(const uint64_t *__restrict__ sorted, uint32_t nv, uint32
         newid[(uint32_t)(sorted[i] & mask)] = i;
 }
 
-/* col_r = newid[col] in the chunk layout of load_chunk (chunk_slot), whole
- * chunks: slots past the last edge hold 0 */
-__global__ void k_relabel(const uint32_t *__restrict__ col, uint64_t ne, uint64_t nslots,
-                          const uint32_t *__restrict__ newid, uint32_t *__restrict__ col_r) {
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nslots;
-         e += (uint64_t)gridDim.x * blockDim.x)
-        col_r[chunk_slot(e)] = e < ne ? newid[col[e]] : 0u;
+/* col_r = newid[col] of the rows in plan order, in the chunk layout of
+ * load_chunk (chunk_slot), whole chunks (slots past the last edge hold 0): one
+ * warp per chunk copies the pieces of the rows that overlap it, each row's
+ * sources in their CSR order */
+__global__ void k_relabel_rows(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
+                               const uint32_t *__restrict__ nz_rows, const uint32_t *__restrict__ nz_start,
+                               uint32_t nnz, uint64_t ne, uint32_t nchunks, const uint32_t *__restrict__ chunk_nz,
+                               const uint32_t *__restrict__ newid, uint32_t *__restrict__ col_r) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = w0; c < nchunks; c += nw) {
+        const uint64_t c0 = c * CH, c1 = c0 + CH < ne ? c0 + CH : ne;
+        for (uint64_t e = c1 + lane; e < c0 + CH; e += 32) col_r[chunk_slot(e)] = 0u;
+        for (uint32_t i = chunk_nz[c]; i < nnz; ++i) {
+            const uint64_t rs = nz_start[i];
+            if (rs >= c1) break;
+            const uint64_t re = i + 1 < nnz ? nz_start[i + 1] : ne;
+            const uint64_t lo = rs > c0 ? rs : c0, hi = re < c1 ? re : c1;
+            const uint64_t src = rowptr[nz_rows[i]];
+            for (uint64_t e = lo + lane; e < hi; e += 32) col_r[chunk_slot(e)] = newid[col[src + (e - rs)]];
+        }
+    }
 }
 
 __global__ void k_max_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t *out) {
@@ -407,10 +438,10 @@ __global__ void k_long_list(const uint4 *__restrict__ split, uint32_t nsplit, ui
 /* ---- source tiers ---------------------------------------------------------- */
 /* tier of each edge: k >= 1 when its relabelled source lies in [k w, (k+1) w)
  * for k < ntiers, else 0 */
-__global__ void k_edge_tier(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
-                            uint32_t width, uint32_t ntiers, uint8_t *__restrict__ tier) {
+__global__ void k_edge_tier(const uint32_t *__restrict__ col_r, uint64_t ne, uint32_t width, uint32_t ntiers,
+                            uint8_t *__restrict__ tier) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = newid[col[e]] / width;
+        const uint32_t k = col_r[chunk_slot(e)] / width;
         tier[e] = (uint8_t)(k < ntiers ? k : 0u);
     }
 }
@@ -421,23 +452,23 @@ __global__ void k_tier_flags(const uint8_t *__restrict__ tier, uint64_t ne, uint
         f[e] = e < ne && tier[e] == k ? 1u : 0u;
 }
 
-/* rows of tier k: a global nz row has tier-k edges when the scanned positions
- * at its two ends differ */
-__global__ void k_tier_row_flags(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ nz_rows, uint32_t nnz,
+/* rows of tier k: nz row i (edges [nz_start[i], next start or ne) in plan
+ * order) has tier-k edges when the scanned positions at its two ends differ */
+__global__ void k_tier_row_flags(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint64_t ne,
                                  const uint32_t *__restrict__ epos, uint32_t *__restrict__ rf) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
-        const uint32_t v = nz_rows[i];
-        rf[i] = epos[rowptr[v + 1]] > epos[rowptr[v]] ? 1u : 0u;
+        const uint64_t e1 = i + 1 < nnz ? nz_start[i + 1] : ne;
+        rf[i] = epos[e1] > epos[nz_start[i]] ? 1u : 0u;
     }
 }
 
-__global__ void k_tier_rows(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ nz_rows, uint32_t nnz,
+__global__ void k_tier_rows(const uint32_t *__restrict__ nz_start, uint32_t nnz, uint64_t ne,
                             const uint32_t *__restrict__ epos, const uint32_t *__restrict__ rpos,
                             uint32_t *__restrict__ idx, uint32_t *__restrict__ start) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
-        const uint32_t v = nz_rows[i];
-        const uint32_t b = epos[rowptr[v]];
-        if (epos[rowptr[v + 1]] > b) {
+        const uint64_t e1 = i + 1 < nnz ? nz_start[i + 1] : ne;
+        const uint32_t b = epos[nz_start[i]];
+        if (epos[e1] > b) {
             idx[i] = rpos[i];
             start[rpos[i]] = b;
         } else {
@@ -447,11 +478,11 @@ __global__ void k_tier_rows(const uint32_t *__restrict__ rowptr, const uint32_t 
 }
 
 /* tier k's columns in the chunk layout, relative to the tier's first id */
-__global__ void k_tier_cols(const uint32_t *__restrict__ col, uint64_t ne, const uint32_t *__restrict__ newid,
-                            const uint8_t *__restrict__ tier, uint8_t k, uint32_t first,
-                            const uint32_t *__restrict__ epos, uint32_t *__restrict__ out) {
+__global__ void k_tier_cols(const uint32_t *__restrict__ col_r, uint64_t ne, const uint8_t *__restrict__ tier,
+                            uint8_t k, uint32_t first, const uint32_t *__restrict__ epos,
+                            uint32_t *__restrict__ out) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < ne; e += (uint64_t)gridDim.x * blockDim.x)
-        if (tier[e] == k) out[chunk_slot(epos[e])] = newid[col[e]] - first;
+        if (tier[e] == k) out[chunk_slot(epos[e])] = col_r[chunk_slot(e)] - first;
 }
 
 inline unsigned grid1d(uint64_t n, uint64_t cap_per_sm = 16) {
@@ -527,35 +558,13 @@ int ensure_chunk_plan(gcg_graph *g) {
         return st;
     };
     p->nchunks = (uint32_t)((ne + CH - 1) / CH);
-    tbuf<uint32_t> flags, pos, nz_start, total;
-    if (flags.alloc(std::max<uint64_t>(nv, 1), s) || pos.alloc(std::max<uint64_t>(nv, 1), s) ||
-        total.alloc(1, s) || nz_start.alloc(std::max<uint64_t>(nv, 1), s))
-        return bail(GCG_ERR_NOMEM);
-    k_nonzero_flags<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, flags.get());
-    int st = scan_u32(flags.get(), pos.get(), nv, total.get(), s);
-    if (st) return bail(st);
-    uint32_t nnz = 0;
-    if (cudaMemcpyAsync(&nnz, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-        return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
-    p->nnz = nnz;
-    p->nzero = nv - nnz;
-    if (p->nz_rows.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_rows.alloc(std::max<uint32_t>(p->nzero, 1)) ||
-        p->od_nz.alloc(std::max<uint32_t>(nnz, 1)))
-        return bail(GCG_ERR_NOMEM);
-    k_split_rows<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), nv, pos.get(), p->nz_rows.get(), nz_start.get(),
-                                            p->zero_rows.get());
-    if (nnz) k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), g->outdeg.get(), p->od_nz.get());
-    if ((st = build_segments(nz_start.get(), nnz, ne, s, p->nchunks, p->head_bits, p->chunk_nz, p->split,
-                             p->long_split, p->nsplit, p->nlong)))
-        return bail(st);
+    int st = GCG_OK;
     /* relabel sources by out-degree so the hottest contribs sit at ids [0, hub) */
     {
         tbuf<uint32_t> dmax;
         tbuf<uint64_t> keys, tmp;
         if (dmax.alloc(1, s) || keys.alloc(std::max<uint32_t>(nv, 1), s) || tmp.alloc(std::max<uint32_t>(nv, 1), s) ||
-            p->newid.alloc(std::max<uint32_t>(nv, 1)) || p->col_r.alloc(std::max<uint64_t>((uint64_t)p->nchunks * CH, CH)) ||
-            p->nz_cidx.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_cidx.alloc(std::max<uint32_t>(p->nzero, 1)))
+            p->newid.alloc(std::max<uint32_t>(nv, 1)))
             return bail(GCG_ERR_NOMEM);
         cudaMemsetAsync(dmax.get(), 0, 4, s);
         k_max_u32<<<grid1d(nv), 256, 0, s>>>(g->outdeg.get(), nv, dmax.get());
@@ -582,16 +591,51 @@ int ensure_chunk_plan(gcg_graph *g) {
                 return bail(st);
         }
         k_newid<<<grid1d(nv), 256, 0, s>>>(sorted, nv, g->vbits, p->newid.get());
-        if (ne)
-            k_relabel<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, (uint64_t)p->nchunks * CH, p->newid.get(),
-                                                     p->col_r.get());
-        if (nnz) k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), p->newid.get(), p->nz_cidx.get());
-        if (p->nzero)
-            k_gather_u32<<<grid1d(p->nzero), 256, 0, s>>>(p->nzero, p->zero_rows.get(), p->newid.get(),
-                                                         p->zero_cidx.get());
         p->hub = std::min<uint32_t>(nv, HUB_MAX);
-        if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(GCG_ERR_CUDA, "chunk plan: relabel"));
     }
+    /* rows in relabelled order, unless this is a union whose relabelling mixes
+     * its graphs' id ranges (each graph's rows must stay one contiguous range) */
+    p->rows_relabelled = !(g->relabel_per_interval && !p->per_interval);
+    tbuf<uint32_t> row_of, nzf, pos, start, total;
+    const uint64_t nv1 = std::max<uint64_t>(nv, 1);
+    if (nzf.alloc(nv1, s) || pos.alloc(nv1, s) || start.alloc(nv1, s) || total.alloc(1, s) ||
+        (p->rows_relabelled && row_of.alloc(nv1, s)))
+        return bail(GCG_ERR_NOMEM);
+    if (p->rows_relabelled) k_invert<<<grid1d(nv), 256, 0, s>>>(p->newid.get(), nv, row_of.get());
+    k_order_deg<<<grid1d(nv), 256, 0, s>>>(g->in_rowptr.get(), p->rows_relabelled ? row_of.get() : nullptr, nv,
+                                           nzf.get(), start.get());
+    if ((st = scan_u32(nzf.get(), pos.get(), nv, total.get(), s))) return bail(st);
+    uint32_t nnz = 0;
+    if (cudaMemcpyAsync(&nnz, total.get(), 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return bail(fail(GCG_ERR_CUDA, "chunk plan: readback"));
+    if ((st = scan_u32(start.get(), start.get(), nv, nullptr, s))) return bail(st);
+    p->nnz = nnz;
+    p->nzero = nv - nnz;
+    if (p->nz_rows.alloc(std::max<uint32_t>(nnz, 1)) || p->nz_start.alloc(std::max<uint32_t>(nnz, 1)) ||
+        p->zero_rows.alloc(std::max<uint32_t>(p->nzero, 1)) || p->od_nz.alloc(std::max<uint32_t>(nnz, 1)) ||
+        p->nz_cidx.alloc(std::max<uint32_t>(nnz, 1)) || p->zero_cidx.alloc(std::max<uint32_t>(p->nzero, 1)) ||
+        p->col_r.alloc(std::max<uint64_t>((uint64_t)p->nchunks * CH, CH)))
+        return bail(GCG_ERR_NOMEM);
+    k_split_rows<<<grid1d(nv), 256, 0, s>>>(p->rows_relabelled ? row_of.get() : nullptr, nzf.get(), nv, pos.get(),
+                                            start.get(), p->nz_rows.get(), p->nz_start.get(), p->zero_rows.get());
+    if (nnz) {
+        k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), g->outdeg.get(), p->od_nz.get());
+        k_gather_u32<<<grid1d(nnz), 256, 0, s>>>(nnz, p->nz_rows.get(), p->newid.get(), p->nz_cidx.get());
+    }
+    if (p->nzero)
+        k_gather_u32<<<grid1d(p->nzero), 256, 0, s>>>(p->nzero, p->zero_rows.get(), p->newid.get(),
+                                                     p->zero_cidx.get());
+    if ((st = build_segments(p->nz_start.get(), nnz, ne, s, p->nchunks, p->head_bits, p->chunk_nz, p->split,
+                             p->long_split, p->nsplit, p->nlong)))
+        return bail(st);
+    if (p->nchunks)
+        k_relabel_rows<<<grid1d((uint64_t)p->nchunks * 32, 32), 256, 0, s>>>(
+            g->in_rowptr.get(), g->in_col.get(), p->nz_rows.get(), p->nz_start.get(), nnz, ne, p->nchunks,
+            p->chunk_nz.get(), p->newid.get(), p->col_r.get());
+    else
+        cudaMemsetAsync(p->col_r.get(), 0, CH * 4, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(GCG_ERR_CUDA, "chunk plan: relabel"));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return bail(fail(GCG_ERR_CUDA, std::string("chunk plan: ") + cudaGetErrorString(e)));
     g->cplan = p;
@@ -620,8 +664,7 @@ int ensure_tier_plan(gcg_graph *g, int ntiers, uint32_t width) {
     GCG_TRY(total.alloc(1, s));
     GCG_TRY(tp.idx.alloc((size_t)ntiers * std::max<uint32_t>(nnz, 1)));
     if (ne)
-        k_edge_tier<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, pl.newid.get(), width, (uint32_t)ntiers,
-                                                   tier.get());
+        k_edge_tier<<<grid1d(ne, 32), 256, 0, s>>>(pl.col_r.get(), ne, width, (uint32_t)ntiers, tier.get());
     for (int k = 0; k < ntiers; ++k) {
         EdgeTier &t = tp.t[k];
         k_tier_flags<<<grid1d(ne + 1, 32), 256, 0, s>>>(tier.get(), ne, (uint8_t)k, epos.get());
@@ -635,12 +678,11 @@ int ensure_tier_plan(gcg_graph *g, int ntiers, uint32_t width) {
                        : (t.first < g->nv ? std::min<uint32_t>(width, g->nv - t.first) : 0u); /* empty past nv */
         uint32_t nrows = 0;
         if (nnz) {
-            k_tier_row_flags<<<grid1d(nnz), 256, 0, s>>>(g->in_rowptr.get(), pl.nz_rows.get(), nnz, epos.get(),
-                                                        rflag.get());
+            k_tier_row_flags<<<grid1d(nnz), 256, 0, s>>>(pl.nz_start.get(), nnz, ne, epos.get(), rflag.get());
             GCG_TRY(scan_u32(rflag.get(), rpos.get(), nnz, total.get(), s));
             GCG_CUDA(cudaMemcpyAsync(&nrows, total.get(), 4, cudaMemcpyDeviceToHost, s));
             GCG_CUDA(cudaStreamSynchronize(s));
-            k_tier_rows<<<grid1d(nnz), 256, 0, s>>>(g->in_rowptr.get(), pl.nz_rows.get(), nnz, epos.get(), rpos.get(),
+            k_tier_rows<<<grid1d(nnz), 256, 0, s>>>(pl.nz_start.get(), nnz, ne, epos.get(), rpos.get(),
                                                    tp.idx.get() + (size_t)k * nnz, start.get());
         }
         t.nrows = nrows;
@@ -650,8 +692,8 @@ int ensure_tier_plan(gcg_graph *g, int ntiers, uint32_t width) {
         GCG_TRY(t.col.alloc(slots));
         GCG_CUDA(cudaMemsetAsync(t.col.get(), 0, slots * 4, s));
         if (ne)
-            k_tier_cols<<<grid1d(ne, 32), 256, 0, s>>>(g->in_col.get(), ne, pl.newid.get(), tier.get(), (uint8_t)k,
-                                                       t.first, epos.get(), t.col.get());
+            k_tier_cols<<<grid1d(ne, 32), 256, 0, s>>>(pl.col_r.get(), ne, tier.get(), (uint8_t)k, t.first,
+                                                       epos.get(), t.col.get());
         GCG_TRY(t.nzsum.alloc(std::max<uint32_t>(nrows, 1)));
         GCG_TRY(t.parts.alloc((size_t)2 * t.nchunks + 2));
         GCG_LAUNCH_CHECK();

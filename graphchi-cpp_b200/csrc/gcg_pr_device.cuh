@@ -329,11 +329,17 @@ struct ChunkPlan {
     TierPlan tiers;
     uint32_t tune_tiers = 1; /* source tiers of the edge phase (1: one pass) */
     uint32_t nchunks = 0, nnz = 0, nzero = 0, nsplit = 0;
-    dbuf<uint32_t> nz_rows, zero_rows, head_bits, chunk_nz, od_nz;
+    /* rows are taken in relabelled order (row j is the vertex relabelled j), so
+     * the vertex pass writes contributions in sequence; false only for a union
+     * whose relabelling could not keep every graph's id range */
+    bool rows_relabelled = true;
+    /* nz row i: original vertex id, first edge position in col_r's order */
+    dbuf<uint32_t> nz_rows, nz_start, zero_rows, head_bits, chunk_nz, od_nz;
     dbuf<uint4> split;
     uint32_t nlong = 0;
     dbuf<uint32_t> long_split; /* split rows spanning more than LONG_SPAN chunks */
-    /* sources relabelled by out-degree (descending): col_r = newid[col] */
+    /* sources relabelled by out-degree (descending): col_r holds newid[col] of
+     * the rows in plan order, each row's sources ascending */
     uint32_t hub = 0;
     dbuf<uint32_t> newid, col_r, nz_cidx, zero_cidx;
     /* launch configuration of the edge kernel (gcg_pagerank_autotune):
