@@ -235,13 +235,16 @@ uint32_t id_bits(uint32_t maxid) {
  * PIPE_CHUNKS pieces on a copy stream; each piece is scanned (self-loops, max
  * id, range) as soon as it lands; its keys (dst << 32 | src) are radix-sorted on
  * the sort stream while later pieces are still in flight (only the digits its
- * largest id needs), and sorted runs are merged pairwise as soon as two of equal
- * length exist, all but the last merge, which the caller fuses with the
- * duplicate filter and the CSR decode. After the last piece lands, only its sort
- * and the merges that take it in remain. The two final runs come back in
- * run[0], run[1] (pointer, length); the scan results of all pieces are combined
- * into *info. With outcnt, the raw out-degree of every id is counted into
- * outcnt (grown as larger ids arrive; outgrown buffers are kept in old). */
+ * largest id needs) and merged at once into one run of all earlier pieces,
+ * except the last piece, whose merge the caller fuses with the duplicate filter
+ * and the CSR decode. After the last piece lands, only its sort remains. The
+ * run of the earlier pieces occupies [0, len) of keys or tmp (the buffers swap
+ * at every merge); a sorted piece is moved to that buffer at its own offset, so
+ * a merge never writes over a run it reads. The two final runs come back in
+ * run[0], run[1] (pointer, length; both in one buffer); the scan results of all
+ * pieces are combined into *info. With outcnt, the raw out-degree of every id is
+ * counted into outcnt (grown as larger ids arrive; outgrown buffers are kept in
+ * old). */
 struct SortedRuns {
     const uint64_t *p[2];
     uint64_t n[2];
@@ -303,12 +306,8 @@ int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bo
     }
     if (cudaGetLastError() != cudaSuccess) return done(fail(GCG_ERR_CUDA, "edge pipeline: queueing failed"));
 
-    struct Run {
-        int level;
-        uint64_t start, len;
-    };
-    Run stack[PIPE_CHUNKS + 1];
-    int top = 0;
+    uint64_t *acc = keys; /* buffer of the run of the earlier pieces, at [0, acc_len) */
+    uint64_t acc_len = 0;
     info->kept = 0;
     info->maxid = 0;
     info->bad = 0;
@@ -353,25 +352,27 @@ int sort_host_edges(const uint32_t *src_u, const uint32_t *dst_u, uint64_t m, bo
             if ((st = radix_sort_u64(keys + k0, tmp + k0, kn, 0, cb, &r1, ks))) return done(st);
             uint64_t *o1 = (r1 == keys + k0) ? tmp + k0 : keys + k0;
             if ((st = radix_sort_u64(r1, o1, kn, 32, 32 + cb, &r2, ks))) return done(st);
-            if (r2 != keys + k0 &&
-                cudaMemcpyAsync(keys + k0, r2, kn * 8, cudaMemcpyDeviceToDevice, ks) != cudaSuccess)
+            if (i == 0) acc = (r2 == keys + k0) ? keys : tmp; /* the first run stays where it was sorted */
+            if (r2 != acc + k0 && cudaMemcpyAsync(acc + k0, r2, kn * 8, cudaMemcpyDeviceToDevice, ks) != cudaSuccess)
                 return done(fail(GCG_ERR_CUDA, "edge pipeline: run copy"));
         }
-        /* runs of level L live in keys (L even) or tmp (L odd); the final merge is the caller's */
-        stack[top++] = Run{0, k0, kn};
-        while (top >= 2 && stack[top - 1].level == stack[top - 2].level && !(i == K - 1 && top == 2)) {
-            const Run b = stack[--top], a = stack[--top];
-            uint64_t *from = (a.level & 1) ? tmp : keys, *to = (a.level & 1) ? keys : tmp;
-            if ((st = merge_u64(from + a.start, a.len, from + b.start, b.len, to + a.start, ks))) return done(st);
-            stack[top++] = Run{a.level + 1, a.start, a.len + b.len};
+        if (i == 0 || i == K - 1) {
+            if (i == 0) acc_len = kn;
+            continue; /* the last piece's merge is the caller's */
+        }
+        if (kn) {
+            uint64_t *to = (acc == keys) ? tmp : keys;
+            if ((st = merge_u64(acc, acc_len, acc + k0, kn, to, ks))) return done(st);
+            acc = to;
+            acc_len += kn;
         }
     }
-    if (top != 2 || stack[0].level != stack[1].level)
-        return done(fail(GCG_ERR_CUDA, "edge pipeline: runs left unmerged"));
-    for (int r = 0; r < 2; ++r) {
-        runs->p[r] = ((stack[r].level & 1) ? tmp : keys) + stack[r].start;
-        runs->n[r] = stack[r].len;
-    }
+    const uint64_t kl = kmul * std::min<uint64_t>(m, (uint64_t)(K - 1) * cm); /* the last piece's offset */
+    if (acc_len != kl) return done(fail(GCG_ERR_CUDA, "edge pipeline: runs left unmerged"));
+    runs->p[0] = acc;
+    runs->n[0] = acc_len;
+    runs->p[1] = acc + kl;
+    runs->n[1] = kmul * m - kl;
     if (cudaStreamSynchronize(ks) != cudaSuccess || cudaGetLastError() != cudaSuccess)
         return done(fail(GCG_ERR_CUDA, std::string("edge pipeline: ") + cudaGetErrorString(cudaGetLastError())));
     return done(GCG_OK);

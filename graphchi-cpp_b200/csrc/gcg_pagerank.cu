@@ -372,8 +372,10 @@ __global__ void k_newid(const uint64_t *__restrict__ sorted, uint32_t nv, uint32
 
 /* col_r = newid[col] of the rows in plan order, in the chunk layout of
  * load_chunk (chunk_slot), whole chunks (slots past the last edge hold 0): one
- * warp per chunk copies the pieces of the rows that overlap it, each row's
- * sources in their CSR order */
+ * warp per chunk. The rows overlapping the chunk are consecutive from
+ * chunk_nz[c]; the warp reads their extents and CSR offsets 32 rows at a time
+ * (one lane per row), then copies each row's piece with all lanes, each row's
+ * sources in their CSR order. */
 __global__ void k_relabel_rows(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ col,
                                const uint32_t *__restrict__ nz_rows, const uint32_t *__restrict__ nz_start,
                                uint32_t nnz, uint64_t ne, uint32_t nchunks, const uint32_t *__restrict__ chunk_nz,
@@ -384,13 +386,27 @@ __global__ void k_relabel_rows(const uint32_t *__restrict__ rowptr, const uint32
     for (uint64_t c = w0; c < nchunks; c += nw) {
         const uint64_t c0 = c * CH, c1 = c0 + CH < ne ? c0 + CH : ne;
         for (uint64_t e = c1 + lane; e < c0 + CH; e += 32) col_r[chunk_slot(e)] = 0u;
-        for (uint32_t i = chunk_nz[c]; i < nnz; ++i) {
-            const uint64_t rs = nz_start[i];
-            if (rs >= c1) break;
-            const uint64_t re = i + 1 < nnz ? nz_start[i + 1] : ne;
-            const uint64_t lo = rs > c0 ? rs : c0, hi = re < c1 ? re : c1;
-            const uint64_t src = rowptr[nz_rows[i]];
-            for (uint64_t e = lo + lane; e < hi; e += 32) col_r[chunk_slot(e)] = newid[col[src + (e - rs)]];
+        for (uint32_t ib = chunk_nz[c];; ib += 32u) {
+            const uint32_t i = ib + lane;
+            uint64_t rs = 0, re = 0, src = 0;
+            bool have = false;
+            if (i < nnz) {
+                rs = nz_start[i];
+                if (rs < c1) {
+                    have = true;
+                    re = i + 1 < nnz ? nz_start[i + 1] : ne;
+                    src = rowptr[nz_rows[i]];
+                }
+            }
+            const uint32_t hm = __ballot_sync(0xFFFFFFFFu, have); /* a prefix of the lanes */
+            for (uint32_t m = hm; m; m &= m - 1u) {
+                const int j = __ffs((int)m) - 1;
+                const uint64_t rsj = __shfl_sync(0xFFFFFFFFu, rs, j), rej = __shfl_sync(0xFFFFFFFFu, re, j);
+                const uint64_t srcj = __shfl_sync(0xFFFFFFFFu, src, j);
+                const uint64_t lo = rsj > c0 ? rsj : c0, hi = rej < c1 ? rej : c1;
+                for (uint64_t e = lo + lane; e < hi; e += 32) col_r[chunk_slot(e)] = newid[col[srcj + (e - rsj)]];
+            }
+            if (hm != 0xFFFFFFFFu) break; /* the chunk's last row was in this batch */
         }
     }
 }
