@@ -133,15 +133,29 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     pdl_wait();
     pdl_launch_next();
     if (*(volatile const int *)a.done) return;
-    extern __shared__ float s_hub[];
+    extern __shared__ __align__(16) float s_hub[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_fail;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint64_t pol_stream = policy_evict_first();
     const uint64_t pol_keep = policy_evict_last();
-    /* hub cache: contribs of the highest out-degree sources (relabelled 0..hub-1) */
-    load_hub(a, s_hub);
+    /* hub cache: contribs of the highest out-degree sources (relabelled
+     * 0..hub-1), staged by one bulk copy (TMA) of its whole 16-byte part (c_old
+     * and the hub are 16-byte aligned) while the warps load their first chunk;
+     * the last hub % 4 entries by plain loads */
+    const uint32_t hub4 = a.hub & ~3u;
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(&s_bar, 1);
+    }
     __syncthreads();
+    if (threadIdx.x == 0 && hub4) {
+        mbar_arrive_expect_tx(&s_bar, hub4 * 4u);
+        bulk_copy_g2s(s_hub, a.c_old, hub4 * 4u, &s_bar);
+    }
+    for (uint32_t i = hub4 + threadIdx.x; i < a.hub; i += blockDim.x) s_hub[i] = __ldcg(a.c_old + i);
 
     /* Warp w takes runs of a.run consecutive chunks: runs w, w + nwarps, ...
      * Software pipeline: while a chunk's gathers are in flight, the next chunk's
@@ -150,6 +164,19 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_pr_edges(SweepArgs a) {
     uint64_t q = gwarp, ch = q * R, end = ch + R < nch ? ch + R : nch;
     uint32_t col[EPL], flags = 0, nvalid = 0, base = 0;
     if (ch < end) load_chunk(a, (uint32_t)ch, lane, pol_stream, col, flags, nvalid, base, a.ne);
+    if (hub4) { /* bounded wait for the hub copy */
+        bool ok = false;
+        for (long long spin = 0; !ok && spin < MBAR_SPIN; ++spin) ok = mbar_try_wait(&s_bar, 0u);
+        if (!ok) s_fail = 1;
+    }
+    __syncthreads(); /* also publishes the plainly loaded hub entries */
+    if (s_fail) { /* the copy did not complete: report it and stop the solve */
+        if (threadIdx.x == 0) {
+            atomicExch(a.err, 1);
+            atomicExch(a.done, 1);
+        }
+        return;
+    }
     while (ch < end) {
         float val[EPL];
         if (TEX) {
@@ -862,6 +889,7 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
     a.ticket = ctl.get();
     a.done = (int *)(ctl.get() + 1);
     a.sweeps_done = (int *)(ctl.get() + 2);
+    a.err = (int *)(ctl.get() + 3);
     a.res_log = dres.get();
     a.last_res = dres.get() + max_sweeps;
     a.delta_log = (p->delta_log || p->work_log) ? dres.get() + max_sweeps + 1 : nullptr;
@@ -1000,8 +1028,12 @@ static int pagerank_jacobi(gcg_graph *g, const gcg_pr_params *p, float *out_rank
         return status;
     }
 
-    uint32_t h_ctl[4];
+    uint32_t h_ctl[4]; /* ticket, done, sweeps_done, err */
     GCG_CUDA(cudaMemcpy(h_ctl, ctl.get(), sizeof(h_ctl), cudaMemcpyDeviceToHost));
+    if (h_ctl[3]) {
+        for (auto e : sweep_ev) cudaEventDestroy(e);
+        return fail(GCG_ERR_TIMEOUT, "pagerank: the shared-memory hub copy did not complete");
+    }
     const int sweeps = (int)h_ctl[2];
     const int done = (int)h_ctl[1];
     double sweep_ms = 0.0;

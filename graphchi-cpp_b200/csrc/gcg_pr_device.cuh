@@ -38,6 +38,38 @@ __device__ __forceinline__ float ld_keep_f32(const float *p, uint64_t pol) {
     return r;
 }
 
+/* ---- bulk copies into shared memory (TMA), completion on an mbarrier ------ */
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    /* the initialised barrier is visible to the copy engine before any copy names it */
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+/* the calling thread's arrival, announcing `bytes` of copies that complete on bar */
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+/* global -> shared bulk copy; dst, src 16-byte aligned, bytes a multiple of 16 */
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+/* bound on the polls of a barrier wait (each try_wait may itself suspend the
+ * thread for a while): far above any copy's completion time */
+constexpr long long MBAR_SPIN = 1ll << 22;
+
 /* ---- sweep kernels ------------------------------------------------------ */
 struct SweepArgs {
     /* graph / plan */
@@ -68,6 +100,7 @@ struct SweepArgs {
     uint32_t run;    /* edge kernel: each warp takes runs of this many consecutive chunks (>= 1) */
     double *delta_log; /* optional: per sweep, sum |r' - r| (FP64) */
     unsigned long long tex_old; /* texture object over c_old (edge kernel's texture-path gathers) */
+    int *err;                   /* edge kernel: set when the hub copy's wait ran out */
     /* source tiers (vertex kernel): a row's sum is the sum over tiers k of
      * tier_sum[k][tier_idx[k * nnz + i]] (entries equal to GCG_NO_SOURCE: no
      * in-edge of the row in that tier), tiers added in order; ntiers <= 1: nzsum */
@@ -244,11 +277,11 @@ __device__ __forceinline__ void reduce_chunk(const A &a, uint32_t ch, uint32_t l
 constexpr int EDGE_THREADS = 1024;
 constexpr uint32_t HUB_MAX = 49152; /* 192 KB of shared memory */
 /* Default hub of the edge kernel: the largest that fits the 164 KB shared-memory
- * carve-out (163 KB + the 1 KB the driver reserves per block), leaving ~92 KB of
- * L1; one more 1 KB step moves the SM to the 196 KB carve-out and halves L1. At
- * R-MAT scale 24 the edge kernel takes 0.693 ms with it (and chunk runs of 2)
- * against 0.729 ms with the full 192 KB hub. */
-constexpr uint32_t HUB_DEFAULT = 41728;
+ * carve-out together with the kernel's 16 bytes of static shared memory (the
+ * hub copy's mbarrier) and the 1 KB the driver reserves per block, leaving
+ * ~92 KB of L1; one more byte moves the SM to the 196 KB carve-out and cuts L1
+ * by a third (the edge kernel then takes 16 % longer at R-MAT scale 24). */
+constexpr uint32_t HUB_DEFAULT = 41724;
 constexpr uint32_t RUN_DEFAULT = 1; /* with texture gathers, 0.4 % faster than runs of 2 */
 
 /* Sweep workspace of one graph, reused across calls. */

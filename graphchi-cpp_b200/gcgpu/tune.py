@@ -6,7 +6,7 @@ measured copy bandwidth in MEASURED_PEAKS.json, else 6650 GB/s). Every
 configuration computes the same sums in the same order except source tiers
 (tiers > 1), whose rows add per-tier partial sums.
 
-    python -m gcgpu.tune --scale 24 [--tiers 1 2 3 4] [--hub 41728 32768]
+    python -m gcgpu.tune --scale 24 [--tiers 1 2 3 4] [--hub 41724 32768]
 
 With --batch LO HI it reports the many-graph persistent launch instead: 64
 graphs, vertex counts log-uniform in [LO, HI] (seeded), alternating
@@ -81,7 +81,7 @@ def main():
     ap.add_argument("--scale", type=int, nargs="+", default=[24])
     ap.add_argument("--ef", type=int, default=16)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--hub", type=int, nargs="+", default=[41728])
+    ap.add_argument("--hub", type=int, nargs="+", default=[41724])
     ap.add_argument("--tiers", type=int, nargs="+", default=[1])
     ap.add_argument("--batch", type=float, nargs=2, default=None, metavar=("LO", "HI"))
     args = ap.parse_args()

@@ -239,11 +239,11 @@ int gcg_pagerank(gcg_graph *g, const gcg_pr_params *params, float *out_rank, gcg
  * depend on it): hub_entries = shared-memory contribution cache entries (sources
  * whose out-degree rank is below it are read from shared memory; capped at the
  * plan's 49152), chunk_run = consecutive 256-edge chunks a warp takes at a time
- * (1 = warps stride chunk by chunk). Default: 41728 entries (the largest hub
+ * (1 = warps stride chunk by chunk). Default: 41724 entries (the largest hub
  * that leaves the SM its 164 KB shared-memory carve-out, so L1 keeps ~92 KB) and
  * chunk_run 1, the fastest measured at R-MAT scale 24. gcg_pagerank_autotune
  * times `sweeps` fixed sweeps (the whole sweep, device time) of each candidate
- * (hub entries {0, 16384, 32768, 41728, 49152, the plan's} x runs {1, 2, 4, 16},
+ * (hub entries {0, 16384, 32768, 41724, 49152, the plan's} x runs {1, 2, 4, 16},
  * then 2..4 source tiers of the chosen hub, gcg_pagerank_set_tiers), keeps the
  * fastest for later calls on this graph and reports it (outputs may be NULL;
  * gcg_pagerank_get_tiers gives the tier count chosen). */
@@ -312,8 +312,8 @@ int gcg_batch_pagerank(gcg_batch *b, const gcg_pr_params *params, float *out_ran
  * depend on it). Candidates: shared-memory hub entries per graph (each graph's
  * sources whose out-degree rank within the graph is below it are read from
  * shared memory: the degree threshold of the cache) in {0, 8192, 16384, 32768,
- * 41728, 49152, the plan's}. Each CTA takes an equal share of the active graphs'
- * chunks. Only when the union's ids are too wide for per-graph relabelling
+ * 41724, 49152, the plan's}. CTAs take ranges of the active graphs' chunks from a
+ * device cursor, large ranges first and smaller ones as the work runs out. Only when the union's ids are too wide for per-graph relabelling
  * (more than 64 sort-key bits) is there one hub over the union's hottest sources
  * and the edge phase's work distribution a second candidate: warps striding over
  * the chunks (queue_run 0) or taking runs of 1, 4 or 16 chunks from a device

@@ -129,7 +129,7 @@ def test_pagerank_gs_exact_scale20_vs_reference():
 @pytest.mark.parametrize("scale", [20, 22])
 def test_pagerank_converged_vs_fp64_oracle(scale):
     """Jacobi to normalised L1 residual 1e-8 at scales where V is far above the
-    41,728-entry shared-memory hub (texture-path gathers and long-row fix-up both
+    41,724-entry shared-memory hub (texture-path gathers and long-row fix-up both
     run): within 1e-6 of the FP64 oracle's fixed point (residual 1e-12) and of the
     FP32 oracle iteration run to the same tolerance."""
     s, d = O.rmat_edges(scale, 16 << scale, seed=9)
