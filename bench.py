@@ -58,13 +58,12 @@ def load_peaks():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pr_edges
-# launch per edge at R-MAT scale 24: 1.130 GB + 18.1 MB for 263,430,537 edges in
-# one ncu capture of the full-size workload (ncu --metrics
-# dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-# --clock-control none -k regex:k_pr_edges -s 2 -c 1 python bench.py --steps 1
-# --warmup 0 --e2e-steps 0 --e2e-warmup 0 --no-extras --no-cpu-baseline
-# --no-oracle-check); traffic scales with the edges swept.
-TRAFFIC_BYTES_PER_EDGE = 4.36
+# launch per edge at R-MAT scale 24: 1.130 GB + 15.7 MB for 263,430,537 edges in
+# one ncu capture of the full-size workload (ncu --set full --clock-control none
+# -k regex:"k_pr_(edges|vertex)" -s 4 -c 2 python bench.py --steps 1 --warmup 1
+# --e2e-steps 0 --e2e-warmup 0 --no-extras --no-cpu-baseline --no-oracle-check);
+# traffic scales with the edges swept.
+TRAFFIC_BYTES_PER_EDGE = 4.35
 
 
 class ClockSampler:
