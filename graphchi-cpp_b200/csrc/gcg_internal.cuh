@@ -171,8 +171,11 @@ struct gcg_graph {
     gcg::PprPlan *pplan = nullptr;
     /* level schedule of the exact Gauss-Seidel modes, built on first use */
     gcg::GsPlan *gsplan = nullptr;
-    /* PageRank plan option: relabel sources by out-degree within each interval
-     * (the many-graph union: every graph keeps its own id range) */
+    /* PageRank plan options of the many-graph union: it is one (each interval a
+     * graph, whose rows must stay one contiguous range), and whether to relabel
+     * its sources by out-degree within each interval (every graph keeps its own
+     * id range) */
+    bool union_of_graphs = false;
     bool relabel_per_interval = false;
 
     ~gcg_graph();

@@ -602,7 +602,7 @@ struct gcg_batch {
 
 namespace gcg {
 
-static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
+static int batch_build(gcg_graph *const *graphs, uint32_t ng, uint32_t flags, gcg_batch *b) {
     b->ng = ng;
     b->voff.assign(ng + 1, 0);
     b->eoff.assign(ng + 1, 0);
@@ -651,7 +651,9 @@ static int batch_build(gcg_graph *const *graphs, uint32_t ng, gcg_batch *b) {
     u->intervals_host = (uint32_t *)malloc((size_t)ng * 4);
     for (uint32_t g = 0; g < ng; ++g) u->intervals_host[g] = b->voff[g + 1] - 1;
     GCG_CUDA(cudaMemcpy(u->intervals_dev.get(), u->intervals_host, (size_t)ng * 4, cudaMemcpyHostToDevice));
-    u->relabel_per_interval = true; /* every graph keeps its id range: per-graph hubs */
+    u->union_of_graphs = true;
+    /* by default every graph keeps its id range: per-graph hubs */
+    u->relabel_per_interval = (flags & GCG_BATCH_ONE_HUB) == 0;
     GCG_TRY(ensure_chunk_plan(u));
     const ChunkPlan &pl = *u->cplan;
     /* per-graph ranges (padding vertices excluded) by binary search on the device:
@@ -1026,14 +1028,19 @@ using namespace gcg;
 extern "C" {
 
 int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out) {
+    return gcg_batch_create_ex(graphs, ngraphs, 0u, out);
+}
+
+int gcg_batch_create_ex(gcg_graph *const *graphs, uint32_t ngraphs, uint32_t flags, gcg_batch **out) {
     if (!graphs || !out) return fail(GCG_ERR_INVALID, "gcg_batch_create: null argument");
+    if (flags & ~GCG_BATCH_ONE_HUB) return fail(GCG_ERR_INVALID, "gcg_batch_create_ex: unknown flags");
     *out = nullptr;
     if (ngraphs == 0 || ngraphs > NG_MAX)
         return fail(GCG_ERR_INVALID, "gcg_batch_create: ngraphs must be 1.." + std::to_string(NG_MAX));
     for (uint32_t g = 0; g < ngraphs; ++g)
         if (!graphs[g]) return fail(GCG_ERR_INVALID, "gcg_batch_create: null graph");
     gcg_batch *b = new gcg_batch();
-    int st = batch_build(graphs, ngraphs, b);
+    int st = batch_build(graphs, ngraphs, flags, b);
     if (st == GCG_OK && cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
         b->own = nullptr;
         st = fail(GCG_ERR_CUDA, "gcg_batch_create: cannot create a stream");

@@ -638,7 +638,7 @@ int ensure_chunk_plan(gcg_graph *g) {
     }
     /* rows in relabelled order, unless this is a union whose relabelling mixes
      * its graphs' id ranges (each graph's rows must stay one contiguous range) */
-    p->rows_relabelled = !(g->relabel_per_interval && !p->per_interval);
+    p->rows_relabelled = !g->union_of_graphs || p->per_interval;
     tbuf<uint32_t> row_of, nzf, pos, start, total;
     const uint64_t nv1 = std::max<uint64_t>(nv, 1);
     if (nzf.alloc(nv1, s) || pos.alloc(nv1, s) || start.alloc(nv1, s) || total.alloc(1, s) ||

@@ -39,6 +39,7 @@ PR_GS_EXACT = 1
 PR_DELTA = 2
 PR_GS_EDGE = 3
 PR_TIME_SWEEPS = 0x1
+BATCH_ONE_HUB = 0x1
 
 # Every symbol include/gcgpu.h declares (checked by the CPU test suite).
 EXPORTED = [
@@ -48,7 +49,7 @@ EXPORTED = [
     "gcg_pr_params_default", "gcg_pagerank", "gcg_connected_components", "gcg_triangle_count",
     "gcg_generate_rmat", "gcg_generate_er", "gcg_last_error", "gcg_version",
     "gcg_pagerank_csr_noalloc", "gcg_ppr_batched",
-    "gcg_batch_create", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
+    "gcg_batch_create", "gcg_batch_create_ex", "gcg_batch_vertex_offsets", "gcg_batch_set_stream", "gcg_batch_pagerank", "gcg_batch_free",
     "gcg_batch_autotune", "gcg_batch_get_config", "gcg_batch_set_config",
     "gcg_pagerank_set_config", "gcg_pagerank_get_config", "gcg_pagerank_autotune",
     "gcg_pagerank_set_tiers", "gcg_pagerank_get_tiers",
@@ -151,7 +152,7 @@ _pr_set_tiers = _sig("gcg_pagerank_set_tiers", _i, _vp, _u32)
 _pr_get_tiers = _sig("gcg_pagerank_get_tiers", _i, _vp, C.POINTER(_u32))
 _pr_autotune = _sig("gcg_pagerank_autotune", _i, _vp, _i, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(C.c_double))
 _ppr = _sig("gcg_ppr_batched", _i, _vp, _vp, _u32, C.POINTER(PrParams), _vp, C.POINTER(PrStats))
-_batch_create = _sig("gcg_batch_create", _i, C.POINTER(_vp), _u32, C.POINTER(_vp))
+_batch_create = _sig("gcg_batch_create_ex", _i, C.POINTER(_vp), _u32, _u32, C.POINTER(_vp))
 _batch_offsets = _sig("gcg_batch_vertex_offsets", _i, _vp, _vp)
 _batch_set_stream = _sig("gcg_batch_set_stream", _i, _vp, _vp)
 _batch_pagerank = _sig("gcg_batch_pagerank", _i, _vp, C.POINTER(PrParams), _vp, _vp, _vp, C.POINTER(PrStats))
@@ -480,10 +481,12 @@ def pagerank_csr_noalloc(in_rowptr, in_col, outdeg, out, num_vertices=None, max_
 class Batch:
     """Many graphs solved by one persistent launch (gcg_batch_*)."""
 
-    def __init__(self, graphs):
+    def __init__(self, graphs, one_hub=False):
+        """one_hub: one shared-memory hub over the union's hottest sources, rows in
+        id order (GCG_BATCH_ONE_HUB), instead of a hub per graph."""
         arr = (_vp * len(graphs))(*[g.handle for g in graphs])
         h = _vp()
-        check(_batch_create(arr, len(graphs), C.byref(h)))
+        check(_batch_create(arr, len(graphs), BATCH_ONE_HUB if one_hub else 0, C.byref(h)))
         self._h = h
         self.ngraphs = len(graphs)
         off = np.zeros(len(graphs) + 1, dtype=np.uint64)

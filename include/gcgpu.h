@@ -292,6 +292,15 @@ int gcg_ppr_batched(gcg_graph *g, const uint32_t *sources, uint32_t nsources, co
  * 2^32-1 vertices and edges in total. */
 typedef struct gcg_batch gcg_batch;
 int gcg_batch_create(gcg_graph *const *graphs, uint32_t ngraphs, gcg_batch **out);
+/* The same with flags. GCG_BATCH_ONE_HUB: relabel the union's sources by
+ * out-degree over the whole union (one shared-memory hub holding the union's
+ * hottest sources, rows kept in id order) instead of within each graph's id
+ * range (a hub per graph, rows in relabelled order; the default, and the only
+ * layout whose ranks are bit-identical to each graph's own gcg_pagerank solve).
+ * Without the flag the one-hub layout is taken only when the union's ids are too
+ * wide for per-graph relabelling (more than 64 sort-key bits). */
+#define GCG_BATCH_ONE_HUB 1u
+int gcg_batch_create_ex(gcg_graph *const *graphs, uint32_t ngraphs, uint32_t flags, gcg_batch **out);
 /* First union vertex id of each graph (ngraphs+1 entries, last = total). */
 int gcg_batch_vertex_offsets(const gcg_batch *b, uint64_t *offsets);
 int gcg_batch_set_stream(gcg_batch *b, void *stream);

@@ -123,3 +123,32 @@ def test_batch_graph_replay_and_launch_configs_keep_results():
         assert np.array_equal(r1, r4) and np.array_equal(sw1, sw4)
     for g in gs:
         g.free()
+
+
+def test_batch_one_hub_layout_against_oracle():
+    """GCG_BATCH_ONE_HUB: one hub over the union's hottest sources and the union's
+    rows in id order (the layout the batch falls back to when its ids are too wide
+    for per-graph relabelling). Chunk boundaries differ from the single-graph
+    plans, so each graph is checked against the oracle: the FP32 iteration at
+    fixed sweeps and the FP64 fixed point at the tolerance; every launch
+    configuration of this layout gives the same bits."""
+    gs = make_graphs()
+    oracles = [O.OracleGraph(*edges(*sp)) for sp in SPECS]
+    with gcgpu.Batch(gs, one_hub=True) as b:
+        r, sw, res, st = b.pagerank(max_sweeps=20, tol=0.0)
+        assert list(sw) == [20] * len(gs)
+        for g, go, part in zip(gs, oracles, b.split(r)):
+            assert g.num_vertices == go.nv and g.num_edges == go.ne
+            ref, n, _ = go.pagerank_jacobi(max_sweeps=20)
+            assert nl1(part, ref) <= 1e-6
+        r1, sw1, res1, st = b.pagerank(max_sweeps=1000, tol=1e-8)
+        assert st.converged == 1
+        for k, (go, part) in enumerate(zip(oracles, b.split(r1))):
+            f64, _ = go.pagerank_jacobi_f64(max_sweeps=3000, tol=1e-12)
+            assert nl1(part, f64) <= 1e-6, k
+        for hub, run in [(0, 0), (8192, 1), (100000, 4), (16384, 16)]:
+            b.set_config(hub, run)
+            r3, sw3, res3, _ = b.pagerank(max_sweeps=1000, tol=1e-8)
+            assert np.array_equal(r1, r3) and np.array_equal(sw1, sw3) and np.array_equal(res1, res3), (hub, run)
+    for g in gs:
+        g.free()
