@@ -17,18 +17,19 @@
  *                  edge (the 24576 highest out-degree sources from shared memory),
  *                  a warp segmented reduction of (sum, max, sum), rows crossing
  *                  chunks completed in chunk order
- *   k_warm_infer   fused features + network on tensor cores (mma.sync m16n8k16,
- *                  BF16 operands, FP32 accumulation) over the vertices with
- *                  in-edges (the others are set to teleport): a warp runs 16 vertices,
- *                  layer 1 as 8 MMAs (K = 8 features padded to 16), layer 2 as 32
- *                  MMAs with the layer-1 accumulators re-packed in registers as
- *                  the A operand, layer 3 and exp on the FP32 pipes
+ *   k_warm_infer   the network on the 5th-generation tensor cores (tcgen05.mma,
+ *                  BF16 operands in shared memory, FP32 accumulators in tensor
+ *                  memory) over the vertices with in-edges (the others are set to
+ *                  teleport): a CTA takes tiles of 128 vertices, layer 1 as one
+ *                  M128 x N64 x K16 MMA (8 features padded to 16), layer 2 as four
+ *                  K16 steps, each layer read back with tcgen05.ld; layer 3 and exp
+ *                  on the FP32 pipes
  *   k_mlp_fwd_bwd  training: one sample per thread on the FP32 pipes (forward,
  *                  backward), then per-block weight gradients as small block
  *                  GEMMs over shared-memory activation tiles, one partial slot
  *                  per block (no atomics: the sum order is fixed)
  *   k_mlp_adam     fixed-order sum of the block partials, Adam on the FP32 master
- *                  weights, the BF16-rounded copy and the MMA operand fragments
+ *                  weights, then the BF16-rounded copy the inference reads
  */
 #include <math.h>
 #include <stdio.h>
@@ -52,8 +53,6 @@ constexpr int NP = GCG_MLP_NPARAMS;
 /* offsets in the flat parameter vector */
 constexpr int OW1 = 0, OB1 = OW1 + NH * NIN, OW2 = OB1 + NH, OB2 = OW2 + NH * NH, OW3 = OB2 + NH, OB3 = OW3 + NH;
 static_assert(OB3 + 1 == NP, "parameter layout");
-constexpr int NFRAG1 = 8 * 32;      /* layer-1 B fragments: 8 n-tiles x 32 lanes, one b32 each */
-constexpr int NFRAG2 = 4 * 8 * 64;  /* layer-2 B fragments: 4 k-steps x 8 n-tiles x 32 lanes x 2 b32 */
 constexpr int TRAIN_T = 128;        /* samples per training tile (one per thread) */
 constexpr int HS = NH + 1;          /* padded row stride of the activation tiles */
 
@@ -133,36 +132,33 @@ __global__ void __launch_bounds__(EDGE_THREADS, 1) k_warm_agg_edges(AggArgs a, A
     }
 }
 
-/* rows crossing chunks, in chunk order (the order of the PageRank fix-up) */
-__global__ void __launch_bounds__(256) k_warm_agg_fix(const uint4 *__restrict__ split, uint32_t nsplit, AggOut o) {
+/* rows crossing chunks, in chunk order (the order of the PageRank fix-up): the
+ * long ones (more than LONG_SPAN chunks; rows in relabelled order put them next to each
+ * other) one per warp over the grid, lane-strided partials reduced by an xor
+ * tree; the others one per lane */
+__global__ void __launch_bounds__(256) k_warm_agg_fix(const uint4 *__restrict__ split, uint32_t nsplit,
+                                                      const uint32_t *__restrict__ long_split, uint32_t nlong,
+                                                      AggOut o) {
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t wb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; wb < nsplit; wb += nwarps * 32u) {
-        const uint32_t k = wb + lane;
-        const bool valid = k < nsplit;
-        uint4 sp = make_uint4(0, 0, 0, 0);
-        if (valid) sp = split[k];
-        const bool lng = valid && (sp.z - sp.y) > 8u;
-        if (valid && !lng) {
+    for (uint32_t r = gwarp; r < nlong; r += nwarps) {
+        const uint4 sp = split[long_split[r]];
+        Agg3 v = Agg3{0.0f, 0.0f, 0.0f};
+        for (uint32_t c = sp.y + 1 + lane; c <= sp.z; c += 32u) v = vadd(v, o.head_part[c]);
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1)
+            v = vadd(v, Agg3{__shfl_xor_sync(FULL, v.s, d), __shfl_xor_sync(FULL, v.m, d),
+                             __shfl_xor_sync(FULL, v.t, d)});
+        if (lane == 0) o.nzsum[sp.x] = vadd(o.tail_part[sp.y], v);
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nsplit; k += gridDim.x * blockDim.x) {
+        const uint4 sp = split[k];
+        if (sp.z - sp.y <= LONG_SPAN) {
             Agg3 v = o.tail_part[sp.y];
             for (uint32_t c = sp.y + 1; c <= sp.z; ++c) v = vadd(v, o.head_part[c]);
             o.nzsum[sp.x] = v;
-        }
-        uint32_t m = __ballot_sync(FULL, lng);
-        while (m) {
-            const int src = __ffs(m) - 1;
-            m &= m - 1;
-            const uint32_t row = __shfl_sync(FULL, sp.x, src);
-            const uint32_t cs = __shfl_sync(FULL, sp.y, src);
-            const uint32_t ce = __shfl_sync(FULL, sp.z, src);
-            Agg3 v = Agg3{0.0f, 0.0f, 0.0f};
-            for (uint32_t c = cs + 1 + lane; c <= ce; c += 32u) v = vadd(v, o.head_part[c]);
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1)
-                v = vadd(v, Agg3{__shfl_xor_sync(FULL, v.s, d), __shfl_xor_sync(FULL, v.m, d),
-                                 __shfl_xor_sync(FULL, v.t, d)});
-            if (lane == 0) o.nzsum[row] = vadd(o.tail_part[cs], v);
         }
     }
 }
@@ -203,8 +199,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return bf16_bits(lo) | (bf16_bits(hi) << 16);
 }
 
-/* normalised BF16 inputs of the vertices with in-edges, 16 bytes per row: word t
- * holds features 2t and 2t+1, exactly the layer-1 A-operand word of lane t */
+/* normalised BF16 inputs of the vertices with in-edges, 16 bytes per row:
+ * word t holds features 2t and 2t+1, i.e. the row exactly as the first K core
+ * matrix of the inference's A tile holds it */
 __global__ void k_warm_xfeat(const uint32_t *__restrict__ nz_rows, const uint32_t *__restrict__ od_nz, uint32_t nnz,
                              const uint32_t *__restrict__ indeg, const Agg3 *__restrict__ agg, uint32_t vbits,
                              const float *__restrict__ norm, uint4 *__restrict__ xpk) {
@@ -222,149 +219,225 @@ __global__ void k_warm_xfeat(const uint32_t *__restrict__ nz_rows, const uint32_
     }
 }
 
-/* D += A (16x16, row) * B (16x8, col), BF16 operands, FP32 accumulation */
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1) {
+/* ---- inference on the 5th-generation tensor cores (tcgen05) -------------
+ * One CTA of 128 threads takes tiles of 128 vertices with in-edges (one row per
+ * thread). Both layers are tcgen05.mma of kind f16 (BF16 operands, FP32
+ * accumulation) with M = 128, N = 64, issued by one thread: layer 1 is one MMA
+ * (K = 16: the 8 features and 8 zero columns), layer 2 four (K = 64). The
+ * operands sit in shared memory as K-major "core matrices" without swizzle (8
+ * rows x 16 bytes each, contiguous); the accumulator is a 128-lane x 64-column
+ * FP32 tile in tensor memory, read back with tcgen05.ld (warp w reads lanes
+ * 32w..32w+31, so every thread receives its own row). Each layer's completion
+ * is signalled on an mbarrier by tcgen05.commit; every wait is bounded. */
+constexpr int TC_ROWS = 128;   /* M of the MMA: rows of a tile, threads of a CTA */
+constexpr int TC_COLS = 64;    /* tensor-memory columns held by a CTA (the N of both layers) */
+constexpr uint32_t TC_CTAS_PER_SM = 4;
+/* instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A
+ * (bits 7-9 = 1) and B (bits 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3
+ * in bits 17-22, M >> 4 in bits 24-28 */
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
+                              ((uint32_t)(TC_ROWS >> 4) << 24);
+
+/* shared-memory matrix descriptor, no swizzle: start address, the byte offset
+ * between the two K-adjacent core matrices (lbo) and between 8-row groups (sbo),
+ * all in 16-byte units; descriptor version 1 (bit 46) */
+__device__ __forceinline__ uint64_t tc_desc(const void *smem, uint32_t lbo, uint32_t sbo) {
+    const uint32_t a = smem_u32(smem);
+    return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate)
+        : "memory");
+}
+/* arrives once on bar when every MMA this thread issued before has completed */
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+/* generic-proxy writes to shared memory become visible to the tensor cores */
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+/* 16 consecutive FP32 columns of this thread's tensor-memory lane */
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+/* byte offset of element (row, k) in a K-major core-matrix tile whose rows have
+ * kcores cores of 8 BF16 */
+__host__ __device__ __forceinline__ uint32_t tc_off(uint32_t row, uint32_t k, uint32_t kcores) {
+    return ((row >> 3) * kcores + (k >> 3)) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
 }
 
 struct InferArgs {
     const uint32_t *nz_rows, *od_nz;
-    const uint32_t *xpk;           /* per nz row: 4 words of packed BF16 inputs */
+    const uint4 *xpk;              /* per nz row: 8 normalised BF16 features */
     uint32_t nnz;
-    const uint32_t *frag1, *frag2; /* B operand fragments, lane-major */
-    const float *wb;               /* rounded weights (biases FP32) */
-    const float *norm;             /* mean[8], inv_std[8] */
+    const float *wb;               /* BF16-rounded weights, FP32 biases */
     float teleport;
     float *out;
     double2 *part_mass;            /* per block: sum of the predicted ranks, of those without out-edges */
+    int *err;                      /* set when a wait for the tensor cores ran out */
 };
 
-constexpr int INFER_THREADS = 256;
+__global__ void __launch_bounds__(TC_ROWS) k_warm_infer(InferArgs a) {
+    __shared__ __align__(1024) uint8_t s_a1[TC_ROWS * 16 * 2]; /* X: 128 x 16 BF16 */
+    __shared__ __align__(1024) uint8_t s_b1[NH * 16 * 2];      /* W1: 64 x 16 BF16 */
+    __shared__ __align__(1024) uint8_t s_a2[TC_ROWS * NH * 2]; /* H1: 128 x 64 BF16 */
+    __shared__ __align__(1024) uint8_t s_b2[NH * NH * 2];      /* W2: 64 x 64 BF16 */
+    __shared__ float s_bias1[NH], s_bias2[NH], s_w3[NH];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    __shared__ double s_m[TC_ROWS / 32][2];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
 
-/* one warp = 16 vertices with in-edges per step; lane (g = lane/4, t = lane%4)
- * holds rows g and g+8 of every accumulator tile (the m16n8 C layout), which is
- * also the A layout of the next layer once two adjacent n-tiles are packed to
- * BF16 pairs. Lane t computes features 2t and 2t+1 of its two rows: exactly its
- * part of the layer-1 A operand. */
-__global__ void __launch_bounds__(INFER_THREADS) k_warm_infer(InferArgs a) {
-    const uint32_t FULL = 0xFFFFFFFFu;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t g = lane >> 2, t = lane & 3u;
-    uint32_t B1[8], B2[4][8][2];
-    float bias1[8][2], bias2[8][2], w3[8][2];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-        B1[nt] = a.frag1[nt * 32 + lane];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c = nt * 8 + 2 * (int)t + q;
-            bias1[nt][q] = a.wb[OB1 + c];
-            bias2[nt][q] = a.wb[OB2 + c];
-            w3[nt][q] = a.wb[OW3 + c];
-        }
+    /* weights into the K-major core-matrix layout (layer 1 padded to K = 16) */
+    for (uint32_t e = tid; e < (uint32_t)NH * 16; e += TC_ROWS) {
+        const uint32_t n = e >> 4, k = e & 15u;
+        const float w = k < (uint32_t)NIN ? a.wb[OW1 + n * NIN + k] : 0.0f;
+        *(uint16_t *)(s_b1 + tc_off(n, k, 2)) = (uint16_t)bf16_bits(w);
     }
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const uint2 f = ((const uint2 *)a.frag2)[(ks * 8 + nt) * 32 + lane];
-            B2[ks][nt][0] = f.x;
-            B2[ks][nt][1] = f.y;
-        }
+    for (uint32_t e = tid; e < (uint32_t)NH * NH; e += TC_ROWS) {
+        const uint32_t n = e >> 6, k = e & 63u;
+        *(uint16_t *)(s_b2 + tc_off(n, k, NH / 8)) = (uint16_t)bf16_bits(a.wb[OW2 + n * NH + k]);
+    }
+    for (uint32_t j = tid; j < (uint32_t)NH; j += TC_ROWS) {
+        s_bias1[j] = a.wb[OB1 + j];
+        s_bias2[j] = a.wb[OB2 + j];
+        s_w3[j] = a.wb[OW3 + j];
+    }
+    /* the zero K-columns 8..15 of every X row */
+    *(uint4 *)(s_a1 + tc_off(tid, 8, 2)) = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) {
+        s_fail = 0;
+        mbar_init(&s_bar, 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"((uint32_t)TC_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t taddr = tmem + ((warp * 32u) << 16); /* this warp's 32 lanes */
     const float b3 = a.wb[OB3];
-    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t ntiles = (a.nnz + 15u) >> 4;
+    const uint64_t d_a1 = tc_desc(s_a1, 128, 256), d_b1 = tc_desc(s_b1, 128, 256);
+
     double msum = 0.0, mdang = 0.0;
-    /* inputs of the next tile are loaded while the current one computes */
-    uint32_t nx[2] = {0u, 0u}, nv_[2] = {0u, 0u}, nd[2] = {1u, 1u};
-    auto load_tile = [&](uint32_t tile) {
+    uint32_t phase = 0;
+    const uint32_t ntiles = (a.nnz + TC_ROWS - 1) / TC_ROWS;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t i = tile * TC_ROWS + tid;
+        const bool valid = i < a.nnz;
+        const uint4 x = valid ? a.xpk[i] : make_uint4(0u, 0u, 0u, 0u);
+        const uint32_t v = valid ? a.nz_rows[i] : 0u, od = valid ? a.od_nz[i] : 1u;
+        *(uint4 *)(s_a1 + tc_off(tid, 0, 2)) = x;
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (s_fail) break; /* a wait of the previous tile ran out (uniform: read after the barrier) */
+        tc_fence_after();
+        if (tid == 0) {
+            tc_mma(tmem, d_a1, d_b1, 0u);
+            tc_commit(&s_bar);
+        }
+        bool ok = false;
+        for (long long spin = 0; !ok && spin < MBAR_SPIN; ++spin) ok = mbar_try_wait(&s_bar, phase);
+        phase ^= 1u;
+        if (!ok) s_fail = 1;
+        tc_fence_after();
+        float acc[NH];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const uint32_t i = (tile << 4) + g + 8 * q;
-            nx[q] = 0u;
-            nv_[q] = 0u;
-            nd[q] = 1u;
-            if (tile < ntiles && i < a.nnz) {
-                nx[q] = a.xpk[(size_t)i * 4 + t];
-                nv_[q] = a.nz_rows[i];
-                nd[q] = a.od_nz[i];
+        for (int q = 0; q < NH / 16; ++q) tc_ld16(taddr + 16u * q, acc + 16 * q);
+        tc_wait_ld();
+        /* layer-1 epilogue: bias, ReLU, BF16, into this thread's row of H1 */
+#pragma unroll
+        for (int kc = 0; kc < NH / 8; ++kc) {
+            uint32_t w[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int j = kc * 8 + 2 * t;
+                const float h0 = bf16r(fmaxf(acc[j] + s_bias1[j], 0.0f));
+                const float h1 = bf16r(fmaxf(acc[j + 1] + s_bias1[j + 1], 0.0f));
+                w[t] = bf16_bits(h0) | (bf16_bits(h1) << 16);
             }
+            *(uint4 *)(s_a2 + tc_off(tid, kc * 8, NH / 8)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-    };
-    load_tile(gwarp);
-    for (uint32_t tile = gwarp; tile < ntiles; tile += nwarps) {
-        const uint32_t i0 = tile << 4;
-        const uint32_t xw[2] = {nx[0], nx[1]}, vq[2] = {nv_[0], nv_[1]}, dq[2] = {nd[0], nd[1]};
-        load_tile(tile + nwarps);
-        /* layer 1 -> A operand of layer 2 */
-        uint32_t A2[4][4];
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (s_fail) break;
+        tc_fence_after();
+        if (tid == 0) {
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_bf16(c, xw[0], xw[1], 0u, 0u, B1[nt], 0u);
-            const float h0 = bf16r(fmaxf(c[0] + bias1[nt][0], 0.0f));
-            const float h1 = bf16r(fmaxf(c[1] + bias1[nt][1], 0.0f));
-            const float h2 = bf16r(fmaxf(c[2] + bias1[nt][0], 0.0f));
-            const float h3 = bf16r(fmaxf(c[3] + bias1[nt][1], 0.0f));
-            A2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(h0, h1);
-            A2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(h2, h3);
+            for (int st = 0; st < NH / 16; ++st)
+                tc_mma(tmem, tc_desc(s_a2 + 256 * st, 128, 1024), tc_desc(s_b2 + 256 * st, 128, 1024), st > 0);
+            tc_commit(&s_bar);
         }
-        /* layer 2, then layer 3 on the FP32 pipes */
-        float yg = 0.0f, yg8 = 0.0f;
+        ok = false;
+        for (long long spin = 0; !ok && spin < MBAR_SPIN; ++spin) ok = mbar_try_wait(&s_bar, phase);
+        phase ^= 1u;
+        if (!ok) s_fail = 1;
+        tc_fence_after();
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int q = 0; q < NH / 16; ++q) tc_ld16(taddr + 16u * q, acc + 16 * q);
+        tc_wait_ld();
+        /* layer 2's bias and ReLU, layer 3 on the FP32 pipes */
+        float y = 0.0f;
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks)
-                mma_bf16(d, A2[ks][0], A2[ks][1], A2[ks][2], A2[ks][3], B2[ks][nt][0], B2[ks][nt][1]);
-            yg = fmaf(fmaxf(d[0] + bias2[nt][0], 0.0f), w3[nt][0], yg);
-            yg = fmaf(fmaxf(d[1] + bias2[nt][1], 0.0f), w3[nt][1], yg);
-            yg8 = fmaf(fmaxf(d[2] + bias2[nt][0], 0.0f), w3[nt][0], yg8);
-            yg8 = fmaf(fmaxf(d[3] + bias2[nt][1], 0.0f), w3[nt][1], yg8);
+        for (int j = 0; j < NH; ++j) y = fmaf(fmaxf(acc[j] + s_bias2[j], 0.0f), s_w3[j], y);
+        if (valid) {
+            /* y is clamped so exp stays finite */
+            const float r = a.teleport * expf(fminf(fmaxf(y + b3, -30.0f), 30.0f));
+            a.out[v] = r;
+            msum += (double)r;
+            if (od == 0) mdang += (double)r;
         }
-        yg += __shfl_xor_sync(FULL, yg, 1);
-        yg += __shfl_xor_sync(FULL, yg, 2);
-        yg8 += __shfl_xor_sync(FULL, yg8, 1);
-        yg8 += __shfl_xor_sync(FULL, yg8, 2);
-        if (t == 0) {
-            const float y2[2] = {yg, yg8};
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                if (i0 + g + 8 * q >= a.nnz) continue;
-                /* y is clamped so exp stays finite */
-                const float r = a.teleport * expf(fminf(fmaxf(y2[q] + b3, -30.0f), 30.0f));
-                a.out[vq[q]] = r;
-                msum += (double)r;
-                if (dq[q] == 0) mdang += (double)r;
-            }
-        }
+        tc_fence_before(); /* this tile's tensor-memory reads precede the next tile's MMA */
     }
+    __syncthreads();
+    if (tid == 0 && s_fail) atomicExch(a.err, 1);
     /* block partials of the mass terms, reduced in a fixed order */
-    __shared__ double s_m[INFER_THREADS / 32][2];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        msum += __shfl_xor_sync(FULL, msum, o);
-        mdang += __shfl_xor_sync(FULL, mdang, o);
+        msum += __shfl_xor_sync(0xFFFFFFFFu, msum, o);
+        mdang += __shfl_xor_sync(0xFFFFFFFFu, mdang, o);
     }
     if (lane == 0) {
         s_m[warp][0] = msum;
         s_m[warp][1] = mdang;
     }
+    tc_fence_before();
     __syncthreads();
-    if (threadIdx.x == 0) {
+    tc_fence_after();
+    if (tid == 0) {
         double2 m = make_double2(0.0, 0.0);
-        for (int w = 0; w < INFER_THREADS / 32; ++w) {
+        for (int w = 0; w < TC_ROWS / 32; ++w) {
             m.x += s_m[w][0];
             m.y += s_m[w][1];
         }
         a.part_mass[blockIdx.x] = m;
     }
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TC_COLS)
+                     : "memory");
 }
 
 /* vertices without in-edges: exactly teleport; per block, how many also lack out-edges */
@@ -425,21 +498,6 @@ __global__ void k_warm_scale(const uint32_t *__restrict__ nz_rows, uint32_t nnz,
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) {
         const uint32_t v = nz_rows[i];
         out[v] = (float)((double)out[v] * al);
-    }
-}
-
-/* B operand fragments of layers 1 and 2 from the rounded weights */
-__global__ void k_mlp_pack(const float *__restrict__ wb, uint32_t *__restrict__ frag1, uint32_t *__restrict__ frag2) {
-    for (uint32_t i = threadIdx.x; i < (uint32_t)NFRAG1; i += blockDim.x) {
-        const uint32_t nt = i >> 5, lane = i & 31u, g = lane >> 2, t = lane & 3u;
-        const float *w = wb + OW1 + (nt * 8 + g) * NIN;
-        frag1[i] = pack_bf16(w[2 * t], w[2 * t + 1]);
-    }
-    for (uint32_t i = threadIdx.x; i < (uint32_t)(NFRAG2 / 2); i += blockDim.x) {
-        const uint32_t lane = i & 31u, nt = (i >> 5) & 7u, ks = i >> 8, g = lane >> 2, t = lane & 3u;
-        const float *w = wb + OW2 + (nt * 8 + g) * NH + ks * 16;
-        frag2[2 * i] = pack_bf16(w[2 * t], w[2 * t + 1]);
-        frag2[2 * i + 1] = pack_bf16(w[8 + 2 * t], w[8 + 2 * t + 1]);
     }
 }
 
@@ -636,7 +694,6 @@ __global__ void k_mlp_round(const float *__restrict__ w, float *__restrict__ wb)
 
 struct gcg_mlp {
     gcg::dbuf<float> w, wb, m, v, norm; /* master weights, rounded copy, Adam moments, normalisation */
-    gcg::dbuf<uint32_t> frag;           /* MMA B fragments: layer 1 then layer 2 */
     uint64_t step = 0;                  /* Adam steps taken */
 };
 
@@ -651,10 +708,9 @@ uint64_t splitmix(uint64_t &x) {
 }
 double uniform01(uint64_t &x) { return ((splitmix(x) >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
 
-/* rounded copy and MMA fragments from the master weights (stream-ordered) */
+/* rounded copy of the master weights (stream-ordered) */
 int mlp_prepare(gcg_mlp *m, cudaStream_t s) {
     k_mlp_round<<<(NP + 255) / 256, 256, 0, s>>>(m->w.get(), m->wb.get());
-    k_mlp_pack<<<1, 256, 0, s>>>(m->wb.get(), m->frag.get(), m->frag.get() + NFRAG1);
     GCG_LAUNCH_CHECK();
     return GCG_OK;
 }
@@ -717,7 +773,7 @@ int warm_aggregates(gcg_graph *g, tbuf<Agg3> &agg, cudaStream_t s) {
         if (pl.nsplit) {
             const unsigned fb = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>(((uint64_t)pl.nsplit + 255) / 256, sms * 8ull));
-            k_warm_agg_fix<<<fb, 256, 0, s>>>(pl.split.get(), pl.nsplit, o);
+            k_warm_agg_fix<<<fb, 256, 0, s>>>(pl.split.get(), pl.nsplit, pl.long_split.get(), pl.nlong, o);
         }
     }
     GCG_LAUNCH_CHECK();
@@ -747,7 +803,7 @@ int gcg_mlp_create(uint64_t seed, gcg_mlp **out) {
     for (int i = 0; i < NIN; ++i) norm[NIN + i] = 1.0f;
     int rc;
     if ((rc = m->w.alloc(NP)) || (rc = m->wb.alloc(NP)) || (rc = m->m.alloc(NP)) || (rc = m->v.alloc(NP)) ||
-        (rc = m->norm.alloc(2 * NIN)) || (rc = m->frag.alloc(NFRAG1 + NFRAG2))) {
+        (rc = m->norm.alloc(2 * NIN))) {
         delete m;
         return rc;
     }
@@ -1033,11 +1089,12 @@ int gcg_warm_start_rank(gcg_graph *g, const gcg_mlp *m, double teleport, double 
         tbuf<uint32_t> pzd;
         tbuf<double> alpha;
         tbuf<uint4> xpk;
+        tbuf<int> ierr;
         float *dst = init_rank;
         const bool dev = is_device_ptr(init_rank);
-        const uint64_t tiles = ((uint64_t)pl.nnz + 15) / 16;
-        const unsigned ib = (unsigned)std::max<uint64_t>(
-            1, std::min<uint64_t>((tiles + INFER_THREADS / 32 - 1) / (INFER_THREADS / 32), sms * 2ull));
+        const uint64_t tiles = ((uint64_t)pl.nnz + TC_ROWS - 1) / TC_ROWS;
+        /* at most TC_CTAS_PER_SM CTAs of 64 tensor-memory columns per SM: well inside its 512 */
+        const unsigned ib = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, sms * (uint64_t)TC_CTAS_PER_SM));
         const unsigned zb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)pl.nzero + 255) / 256, sms * 4ull));
         rc = warm_aggregates(g, agg, s);
         if (rc == GCG_OK && !dev) {
@@ -1045,23 +1102,25 @@ int gcg_warm_start_rank(gcg_graph *g, const gcg_mlp *m, double teleport, double 
             dst = stage.get();
         }
         if (rc == GCG_OK && (rc = pmass.alloc(ib, s)) == GCG_OK && (rc = pzd.alloc(zb, s)) == GCG_OK &&
-            (rc = alpha.alloc(1, s)) == GCG_OK && (rc = xpk.alloc(std::max<uint32_t>(pl.nnz, 1), s)) == GCG_OK) {
+            (rc = alpha.alloc(1, s)) == GCG_OK && (rc = xpk.alloc(std::max<uint32_t>(pl.nnz, 1), s)) == GCG_OK &&
+            (rc = ierr.alloc(1, s)) == GCG_OK && (rc = (cudaMemsetAsync(ierr.get(), 0, sizeof(int), s) == cudaSuccess
+                                                            ? GCG_OK
+                                                            : fail(GCG_ERR_CUDA, "gcg_warm_start_rank: memset"))) == GCG_OK) {
             const unsigned xb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)pl.nnz + 255) / 256, sms * 8ull));
             k_warm_xfeat<<<xb, 256, 0, s>>>(pl.nz_rows.get(), pl.od_nz.get(), pl.nnz, g->indeg.get(), agg.get(),
                                             g->vbits, m->norm.get(), xpk.get());
             InferArgs a;
             a.nz_rows = pl.nz_rows.get();
             a.od_nz = pl.od_nz.get();
-            a.xpk = (const uint32_t *)xpk.get();
+            a.xpk = xpk.get();
             a.nnz = pl.nnz;
-            a.frag1 = m->frag.get();
-            a.frag2 = m->frag.get() + NFRAG1;
             a.wb = m->wb.get();
-            a.norm = m->norm.get();
             a.teleport = (float)teleport;
             a.out = dst;
             a.part_mass = pmass.get();
-            k_warm_infer<<<ib, INFER_THREADS, 0, s>>>(a);
+            a.err = ierr.get();
+            if (pl.nnz) k_warm_infer<<<ib, TC_ROWS, 0, s>>>(a);
+            else cudaMemsetAsync(pmass.get(), 0, sizeof(double2), s);
             k_warm_zero<<<zb, 256, 0, s>>>(pl.zero_rows.get(), pl.nzero, g->outdeg.get(), (float)teleport, dst,
                                            pzd.get());
             k_warm_alpha<<<1, 32, 0, s>>>(pmass.get(), ib, pzd.get(), zb, nv, pl.nzero, teleport, damping,
@@ -1073,6 +1132,11 @@ int gcg_warm_start_rank(gcg_graph *g, const gcg_mlp *m, double teleport, double 
         }
         cudaEventRecord(ev1, s);
         if (rc == GCG_OK && !dev) rc = copy_out(init_rank, dst, (size_t)nv * 4, s);
+        int herr = 0;
+        if (rc == GCG_OK && (cudaMemcpyAsync(&herr, ierr.get(), sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                             cudaStreamSynchronize(s) != cudaSuccess))
+            rc = fail(GCG_ERR_CUDA, "gcg_warm_start_rank: readback");
+        if (rc == GCG_OK && herr) rc = fail(GCG_ERR_TIMEOUT, "gcg_warm_start_rank: a tensor-core wait ran out");
     }
     cudaStreamSynchronize(s);
     float ms = 0.0f;
