@@ -136,7 +136,8 @@ __global__ void k_cc_rounds(Nbrs n, uint32_t nv, uint32_t *parent) {
 }
 
 /* the most frequent root among 1024 sampled vertices (ties: the smaller id);
- * one block of 1024 threads: bitonic sort in shared memory, then run lengths */
+ * one block of 1024 threads: bitonic sort in shared memory, then each run's
+ * length from two binary searches by its first thread */
 __global__ void __launch_bounds__(1024) k_cc_sample(const uint32_t *parent, uint32_t nv, uint32_t *giant) {
     __shared__ uint32_t s[1024];
     __shared__ unsigned long long s_best;
@@ -161,11 +162,16 @@ __global__ void __launch_bounds__(1024) k_cc_sample(const uint32_t *parent, uint
             }
             __syncthreads();
         }
-    /* run starting at t: key = (1024 - length) << 32 | value, smallest wins */
+    /* run starting at t: key = (1024 - length) << 32 | value, smallest wins; the
+     * run ends at the first entry above s[t] */
     if (t == 0 || s[t] != s[t - 1]) {
-        uint32_t e = t + 1;
-        while (e < 1024 && s[e] == s[t]) ++e;
-        atomicMin(&s_best, ((unsigned long long)(1024u - (e - t)) << 32) | s[t]);
+        const uint32_t x = s[t];
+        uint32_t lo = t + 1, hi = 1024;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s[mid] > x) hi = mid; else lo = mid + 1;
+        }
+        atomicMin(&s_best, ((unsigned long long)(1024u - (lo - t)) << 32) | x);
     }
     __syncthreads();
     if (t == 0) *giant = (uint32_t)(s_best & 0xFFFFFFFFull);

@@ -13,6 +13,13 @@ graphs, vertex counts log-uniform in [LO, HI] (seeded), alternating
 Erdos-Renyi (mean degree 8) and R-MAT (edge factor 8), solved to 1e-8 in one
 launch for each --hub value, against one gcg_pagerank solve per graph.
 
+With --ppr K it reports batched personalised PageRank on the R-MAT graph of
+each --scale (seed + 6): K seeded sources to 1e-8 in one gcg_ppr_batched call
+(best of two), against E(4 + 4k) + 12Vk bytes per sweep over the k sources still
+iterating. With --cc it reports connected components on the symmetrised R-MAT
+graph of each --scale (best of three calls) against one streaming pass over the
+graph (8E + 12V bytes).
+
 (run with graphchi-cpp_b200 on PYTHONPATH)."""
 from __future__ import annotations
 
@@ -74,6 +81,51 @@ def batch_report(lo, hi, hubs, peak):
         g.free()
 
 
+def ppr_report(scale, ef, seed, k, peak):
+    import numpy as np
+    import torch
+    import gcgpu
+    m = ef << scale
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    gcgpu.generate_rmat(scale, m, 0.57, 0.19, 0.19, seed=seed + 6, src=s, dst=d)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, out_csr=False) as g:
+        del s, d
+        n, E = g.num_vertices, g.num_edges
+        src = np.random.default_rng(3).integers(0, n, k).astype(np.uint32)
+        mat = torch.empty((n, k), dtype=torch.float32, device="cuda")
+        runs = []
+        for _ in range(2):
+            wl = np.zeros(2 * 1000, np.uint64)
+            st = g.ppr_batched(src, max_sweeps=1000, tol=1e-8, teleport=0.15, out=mat, work_log=wl)[1]
+            runs.append((st.device_ms, st.sweeps, wl))
+        ms, sweeps, wl = min(runs, key=lambda r: r[0])
+        upd, gat = int(wl[2 * sweeps - 2]), int(wl[2 * sweeps - 1])
+        byt = 4.0 * E * sweeps + 4.0 * gat + 12.0 * upd
+        print(json.dumps({"ppr": {"scale": scale, "vertices": n, "edges": E, "sources": k, "sweeps": sweeps,
+                                  "source_sweeps": gat // max(1, E), "ms": round(ms, 2),
+                                  "algorithmic_bytes": byt, "frac_of_hbm": round(byt / ms / 1e6 / peak, 3)}}),
+              flush=True)
+
+
+def cc_report(scale, ef, seed, peak):
+    import torch
+    import gcgpu
+    m = ef << scale
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    gcgpu.generate_rmat(scale, m, 0.57, 0.19, 0.19, seed=seed, src=s, dst=d)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, symmetrise=True, out_csr=False) as g:
+        del s, d
+        lab = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+        g.connected_components(out=lab)
+        ms = min(g.connected_components(out=lab)[1].device_ms for _ in range(3))
+        byt = 8.0 * g.num_edges + 12.0 * g.num_vertices
+        print(json.dumps({"cc": {"scale": scale, "vertices": g.num_vertices, "directed_edges": g.num_edges,
+                                 "ms": round(ms, 3), "one_pass_bytes": byt,
+                                 "frac_of_one_pass_at_hbm": round(byt / ms / 1e6 / peak, 3)}}), flush=True)
+
+
 def main():
     import torch
     import gcgpu
@@ -84,10 +136,19 @@ def main():
     ap.add_argument("--hub", type=int, nargs="+", default=[41724])
     ap.add_argument("--tiers", type=int, nargs="+", default=[1])
     ap.add_argument("--batch", type=float, nargs=2, default=None, metavar=("LO", "HI"))
+    ap.add_argument("--ppr", type=int, default=0, metavar="K")
+    ap.add_argument("--cc", action="store_true")
     args = ap.parse_args()
     peak = peak_gbs()
     if args.batch:
         batch_report(args.batch[0], args.batch[1], args.hub, peak)
+        return
+    if args.ppr or args.cc:
+        for scale in args.scale:
+            if args.ppr:
+                ppr_report(scale, args.ef, args.seed, args.ppr, peak)
+            if args.cc:
+                cc_report(scale, args.ef, args.seed, peak)
         return
     for scale in args.scale:
         m = args.ef << scale
