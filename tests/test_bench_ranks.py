@@ -81,6 +81,11 @@ def test_reference_arm_under_torchrun_runs_on_rank_zero_only():
     # the same workload as the GPU arm (scale 12 here), one step = one timed iteration
     assert rec["config"]["workload"] == "pagerank_rmat12_ef16_to_1e-08"
     assert len(rec["cpu_baseline"]["iteration_s"]) == 2 and rec["ms_per_step"] > 0
+    # the value is the engine's in-memory mode (one shard, large budget); the default
+    # configuration's run is reported beside it
+    assert "in-memory mode" in rec["cpu_baseline"]["sample"]
+    db = rec["cpu_baseline"]["default_budget"]
+    assert db["value"] > 0 and len(db["iteration_s"]) == 2, db
 
 
 def test_reference_arm_loads_no_library_code():
