@@ -163,7 +163,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
-constexpr uint32_t GS_DEPTH = 3; /* block class: 256-value batches in flight (2: 11 % slower at scale 24, 4: 1 %, 6: 18 %) */
+/* block class: steps of GS_STEP values, GS_DEPTH of them in flight (per sweep
+ * at R-MAT scale 24, 10 sweeps: 1024 x 2 88.6 ms, 1024 x 3 90.1, 1024 x 4 90.7,
+ * 2048 x 2 88.0, 2048 x 3 92.7, 512 x 2 116.1, 512 x 3 119.7, 256 x 3 108.2) */
+constexpr uint32_t GS_STEP = 1024, GS_DEPTH = 2;
 
 /* value of in-edge (u -> v): this sweep's for u < v (an earlier level, written
  * by an earlier launch), the previous sweep's otherwise */
@@ -195,9 +198,9 @@ __device__ __forceinline__ void gs_apply(uint32_t v, float sum, const uint32_t *
 }
 
 /* One level of a sweep: the level's vertices are independent. Blocks
- * [0, nb) take the block-class vertices (one each: every thread copies one
- * in-edge value of a 256-edge batch into shared memory, GS_DEPTH batches in
- * flight, thread 0 adds the batch in order); the next blocks take the
+ * [0, nb) take the block-class vertices (one each: the threads copy the
+ * in-edge values of a GS_STEP-edge step into shared memory, GS_DEPTH steps in
+ * flight, thread 0 adds the step in order); the next blocks take the
  * warp-class vertices (one per warp: 32 values per batch, lane 0 adds them in
  * order from shuffles, the next batch already loading); the rest take the
  * thread-class vertices (eight loads in flight, then eight adds in order).
@@ -213,35 +216,45 @@ __global__ void __launch_bounds__(256) k_gs_level(const uint32_t *__restrict__ o
     const uint32_t nb = be - bb, nwb = (bb - wb + 7) / 8;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     if (blockIdx.x < nb) { /* block class */
-        /* GS_DEPTH batches of 256 in-edge values in flight: every thread copies
-         * its value of a batch into shared memory with cp.async (the source
-         * column is read one batch ahead), so the loads of later batches overlap
-         * thread 0's in-order adds of the current one */
-        __shared__ __align__(16) float s_val[GS_DEPTH][256];
+        /* GS_DEPTH steps of GS_STEP in-edge values in flight: every thread copies
+         * GS_STEP / 256 values of a step into shared memory with cp.async (the
+         * source columns read one step ahead), so the loads of the next step
+         * overlap thread 0's in-order adds of the current one */
+        constexpr uint32_t GQ = GS_STEP / 256;
+        __shared__ __align__(16) float s_val[GS_DEPTH][GS_STEP];
         const uint32_t v = order[bb + blockIdx.x];
         const uint32_t jb = rowptr[v], je = rowptr[v + 1];
-        const uint32_t nbatch = (je - jb + 255) / 256;
+        const uint32_t nstep = (je - jb + GS_STEP - 1) / GS_STEP;
         float sum = 0.0f;
-        /* this thread's copy for batch b (source column u), then one commit group
-         * per batch, empty past the row's end */
-        auto issue = [&](uint32_t b, uint32_t u) {
-            if (b < nbatch && jb + b * 256 + tid < je)
-                cp_async4(&s_val[b % GS_DEPTH][tid], (u < v ? pr_new : pr_old) + u);
+        /* this thread's copies for step b (source columns u), then one commit
+         * group per step, empty past the row's end */
+        auto issue = [&](uint32_t b, const uint32_t (&u)[GQ]) {
+#pragma unroll
+            for (uint32_t q = 0; q < GQ; ++q)
+                if (b < nstep && jb + b * GS_STEP + q * 256 + tid < je)
+                    cp_async4(&s_val[b % GS_DEPTH][q * 256 + tid], (u[q] < v ? pr_new : pr_old) + u[q]);
             cp_async_commit();
         };
-        auto column = [&](uint32_t b) -> uint32_t {
-            const uint32_t j = jb + b * 256 + tid;
-            return b < nbatch && j < je ? __ldg(col + j) : 0u;
+        auto columns = [&](uint32_t b, uint32_t (&u)[GQ]) {
+#pragma unroll
+            for (uint32_t q = 0; q < GQ; ++q) {
+                const uint32_t j = jb + b * GS_STEP + q * 256 + tid;
+                u[q] = b < nstep && j < je ? __ldg(col + j) : 0u;
+            }
         };
-        for (uint32_t b = 0; b + 1 < GS_DEPTH; ++b) issue(b, column(b));
-        uint32_t cnext = column(GS_DEPTH - 1);
-        for (uint32_t b = 0; b < nbatch; ++b) {
-            cp_async_wait<GS_DEPTH - 2>(); /* this thread's value of batch b has landed */
-            __syncthreads();               /* everyone's; thread 0 is done with batch b - 1 */
-            issue(b + GS_DEPTH - 1, cnext); /* into batch b - 1's buffer */
-            cnext = column(b + GS_DEPTH);
+        uint32_t cn[GQ];
+        for (uint32_t b = 0; b + 1 < GS_DEPTH; ++b) {
+            columns(b, cn);
+            issue(b, cn);
+        }
+        columns(GS_DEPTH - 1, cn);
+        for (uint32_t b = 0; b < nstep; ++b) {
+            cp_async_wait<GS_DEPTH - 2>(); /* this thread's values of step b have landed */
+            __syncthreads();               /* everyone's; thread 0 is done with step b - 1 */
+            issue(b + GS_DEPTH - 1, cn);   /* into step b - 1's buffer */
+            columns(b + GS_DEPTH, cn);
             if (tid == 0) { /* in order, four values per shared-memory load */
-                const uint32_t n = min(256u, je - (jb + b * 256));
+                const uint32_t n = min(GS_STEP, je - (jb + b * GS_STEP));
                 const float *sv = s_val[b % GS_DEPTH];
                 uint32_t k = 0;
                 for (; k + 4 <= n; k += 4) {
