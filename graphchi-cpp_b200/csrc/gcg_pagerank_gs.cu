@@ -106,7 +106,9 @@ __global__ void __launch_bounds__(256) k_gs_round(uint32_t r, const uint32_t *__
  * GS_THREAD_MAX in-edges, a warp one of at most GS_WARP_MAX, a block a longer
  * one. Every class adds the in-edges one after another in ascending source
  * order (a float sum is not associative); the cooperating threads only load. */
-constexpr uint32_t GS_THREAD_MAX = 32, GS_WARP_MAX = 1024;
+/* R-MAT scale 22, per sweep: warp limit 1024: 31.8 ms, 512: 31.1, 256: 29.0, 128: 29.1
+ * (scale 24: 88.6 ms for all four) */
+constexpr uint32_t GS_THREAD_MAX = 32, GS_WARP_MAX = 256;
 constexpr int GS_CLASSES = 4; /* segments per level: thread, warp, block, (unused) */
 
 /* sort key: level, class, vertex id */
