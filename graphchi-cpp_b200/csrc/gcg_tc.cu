@@ -11,10 +11,11 @@
  *      deduplicate (reciprocal edges collapse, like the reference's lastvid
  *      checks, trianglecounting.cpp:182,309) -> CSR of higher-ranked neighbours,
  *      each list ascending.
- *   3. one warp per vertex a; for each b in N+(a) the lanes take the shorter of
- *      N+(a) after b and N+(b), binary-search each element in the longer, and
- *      count matches with warp ballots. A match c is a triangle (a,b,c): c's
- *      count is bumped per match, b's and a's by the ballot totals — the
+ *   3. one warp per vertex a; for each b in N+(a) the shorter of N+(a) after b
+ *      and N+(b) is searched element by element in the longer, the searches of
+ *      32 b's dealt evenly to the lanes. A match c is a triangle (a,b,c): c's
+ *      count is bumped per match, b's and a's by the match totals (counts of
+ *      the top-ranked vertices gathered in shared memory first) — the
  *      per-rank incident-triangle counts of <base>_degord.4B.vout.
  * Algorithmic traffic (whole count): 4*sum_{(a,b)}(d+(a)+d+(b)) + 4*E+ + 4*V.
  */
@@ -84,56 +85,126 @@ __global__ void __launch_bounds__(MP_THREADS) k_orient_keys(const uint32_t *__re
     }
 }
 
-__device__ __forceinline__ bool bsearch_u32(const uint32_t *a, uint32_t n, uint32_t x) {
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(a + mid) < x) lo = mid + 1; else hi = mid;
-    }
-    return lo < n && __ldg(a + lo) == x;
+/* One halving of the search for the last element <= x in the sorted,
+ * duplicate-free cl[base .. base + n), n >= 2: the range that still holds that
+ * element shrinks to ceil(n / 2) values. After ceil(log2 n) halvings n is 1 and
+ * x is present exactly when cl[base] equals it. */
+__device__ __forceinline__ uint32_t last_le_step(const uint32_t *__restrict__ cl, uint32_t base, uint32_t &n,
+                                                 uint32_t x) {
+    const uint32_t h = n >> 1;
+    if (__ldg(cl + base + h) <= x) base += h;
+    n -= h;
+    return base;
 }
 
-__global__ void k_tc_count(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ cl, uint32_t nv,
-                           uint32_t *__restrict__ cnt, unsigned long long *total) {
-    const uint32_t lane = threadIdx.x & 31;
+constexpr uint32_t TC_WARPS = 32;   /* 1024-thread blocks, two per SM */
+constexpr uint32_t TC_TOP = 16384;  /* per-block shared counters for the top-ranked vertices */
+
+/* One warp per vertex a, 32 of its higher-ranked neighbours b at a time. For each
+ * b the shorter of (N+(a) after b) and N+(b) is searched element by element in
+ * the longer; the searches of the 32 b's are laid end to end (a warp prefix sum
+ * of their lengths) and dealt to the lanes two at a time, so every lane runs two
+ * independent searches whatever the lengths. A match c is the triangle (a, b, c):
+ * c's count is bumped per match, b's by its match total, a's by the sum.
+ * Ranks grow with degree, so the highest-ranked vertex of a triangle is nearly
+ * always among the top few thousand ranks: their counts are kept in the block's
+ * shared memory (dynamic, `top` entries for ranks nv - top .. nv - 1) and added
+ * to `cnt` once at the end, which keeps the per-triangle increments off a few
+ * hot global addresses. */
+__global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ cl,
+                                                      uint32_t nv, uint32_t top, uint32_t *__restrict__ cnt,
+                                                      unsigned long long *total) {
+    extern __shared__ uint32_t s_top[];
+    __shared__ uint32_t s_pre[TC_WARPS][32], s_so[TC_WARPS][32], s_lo[TC_WARPS][32], s_nl[TC_WARPS][32],
+        s_hit[TC_WARPS][32];
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t *pre = s_pre[w], *so_ = s_so[w], *lo_ = s_lo[w], *nl_ = s_nl[w], *hit = s_hit[w];
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lo_top = nv - top;
+    for (uint32_t i = threadIdx.x; i < top; i += blockDim.x) s_top[i] = 0;
+    __syncthreads();
+    auto bump = [&](uint32_t v, uint32_t inc) {
+        if (v >= lo_top)
+            atomicAdd(s_top + (v - lo_top), inc);
+        else
+            atomicAdd(cnt + v, inc);
+    };
     unsigned long long mine = 0;
     for (uint32_t a = warp; a < nv; a += nwarps) {
-        const uint32_t ab = rp[a], ae = rp[a + 1];
+        const uint32_t ab = __ldg(rp + a), ae = __ldg(rp + a + 1);
+        if (ae - ab < 2) continue; /* a triangle needs two higher-ranked neighbours */
         uint32_t acc = 0;
-        for (uint32_t j = ab; j + 1 < ae; ++j) {
-            const uint32_t b = __ldg(cl + j);
-            const uint32_t *A = cl + j + 1;
-            const uint32_t na = ae - j - 1;
-            const uint32_t *B = cl + rp[b];
-            const uint32_t nb = rp[b + 1] - rp[b];
-            if (nb == 0) continue;
-            const uint32_t *S = na <= nb ? A : B, *L = na <= nb ? B : A;
-            const uint32_t ns = na <= nb ? na : nb, nl = na <= nb ? nb : na;
-            uint32_t cab = 0;
-            for (uint32_t base = 0; base < ns; base += 32) {
-                const uint32_t k = base + lane;
-                bool f = false;
-                uint32_t x = 0;
-                if (k < ns) {
-                    x = __ldg(S + k);
-                    f = bsearch_u32(L, nl, x);
-                    if (f) atomicAdd(cnt + x, 1u);
+        for (uint32_t j0 = ab; j0 + 1 < ae; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t ns = 0, so = 0, lo = 0, nl = 0, b = 0;
+            if (j + 1 < ae) {
+                b = __ldg(cl + j);
+                const uint32_t na = ae - j - 1, bb = __ldg(rp + b), nb = __ldg(rp + b + 1) - bb;
+                if (nb) {
+                    if (na <= nb) {
+                        ns = na, so = j + 1, lo = bb, nl = nb;
+                    } else {
+                        ns = nb, so = bb, lo = j + 1, nl = na;
+                    }
                 }
-                cab += __popc(__ballot_sync(0xFFFFFFFFu, f));
             }
-            if (cab) {
-                if (lane == 0) atomicAdd(cnt + b, cab);
-                acc += cab;
+            uint32_t inc = ns;
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += t;
             }
+            const uint32_t W = __shfl_sync(FULL, inc, 31);
+            if (W == 0) continue;
+            pre[lane] = inc, so_[lane] = so, lo_[lane] = lo, nl_[lane] = nl, hit[lane] = 0;
+            __syncwarp();
+            for (uint32_t t0 = 0; t0 < W; t0 += 64) {
+                uint32_t x[2], base[2], n[2], q[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t t = t0 + 32 * u + lane;
+                    n[u] = 0, x[u] = 0, base[u] = 0, q[u] = 0;
+                    if (t < W) {
+                        /* owner: how many of the 32 inclusive prefix sums are <= t
+                         * (t < W = pre[31], so at most 31; indexes stay below 31) */
+                        uint32_t qq = 0;
+#pragma unroll
+                        for (uint32_t st = 16; st; st >>= 1)
+                            if (pre[qq + st - 1] <= t) qq += st;
+                        const uint32_t k = t - (qq ? pre[qq - 1] : 0);
+                        x[u] = __ldg(cl + so_[qq] + k);
+                        base[u] = lo_[qq], n[u] = nl_[qq], q[u] = qq;
+                    }
+                }
+                while (n[0] > 1 || n[1] > 1) {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (n[u] > 1) base[u] = last_le_step(cl, base[u], n[u], x[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    if (n[u] == 1 && __ldg(cl + base[u]) == x[u]) {
+                        bump(x[u], 1u);
+                        atomicAdd(hit + q[u], 1u);
+                    }
+            }
+            __syncwarp();
+            const uint32_t h = hit[lane];
+            if (h) bump(b, h);
+            acc += h;
+            __syncwarp(); /* the tables are rewritten for the next 32 neighbours */
         }
-        if (acc && lane == 0) {
-            atomicAdd(cnt + a, acc);
-            mine += acc;
+        const uint32_t A = __reduce_add_sync(FULL, acc);
+        if (A && lane == 0) {
+            bump(a, A);
+            mine += A;
         }
     }
     if (lane == 0 && mine) atomicAdd(total, mine);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < top; i += blockDim.x)
+        if (s_top[i]) atomicAdd(cnt + lo_top + i, s_top[i]);
 }
 
 }  // namespace
@@ -217,8 +288,12 @@ extern "C" int gcg_triangle_count(gcg_graph *g, uint64_t *total, uint32_t *per_r
     GCG_TRY(d_total.alloc(1, s));
     GCG_CUDA(cudaMemsetAsync(cnt_ptr, 0, (size_t)nv * 4, s));
     GCG_CUDA(cudaMemsetAsync(d_total.get(), 0, 8, s));
-    unsigned cb = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)nv * 32 + 255) / 256, (uint64_t)num_sms() * 32));
-    k_tc_count<<<cb, 256, 0, s>>>(rp.get(), cl.get(), nv, cnt_ptr, d_total.get());
+    /* persistent: two 1024-thread blocks per SM, each with its own top-rank counters */
+    const uint32_t top = std::min(nv, TC_TOP);
+    GCG_CUDA(cudaFuncSetAttribute(k_tc_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TC_TOP * 4)));
+    unsigned cb = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)nv + TC_WARPS - 1) / TC_WARPS, (uint64_t)num_sms() * 2));
+    k_tc_count<<<cb, TC_WARPS * 32, (size_t)top * 4, s>>>(rp.get(), cl.get(), nv, top, cnt_ptr, d_total.get());
     GCG_LAUNCH_CHECK();
     GCG_CUDA(cudaEventRecord(ev1, s));
     unsigned long long tri = 0;

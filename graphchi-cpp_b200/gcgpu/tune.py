@@ -18,7 +18,9 @@ each --scale (seed + 6): K seeded sources to 1e-8 in one gcg_ppr_batched call
 (best of two), against E(4 + 4k) + 12Vk bytes per sweep over the k sources still
 iterating. With --cc it reports connected components on the symmetrised R-MAT
 graph of each --scale (best of three calls) against one streaming pass over the
-graph (8E + 12V bytes).
+graph (8E + 12V bytes). With --tc it reports triangle counting (degree
+ranking, orientation, count; per-rank counts into device memory) on the
+symmetrised R-MAT graph of each --scale (best of three calls).
 
 (run with graphchi-cpp_b200 on PYTHONPATH)."""
 from __future__ import annotations
@@ -126,6 +128,22 @@ def cc_report(scale, ef, seed, peak):
                                  "frac_of_one_pass_at_hbm": round(byt / ms / 1e6 / peak, 3)}}), flush=True)
 
 
+def tc_report(scale, ef, seed):
+    import torch
+    import gcgpu
+    m = ef << scale
+    s = torch.empty(m, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    gcgpu.generate_rmat(scale, m, 0.57, 0.19, 0.19, seed=seed, src=s, dst=d)
+    with gcgpu.Graph.from_edges(s, d, dedup=True, symmetrise=True, out_csr=False) as g:
+        del s, d
+        per = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+        tri = g.triangle_count(per_rank=per, vertexmap=None)[0]
+        ms = min(g.triangle_count(per_rank=per, vertexmap=None)[3].device_ms for _ in range(3))
+        print(json.dumps({"tc": {"scale": scale, "vertices": g.num_vertices, "directed_edges": g.num_edges,
+                                 "triangles": tri, "ms": round(ms, 3)}}), flush=True)
+
+
 def main():
     import torch
     import gcgpu
@@ -138,17 +156,20 @@ def main():
     ap.add_argument("--batch", type=float, nargs=2, default=None, metavar=("LO", "HI"))
     ap.add_argument("--ppr", type=int, default=0, metavar="K")
     ap.add_argument("--cc", action="store_true")
+    ap.add_argument("--tc", action="store_true")
     args = ap.parse_args()
     peak = peak_gbs()
     if args.batch:
         batch_report(args.batch[0], args.batch[1], args.hub, peak)
         return
-    if args.ppr or args.cc:
+    if args.ppr or args.cc or args.tc:
         for scale in args.scale:
             if args.ppr:
                 ppr_report(scale, args.ef, args.seed, args.ppr, peak)
             if args.cc:
                 cc_report(scale, args.ef, args.seed, peak)
+            if args.tc:
+                tc_report(scale, args.ef, args.seed)
         return
     for scale in args.scale:
         m = args.ef << scale

@@ -313,6 +313,24 @@ def test_tc_directed_input_vs_oracle():
     assert total == t and np.array_equal(per, p2) and np.array_equal(vm, v2)
 
 
+def test_tc_clique_beside_sparse_graph_vs_oracle():
+    """A 600-vertex clique beside a sparse R-MAT part: the clique's vertices have
+    hundreds of higher-ranked neighbours (searches much longer than a warp, many
+    per lane) and take the top ranks, whose counts are gathered per block in
+    shared memory; the sparse part's counts go straight to global memory."""
+    k = 600
+    cs, cd = np.triu_indices(k, 1)
+    s, d = O.rmat_numpy(12, 8 << 12, seed=4)
+    s = np.concatenate([cs.astype(np.uint32), s + k]).astype(np.uint32)
+    d = np.concatenate([cd.astype(np.uint32), d + k]).astype(np.uint32)
+    go = O.OracleGraph(s, d)
+    with gcgpu.Graph.from_edges(s, d, dedup=True) as g:
+        total, per, vm, st = g.triangle_count()
+    t, p2, v2 = go.tc()
+    assert t >= k * (k - 1) * (k - 2) // 6
+    assert total == t and np.array_equal(per, p2) and np.array_equal(vm, v2)
+
+
 # ---- full-size configs (digests) -------------------------------------------
 
 @pytest.mark.slow
