@@ -81,19 +81,28 @@ __global__ void k_unique_scatter(const uint64_t *__restrict__ keys, uint64_t n, 
         if (i == 0 || keys[i] != keys[i - 1]) out[pos[i]] = keys[i];
 }
 
-/* Sorted keys -> CSR: col = low bits; rowptr[r] = index of the first key of row r.
- * The thread owning key i writes the row pointers of rows (row(i-1), row(i)]. */
+/* Sorted keys -> CSR: col[i] = low bits of key i; rowptr[r] = number of keys
+ * whose row (high bits) is below r, found by a lower-bound search per row. Every
+ * row pointer is its own thread's work, so a long run of empty rows (the
+ * lowest ranks of a degree ordering are the isolated vertices) costs no more
+ * than any other. */
 __global__ void k_csr_from_keys(const uint64_t *__restrict__ keys, uint64_t n, uint32_t vbits, uint32_t nv,
                                 uint32_t *__restrict__ rowptr, uint32_t *__restrict__ col) {
     const uint64_t mask = (1ull << vbits) - 1ull;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t k = keys[i];
-        col[i] = (uint32_t)(k & mask);
-        int64_t row = (int64_t)(k >> vbits);
-        int64_t prev = (i == 0) ? -1 : (int64_t)(keys[i - 1] >> vbits);
-        for (int64_t r = prev + 1; r <= row; ++r) rowptr[r] = (uint32_t)i;
-        if (i == n - 1)
-            for (int64_t r = row + 1; r <= (int64_t)nv; ++r) rowptr[r] = (uint32_t)n;
+    const uint64_t total = n > (uint64_t)nv + 1 ? n : (uint64_t)nv + 1;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (i < n) col[i] = (uint32_t)(__ldg(keys + i) & mask);
+        if (i <= nv) {
+            uint64_t lo = 0, hi = n;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if ((__ldg(keys + mid) >> vbits) < i)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            rowptr[i] = (uint32_t)lo;
+        }
     }
 }
 
@@ -207,7 +216,8 @@ int csr_from_sorted_keys(const uint64_t *keys, uint64_t n, uint32_t vbits, uint3
         GCG_CUDA(cudaMemsetAsync(rowptr, 0, ((size_t)nrows + 1) * 4, s));
         return GCG_OK;
     }
-    k_csr_from_keys<<<grid_for(n), 256, 0, s>>>(keys, n, vbits, nrows, rowptr, col);
+    k_csr_from_keys<<<grid_for(std::max<uint64_t>(n, (uint64_t)nrows + 1)), 256, 0, s>>>(keys, n, vbits, nrows, rowptr,
+                                                                                       col);
     GCG_LAUNCH_CHECK();
     return GCG_OK;
 }

@@ -99,30 +99,47 @@ __device__ __forceinline__ uint32_t last_le_step(const uint32_t *__restrict__ cl
 
 constexpr uint32_t TC_WARPS = 32;   /* 1024-thread blocks, two per SM */
 constexpr uint32_t TC_TOP = 16384;  /* per-block shared counters for the top-ranked vertices */
+constexpr uint32_t TC_SPLIT = 64;   /* top-range vertices with more higher-ranked neighbours go batch by batch */
 
-/* One warp per vertex a, 32 of its higher-ranked neighbours b at a time. For each
- * b the shorter of (N+(a) after b) and N+(b) is searched element by element in
- * the longer; the searches of the 32 b's are laid end to end (a warp prefix sum
- * of their lengths) and dealt to the lanes two at a time, so every lane runs two
- * independent searches whatever the lengths. A match c is the triangle (a, b, c):
- * c's count is bumped per match, b's by its match total, a's by the sum.
+/* Longest higher-ranked neighbour list among rows lo .. nv - 1 (atomicMax into *out). */
+__global__ void k_max_rowlen(const uint32_t *__restrict__ rp, uint32_t lo, uint32_t nv, uint32_t *out) {
+    uint32_t m = 0;
+    for (uint32_t r = lo + blockIdx.x * blockDim.x + threadIdx.x; r < nv; r += gridDim.x * blockDim.x)
+        m = max(m, rp[r + 1] - rp[r]);
+    m = __reduce_max_sync(0xFFFFFFFFu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+/* Triangles through vertex a, 32 of its higher-ranked neighbours b at a time (a
+ * batch). For each b the shorter of (N+(a) after b) and N+(b) is searched element
+ * by element in the longer; the searches of the batch's b's are laid end to end
+ * (a warp prefix sum of their lengths) and dealt to the lanes two at a time, so
+ * every lane runs two independent searches whatever the lengths. A match c is the
+ * triangle (a, b, c): c's count is bumped per match, b's by its match total, a's
+ * by the batch's sum.
+ * Work is spread two ways. Vertex a goes to warp (a mod warps), numbered block
+ * fastest, so the heavy vertices, which sit together in the upper ranks, land on
+ * every SM. Vertices among the top `nsplit` ranks with more than TC_SPLIT
+ * higher-ranked neighbours are not taken whole: their batches are dealt out one
+ * by one after the other vertices, so no warp is left with a whole heavy vertex.
  * Ranks grow with degree, so the highest-ranked vertex of a triangle is nearly
  * always among the top few thousand ranks: their counts are kept in the block's
  * shared memory (dynamic, `top` entries for ranks nv - top .. nv - 1) and added
  * to `cnt` once at the end, which keeps the per-triangle increments off a few
  * hot global addresses. */
 __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ cl,
-                                                      uint32_t nv, uint32_t top, uint32_t *__restrict__ cnt,
-                                                      unsigned long long *total) {
+                                                      uint32_t nv, uint32_t top, uint32_t nsplit,
+                                                      const uint32_t *__restrict__ split_maxlen,
+                                                      uint32_t *__restrict__ cnt, unsigned long long *total) {
     extern __shared__ uint32_t s_top[];
     __shared__ uint32_t s_pre[TC_WARPS][32], s_so[TC_WARPS][32], s_lo[TC_WARPS][32], s_nl[TC_WARPS][32],
         s_hit[TC_WARPS][32];
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t *pre = s_pre[w], *so_ = s_so[w], *lo_ = s_lo[w], *nl_ = s_nl[w], *hit = s_hit[w];
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warp = w * gridDim.x + blockIdx.x;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lo_top = nv - top;
+    const uint32_t lo_top = nv - top, lo_split = nv - nsplit;
     for (uint32_t i = threadIdx.x; i < top; i += blockDim.x) s_top[i] = 0;
     __syncthreads();
     auto bump = [&](uint32_t v, uint32_t inc) {
@@ -131,74 +148,103 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
         else
             atomicAdd(cnt + v, inc);
     };
-    unsigned long long mine = 0;
-    for (uint32_t a = warp; a < nv; a += nwarps) {
-        const uint32_t ab = __ldg(rp + a), ae = __ldg(rp + a + 1);
-        if (ae - ab < 2) continue; /* a triangle needs two higher-ranked neighbours */
-        uint32_t acc = 0;
-        for (uint32_t j0 = ab; j0 + 1 < ae; j0 += 32) {
-            const uint32_t j = j0 + lane;
-            uint32_t ns = 0, so = 0, lo = 0, nl = 0, b = 0;
-            if (j + 1 < ae) {
-                b = __ldg(cl + j);
-                const uint32_t na = ae - j - 1, bb = __ldg(rp + b), nb = __ldg(rp + b + 1) - bb;
-                if (nb) {
-                    if (na <= nb) {
-                        ns = na, so = j + 1, lo = bb, nl = nb;
-                    } else {
-                        ns = nb, so = bb, lo = j + 1, nl = na;
-                    }
+    /* the batch of a's neighbours j0 .. j0 + 31 (ab <= j0, j0 + 1 < ae); returns
+     * this lane's b's match total (0 for lanes past the list) */
+    auto batch = [&](uint32_t ab, uint32_t ae, uint32_t j0) -> uint32_t {
+        const uint32_t j = j0 + lane;
+        uint32_t ns = 0, so = 0, lo = 0, nl = 0, b = 0;
+        if (j + 1 < ae) {
+            b = __ldg(cl + j);
+            const uint32_t na = ae - j - 1, bb = __ldg(rp + b), nb = __ldg(rp + b + 1) - bb;
+            if (nb) {
+                if (na <= nb) {
+                    ns = na, so = j + 1, lo = bb, nl = nb;
+                } else {
+                    ns = nb, so = bb, lo = j + 1, nl = na;
                 }
             }
-            uint32_t inc = ns;
-            for (uint32_t o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(FULL, inc, o);
-                if (lane >= o) inc += t;
+        }
+        uint32_t inc = ns;
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(FULL, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const uint32_t W = __shfl_sync(FULL, inc, 31);
+        if (W == 0) return 0u;
+        pre[lane] = inc, so_[lane] = so, lo_[lane] = lo, nl_[lane] = nl, hit[lane] = 0;
+        __syncwarp();
+        for (uint32_t t0 = 0; t0 < W; t0 += 64) {
+            uint32_t x[2], base[2], n[2], q[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const uint32_t t = t0 + 32 * u + lane;
+                n[u] = 0, x[u] = 0, base[u] = 0, q[u] = 0;
+                if (t < W) {
+                    /* owner: how many of the 32 inclusive prefix sums are <= t
+                     * (t < W = pre[31], so at most 31; indexes stay below 31) */
+                    uint32_t qq = 0;
+#pragma unroll
+                    for (uint32_t st = 16; st; st >>= 1)
+                        if (pre[qq + st - 1] <= t) qq += st;
+                    const uint32_t k = t - (qq ? pre[qq - 1] : 0);
+                    x[u] = __ldg(cl + so_[qq] + k);
+                    base[u] = lo_[qq], n[u] = nl_[qq], q[u] = qq;
+                }
             }
-            const uint32_t W = __shfl_sync(FULL, inc, 31);
-            if (W == 0) continue;
-            pre[lane] = inc, so_[lane] = so, lo_[lane] = lo, nl_[lane] = nl, hit[lane] = 0;
-            __syncwarp();
-            for (uint32_t t0 = 0; t0 < W; t0 += 64) {
-                uint32_t x[2], base[2], n[2], q[2];
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    const uint32_t t = t0 + 32 * u + lane;
-                    n[u] = 0, x[u] = 0, base[u] = 0, q[u] = 0;
-                    if (t < W) {
-                        /* owner: how many of the 32 inclusive prefix sums are <= t
-                         * (t < W = pre[31], so at most 31; indexes stay below 31) */
-                        uint32_t qq = 0;
-#pragma unroll
-                        for (uint32_t st = 16; st; st >>= 1)
-                            if (pre[qq + st - 1] <= t) qq += st;
-                        const uint32_t k = t - (qq ? pre[qq - 1] : 0);
-                        x[u] = __ldg(cl + so_[qq] + k);
-                        base[u] = lo_[qq], n[u] = nl_[qq], q[u] = qq;
-                    }
-                }
-                while (n[0] > 1 || n[1] > 1) {
-#pragma unroll
-                    for (int u = 0; u < 2; ++u)
-                        if (n[u] > 1) base[u] = last_le_step(cl, base[u], n[u], x[u]);
-                }
+            while (n[0] > 1 || n[1] > 1) {
 #pragma unroll
                 for (int u = 0; u < 2; ++u)
-                    if (n[u] == 1 && __ldg(cl + base[u]) == x[u]) {
-                        bump(x[u], 1u);
-                        atomicAdd(hit + q[u], 1u);
-                    }
+                    if (n[u] > 1) base[u] = last_le_step(cl, base[u], n[u], x[u]);
             }
-            __syncwarp();
-            const uint32_t h = hit[lane];
-            if (h) bump(b, h);
-            acc += h;
-            __syncwarp(); /* the tables are rewritten for the next 32 neighbours */
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (n[u] == 1 && __ldg(cl + base[u]) == x[u]) {
+                    bump(x[u], 1u);
+                    atomicAdd(hit + q[u], 1u);
+                }
         }
+        __syncwarp();
+        const uint32_t h = hit[lane];
+        if (h) bump(b, h);
+        __syncwarp(); /* the tables are rewritten by the next batch */
+        return h;
+    };
+    unsigned long long mine = 0;
+    auto finish = [&](uint32_t a, uint32_t acc) {
         const uint32_t A = __reduce_add_sync(FULL, acc);
         if (A && lane == 0) {
             bump(a, A);
             mine += A;
+        }
+    };
+    for (uint32_t a = warp; a < nv; a += nwarps) {
+        const uint32_t ab = __ldg(rp + a), ae = __ldg(rp + a + 1);
+        if (ae - ab < 2) continue; /* a triangle needs two higher-ranked neighbours */
+        if (a >= lo_split && ae - ab > TC_SPLIT) continue; /* dealt out batch by batch below */
+        uint32_t acc = 0;
+        for (uint32_t j0 = ab; j0 + 1 < ae; j0 += 32) acc += batch(ab, ae, j0);
+        finish(a, acc);
+    }
+    /* the split vertices' batches: item t is batch t / nsplit of vertex
+     * lo_split + t % nsplit, and goes to warp t mod warps (neighbouring vertices'
+     * batches to different warps); each lane checks one of its warp's items, the
+     * warp runs the real ones */
+    const uint64_t items = (uint64_t)nsplit * ((*split_maxlen + 31) / 32);
+    for (uint64_t k0 = 0; warp + (uint64_t)nwarps * k0 < items; k0 += 32) {
+        const uint64_t t = warp + (uint64_t)nwarps * (k0 + lane);
+        uint32_t a = 0, ab = 0, ae = 0, j0 = 0;
+        bool real = false;
+        if (t < items) {
+            a = lo_split + (uint32_t)(t % nsplit);
+            ab = __ldg(rp + a), ae = __ldg(rp + a + 1);
+            j0 = ab + 32u * (uint32_t)(t / nsplit);
+            real = ae - ab > TC_SPLIT && j0 + 1 < ae;
+        }
+        for (uint32_t m = __ballot_sync(FULL, real); m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const uint32_t va = __shfl_sync(FULL, a, l), vab = __shfl_sync(FULL, ab, l),
+                           vae = __shfl_sync(FULL, ae, l), vj0 = __shfl_sync(FULL, j0, l);
+            finish(va, batch(vab, vae, vj0));
         }
     }
     if (lane == 0 && mine) atomicAdd(total, mine);
@@ -290,10 +336,19 @@ extern "C" int gcg_triangle_count(gcg_graph *g, uint64_t *total, uint32_t *per_r
     GCG_CUDA(cudaMemsetAsync(d_total.get(), 0, 8, s));
     /* persistent: two 1024-thread blocks per SM, each with its own top-rank counters */
     const uint32_t top = std::min(nv, TC_TOP);
+    const uint32_t nsplit = std::min(nv, std::max<uint32_t>(65536u, nv / 16));
+    tbuf<uint32_t> split_maxlen;
+    GCG_TRY(split_maxlen.alloc(1, s));
+    GCG_CUDA(cudaMemsetAsync(split_maxlen.get(), 0, 4, s));
+    if (nsplit) {
+        k_max_rowlen<<<vgrid(nsplit), 256, 0, s>>>(rp.get(), nv - nsplit, nv, split_maxlen.get());
+        GCG_LAUNCH_CHECK();
+    }
     GCG_CUDA(cudaFuncSetAttribute(k_tc_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TC_TOP * 4)));
     unsigned cb = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>(((uint64_t)nv + TC_WARPS - 1) / TC_WARPS, (uint64_t)num_sms() * 2));
-    k_tc_count<<<cb, TC_WARPS * 32, (size_t)top * 4, s>>>(rp.get(), cl.get(), nv, top, cnt_ptr, d_total.get());
+    k_tc_count<<<cb, TC_WARPS * 32, (size_t)top * 4, s>>>(rp.get(), cl.get(), nv, top, nsplit, split_maxlen.get(),
+                                                          cnt_ptr, d_total.get());
     GCG_LAUNCH_CHECK();
     GCG_CUDA(cudaEventRecord(ev1, s));
     unsigned long long tri = 0;
