@@ -58,9 +58,12 @@ __global__ void __launch_bounds__(MP_THREADS) k_orient_keys(const uint32_t *__re
                                                             const uint32_t *__restrict__ col,
                                                             const uint32_t *__restrict__ tile_row,
                                                             const uint32_t *__restrict__ tile_edge, uint32_t ntiles,
-                                                            const uint32_t *__restrict__ rank, uint32_t vbits,
-                                                            uint64_t *__restrict__ keys) {
+                                                            const uint32_t *__restrict__ rank, uint32_t vbits, int half,
+                                                            uint32_t *__restrict__ count, uint64_t *__restrict__ keys) {
     __shared__ uint32_t s_rowend[MP_TILE];
+    __shared__ uint32_t s_wsum[MP_THREADS / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const uint32_t r0 = tile_row[t], r1 = tile_row[t + 1];
         const uint32_t e0 = tile_edge[t], e1 = tile_edge[t + 1];
@@ -70,15 +73,63 @@ __global__ void __launch_bounds__(MP_THREADS) k_orient_keys(const uint32_t *__re
         const uint32_t items = nrows + nedges;
         const uint32_t d0 = min((uint32_t)threadIdx.x * MP_ITEMS, items);
         const uint32_t d1 = min(d0 + MP_ITEMS, items);
-        uint32_t ti = mp_search(s_rowend, nrows, nedges, d0);
-        uint32_t tj = d0 - ti;
-        for (uint32_t d = d0; d < d1; ++d) {
-            if (ti < nrows && s_rowend[ti] <= tj) {
-                ++ti;
-            } else {
-                uint64_t a = rank[__ldg(col + e0 + tj)], b = rank[r0 + ti];
-                keys[e0 + tj] = a < b ? ((a << vbits) | b) : ((b << vbits) | a);
-                ++tj;
+        const uint32_t ti0 = mp_search(s_rowend, nrows, nedges, d0);
+        if (!half) {
+            uint32_t ti = ti0, tj = d0 - ti0;
+            for (uint32_t d = d0; d < d1; ++d) {
+                if (ti < nrows && s_rowend[ti] <= tj) {
+                    ++ti;
+                } else {
+                    uint64_t a = rank[__ldg(col + e0 + tj)], b = rank[r0 + ti];
+                    keys[e0 + tj] = a < b ? ((a << vbits) | b) : ((b << vbits) | a);
+                    ++tj;
+                }
+            }
+        } else {
+            /* symmetric graph: every edge is stored both ways and both give the
+             * same key, so only the copy in the higher-ranked endpoint's row is
+             * kept, compacted: count, block prefix sum, one global claim per
+             * tile, write (the sort that follows fixes the order) */
+            uint32_t kept = 0;
+            {
+                uint32_t ti = ti0, tj = d0 - ti0;
+                for (uint32_t d = d0; d < d1; ++d) {
+                    if (ti < nrows && s_rowend[ti] <= tj) {
+                        ++ti;
+                    } else {
+                        kept += rank[__ldg(col + e0 + tj)] <= rank[r0 + ti];
+                        ++tj;
+                    }
+                }
+            }
+            uint32_t incl = kept;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (lane == 31) s_wsum[w] = incl;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t run = 0;
+                for (uint32_t k = 0; k < MP_THREADS / 32; ++k) {
+                    const uint32_t x = s_wsum[k];
+                    s_wsum[k] = run;
+                    run += x;
+                }
+                s_base = run ? atomicAdd(count, run) : 0u;
+            }
+            __syncthreads();
+            uint64_t pos = (uint64_t)s_base + s_wsum[w] + (incl - kept);
+            uint32_t ti = ti0, tj = d0 - ti0;
+            for (uint32_t d = d0; d < d1; ++d) {
+                if (ti < nrows && s_rowend[ti] <= tj) {
+                    ++ti;
+                } else {
+                    const uint64_t a = rank[__ldg(col + e0 + tj)], b = rank[r0 + ti];
+                    if (a <= b) keys[pos++] = (a << vbits) | b;
+                    ++tj;
+                }
             }
         }
         __syncthreads();
@@ -299,22 +350,38 @@ extern "C" int gcg_triangle_count(gcg_graph *g, uint64_t *total, uint32_t *per_r
     if (ne > 0) {
         int per_sm = 4;
         unsigned tb = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>(pl.ntiles, (uint32_t)(num_sms() * per_sm)));
-        k_orient_keys<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(),
-                                               pl.tile_edge.get(), pl.ntiles, rank.get(), vbits, keys.get());
-        GCG_LAUNCH_CHECK();
-        GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), ne, 0, 2 * (int)vbits, &sorted, s));
-        /* unique: flags + scan + scatter, then CSR by the low-rank half */
+        /* a symmetric graph keeps one of the two stored copies of every edge */
+        const int half = g->symmetric ? 1 : 0;
         tbuf<uint32_t> fl, d_tot;
-        GCG_TRY(fl.alloc(ne, s));
         GCG_TRY(d_tot.alloc(1, s));
-        uint64_t *other = sorted == keys.get() ? tmp.get() : keys.get();
-        GCG_TRY(unique_u64(sorted, ne, fl.get(), d_tot.get(), other, s));
-        uint32_t tot = 0;
-        GCG_CUDA(cudaMemcpyAsync(&tot, d_tot.get(), 4, cudaMemcpyDeviceToHost, s));
-        GCG_CUDA(cudaStreamSynchronize(s));
-        m_or = tot;
-        GCG_TRY(cl.alloc(m_or));
-        GCG_TRY(csr_from_sorted_keys(other, m_or, vbits, nv, rp.get(), cl.get(), s));
+        GCG_CUDA(cudaMemsetAsync(d_tot.get(), 0, 4, s));
+        k_orient_keys<<<tb, MP_THREADS, 0, s>>>(g->in_rowptr.get(), g->in_col.get(), pl.tile_row.get(),
+                                               pl.tile_edge.get(), pl.ntiles, rank.get(), vbits, half, d_tot.get(),
+                                               keys.get());
+        GCG_LAUNCH_CHECK();
+        uint64_t nk = ne;
+        if (half) {
+            uint32_t kept = 0;
+            GCG_CUDA(cudaMemcpyAsync(&kept, d_tot.get(), 4, cudaMemcpyDeviceToHost, s));
+            GCG_CUDA(cudaStreamSynchronize(s));
+            nk = kept;
+        }
+        if (nk > 0) {
+            GCG_TRY(radix_sort_u64(keys.get(), tmp.get(), nk, 0, 2 * (int)vbits, &sorted, s));
+            /* unique: flags + scan + scatter, then CSR by the low-rank half */
+            GCG_TRY(fl.alloc(nk, s));
+            uint64_t *other = sorted == keys.get() ? tmp.get() : keys.get();
+            GCG_TRY(unique_u64(sorted, nk, fl.get(), d_tot.get(), other, s));
+            uint32_t tot = 0;
+            GCG_CUDA(cudaMemcpyAsync(&tot, d_tot.get(), 4, cudaMemcpyDeviceToHost, s));
+            GCG_CUDA(cudaStreamSynchronize(s));
+            m_or = tot;
+            GCG_TRY(cl.alloc(m_or));
+            GCG_TRY(csr_from_sorted_keys(other, m_or, vbits, nv, rp.get(), cl.get(), s));
+        } else {
+            GCG_TRY(cl.alloc(1));
+            GCG_CUDA(cudaMemsetAsync(rp.get(), 0, ((size_t)nv + 1) * 4, s));
+        }
     } else {
         GCG_TRY(cl.alloc(1));
         GCG_CUDA(cudaMemsetAsync(rp.get(), 0, ((size_t)nv + 1) * 4, s));
