@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
     auto batch = [&](uint32_t ab, uint32_t ae, uint32_t j0) -> uint32_t {
         const uint32_t j = j0 + lane;
         uint32_t ns = 0, so = 0, lo = 0, nl = 0, b = 0;
+        bool mrg = false;
         if (j + 1 < ae) {
             b = __ldg(cl + j);
             const uint32_t na = ae - j - 1, bb = __ldg(rp + b), nb = __ldg(rp + b + 1) - bb;
@@ -213,6 +214,14 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
                 } else {
                     ns = nb, so = bb, lo = j + 1, nl = na;
                 }
+                /* both lists long: a merge of the two (a warp walking na + nb
+                 * values, one partition search per lane) when the ns searches of
+                 * log2(nl) steps would take more than three steps per merged value
+                 * (a merge step is a dependent load; 1.5, 3 and 6 were measured) */
+                const uint32_t tot = na + nb;
+                if (ns * (32 - __clz((nl - 1) | 1)) > 3 * tot + 32 * (32 - __clz((tot - 1) | 1))) {
+                    mrg = true, ns = 0;
+                }
             }
         }
         uint32_t inc = ns;
@@ -221,7 +230,8 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
             if (lane >= o) inc += t;
         }
         const uint32_t W = __shfl_sync(FULL, inc, 31);
-        if (W == 0) return 0u;
+        const uint32_t merges = __ballot_sync(FULL, mrg);
+        if (W == 0 && merges == 0) return 0u;
         pre[lane] = inc, so_[lane] = so, lo_[lane] = lo, nl_[lane] = nl, hit[lane] = 0;
         __syncwarp();
         for (uint32_t t0 = 0; t0 < W; t0 += 64) {
@@ -255,6 +265,43 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
                 }
         }
         __syncwarp();
+        /* the merged pairs, one at a time by the whole warp: A = N+(a) after b,
+         * B = N+(b); lane l walks diagonals [l per, (l + 1) per) of the merge that
+         * takes A[i] when A[i] <= B[j], so B[j] is the least B value not below
+         * A[i] and A[i] is in B exactly when they are equal */
+        for (uint32_t m = merges; m; m &= m - 1) {
+            const int l = __ffs(m) - 1;
+            const uint32_t jl = j0 + (uint32_t)l, A = jl + 1, na = ae - jl - 1;
+            const uint32_t bl = __shfl_sync(FULL, b, l), B = __ldg(rp + bl), nb = __ldg(rp + bl + 1) - B;
+            const uint32_t tot = na + nb, per = (tot + 31) / 32;
+            const uint32_t d0 = min(lane * per, tot), d1 = min(d0 + per, tot);
+            uint32_t i = d0 > nb ? d0 - nb : 0, hi = min(d0, na);
+            while (i < hi) { /* first i with A[i] > B[d0 - 1 - i] */
+                const uint32_t mid = (i + hi) >> 1;
+                if (__ldg(cl + A + mid) <= __ldg(cl + B + d0 - 1 - mid))
+                    i = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint32_t k = d0 - i, found = 0;
+            uint32_t av = i < na ? __ldg(cl + A + i) : 0u, bv = k < nb ? __ldg(cl + B + k) : 0u;
+            for (uint32_t d = d0; d < d1; ++d) {
+                if (i < na && (k >= nb || av <= bv)) {
+                    if (k < nb && av == bv) {
+                        bump(av, 1u);
+                        ++found;
+                    }
+                    ++i;
+                    if (i < na) av = __ldg(cl + A + i);
+                } else {
+                    ++k;
+                    if (k < nb) bv = __ldg(cl + B + k);
+                }
+            }
+            found = __reduce_add_sync(FULL, found);
+            if (lane == 0 && found) hit[l] += found;
+            __syncwarp();
+        }
         const uint32_t h = hit[lane];
         if (h) bump(b, h);
         __syncwarp(); /* the tables are rewritten by the next batch */
