@@ -13,7 +13,8 @@
  *      each list ascending.
  *   3. one warp per vertex a; for each b in N+(a) the shorter of N+(a) after b
  *      and N+(b) is searched element by element in the longer, the searches of
- *      32 b's dealt evenly to the lanes. A match c is a triangle (a,b,c): c's
+ *      32 b's dealt evenly to the lanes (two long lists are merged by the warp
+ *      instead). A match c is a triangle (a,b,c): c's
  *      count is bumped per match, b's and a's by the match totals (counts of
  *      the top-ranked vertices gathered in shared memory first) — the
  *      per-rank incident-triangle counts of <base>_degord.4B.vout.
