@@ -168,7 +168,8 @@ __global__ void k_max_rowlen(const uint32_t *__restrict__ rp, uint32_t lo, uint3
  * (a warp prefix sum of their lengths) and dealt to the lanes two at a time, so
  * every lane runs two independent searches whatever the lengths. A match c is the
  * triangle (a, b, c): c's count is bumped per match, b's by its match total, a's
- * by the batch's sum.
+ * by the batch's sum. A b whose two lists are both long is not searched: the
+ * whole warp merges the two lists instead, after the searches.
  * Work is spread two ways. Vertex a goes to warp (a mod warps), numbered block
  * fastest, so the heavy vertices, which sit together in the upper ranks, land on
  * every SM. Vertices among the top `nsplit` ranks with more than TC_SPLIT
@@ -218,7 +219,8 @@ __global__ void __launch_bounds__(1024, 2) k_tc_count(const uint32_t *__restrict
                 /* both lists long: a merge of the two (a warp walking na + nb
                  * values, one partition search per lane) when the ns searches of
                  * log2(nl) steps would take more than three steps per merged value
-                 * (a merge step is a dependent load; 1.5, 3 and 6 were measured) */
+                 * (a merge step is a dependent load; 1.5, 2, 3, 4 and 6 were
+                 * measured) */
                 const uint32_t tot = na + nb;
                 if (ns * (32 - __clz((nl - 1) | 1)) > 3 * tot + 32 * (32 - __clz((tot - 1) | 1))) {
                     mrg = true, ns = 0;
